@@ -1,0 +1,186 @@
+"""Seeded synthetic MD systems (the reference's benchmark shapes).
+
+No dataset is involved anywhere: every state is generated from a seed, with the
+sizes, densities and temperatures of the configurations the hot path is
+measured on.  Units are reduced LJ units (epsilon = sigma = m = k_b = 1), as in
+the reference (`src/caviar/objects/force_field/lj.cpp`, `atom_data.cpp:121-126`).
+
+`MDSystem` carries one periodic system: the box (`domain box`), per-type mass
+and charge (`atom_data add_type_mass / add_type_charge`), the atoms, and the
+settings of the reference objects on the hot path (`neighborlist basic`,
+`force_field lj`, `force_field electrostatic_ewald_r`,
+`force_field electrostatic_ewald_k`, `md_simulator basic`).
+"""
+from __future__ import annotations
+
+import dataclasses
+from typing import Optional
+
+import numpy as np
+
+
+@dataclasses.dataclass
+class LJParams:
+    """force_field lj: cutoff, per-type-pair epsilon/sigma, optional cutoff_list."""
+    cutoff: float
+    epsilon: np.ndarray  # (T, T)
+    sigma: np.ndarray  # (T, T)
+    cutoff_list: Optional[np.ndarray] = None  # (T, T) or None
+    ignore_intra_molecule: bool = False
+    jump_tol: float = 0.0  # > 0 enables the reference's jump_tol clamp
+
+
+@dataclasses.dataclass
+class EwaldRParams:
+    """force_field electrostatic_ewald_r: alpha, k_electrostatic.
+
+    cutoff < 0 keeps the reference's behaviour: every Verlet-list pair is
+    summed (electrostatic_ewald_r.cpp:142-226 has no cutoff test)."""
+    alpha: float
+    k_electrostatic: float = 1.0
+    cutoff: float = -1.0
+    lam: Optional[np.ndarray] = None  # (T, T) same-molecule scaling, or None
+
+
+@dataclasses.dataclass
+class EwaldKParams:
+    """force_field electrostatic_ewald_k: alpha, k_max per axis, k_electrostatic."""
+    alpha: float
+    kmax: tuple
+    k_electrostatic: float = 1.0
+
+
+@dataclasses.dataclass
+class MDSystem:
+    lo: np.ndarray
+    hi: np.ndarray
+    mass: np.ndarray  # (T,)
+    charge: np.ndarray  # (T,)
+    pos: np.ndarray  # (N, 3) float64
+    vel: np.ndarray  # (N, 3) float64
+    type: np.ndarray  # (N,) int32
+    cutoff: float  # neighborlist cutoff
+    coef: float  # neighborlist cutoff_extra_coef
+    ghost_cutoff: float  # atom_data ghost_cutoff
+    dt: float
+    bc: tuple = (1, 1, 1)
+    mol: Optional[np.ndarray] = None  # (N,) int32 molecule index, -1 = none
+    lj: Optional[LJParams] = None
+    ewald_r: Optional[EwaldRParams] = None
+    ewald_k: Optional[EwaldKParams] = None
+    k_b: float = 1.0
+    name: str = ""
+
+    @property
+    def n(self) -> int:
+        return int(self.pos.shape[0])
+
+    @property
+    def n_types(self) -> int:
+        return int(len(self.mass))
+
+    @property
+    def box(self) -> np.ndarray:
+        return np.asarray(self.hi, np.float64) - np.asarray(self.lo, np.float64)
+
+    def copy(self) -> "MDSystem":
+        return dataclasses.replace(self, pos=self.pos.copy(), vel=self.vel.copy(), type=self.type.copy(),
+                                   mol=None if self.mol is None else self.mol.copy())
+
+
+def maxwell_boltzmann(n: int, temperature: float, rng: np.random.Generator, mass: float = 1.0) -> np.ndarray:
+    """Gaussian velocities, centre-of-mass motion removed, rescaled so that
+    2 KE / (3N - 3) = T (the reference's periodic dof, kinetic_energy.cpp:646-718)."""
+    v = rng.normal(0.0, np.sqrt(temperature / mass), size=(n, 3))
+    v -= v.mean(axis=0)
+    ke = 0.5 * mass * np.sum(v * v)
+    t_now = 2.0 * ke / (3 * n - 3)
+    if t_now > 0:
+        v *= np.sqrt(temperature / t_now)
+    return v
+
+
+def fcc_lattice(ncell: int, density: float, temperature: float, seed: int, cutoff: float = 2.5,
+                skin: float = 0.3, dt: float = 0.005) -> MDSystem:
+    """Plain LJ fluid on an FCC lattice (4 atoms per cubic cell) in a periodic
+    cube, epsilon = sigma = m = 1, lattice offset a/4 from the faces."""
+    a = (4.0 / density) ** (1.0 / 3.0)
+    L = ncell * a
+    basis = np.array([[0, 0, 0], [0.5, 0.5, 0], [0.5, 0, 0.5], [0, 0.5, 0.5]], np.float64)
+    g = np.arange(ncell, dtype=np.float64)
+    cells = np.stack(np.meshgrid(g, g, g, indexing="ij"), axis=-1).reshape(-1, 3)
+    pos = ((cells[:, None, :] + basis[None, :, :]).reshape(-1, 3) + 0.25) * a
+    n = pos.shape[0]
+    rng = np.random.default_rng(seed)
+    vel = maxwell_boltzmann(n, temperature, rng)
+    coef = (cutoff + skin) / cutoff
+    lj = LJParams(cutoff=cutoff, epsilon=np.ones((1, 1)), sigma=np.ones((1, 1)))
+    return MDSystem(lo=np.zeros(3), hi=np.full(3, L), mass=np.ones(1), charge=np.zeros(1), pos=pos, vel=vel,
+                    type=np.zeros(n, np.int32), cutoff=cutoff, coef=coef, ghost_cutoff=cutoff * coef, dt=dt,
+                    lj=lj, name=f"fcc{ncell}_N{n}")
+
+
+def random_ions(n: int, box: float, seed: int, min_sep: float = 0.9, temperature: float = 1.0,
+                lj_cutoff: float = 2.5, alpha: float = 0.3, rc: float = 10.0, coef: float = 1.03,
+                kmax: int = 8, dt: float = 0.005) -> MDSystem:
+    """Charged LJ electrolyte: n ions alternating type 0 (q=+1) / type 1 (q=-1),
+    uniform in a periodic cube with a minimum separation (cell-grid
+    rejection), Gaussian velocities at T with COM removed.
+
+    The neighbour list is sized for the Ewald real-space cutoff rc (the larger
+    one); LJ keeps its own 2.5 sigma cutoff test on that list."""
+    rng = np.random.default_rng(seed)
+    ncell = max(1, int(np.floor(box / min_sep)))
+    w = box / ncell
+    grid: dict = {}
+    pos = np.empty((n, 3))
+    k = 0
+    ms2 = min_sep * min_sep
+    while k < n:
+        p = rng.uniform(0.0, box, size=3)
+        c = tuple(int(x) for x in np.minimum((p / w).astype(np.int64), ncell - 1))
+        ok = True
+        for dx in (-1, 0, 1):
+            for dy in (-1, 0, 1):
+                for dz in (-1, 0, 1):
+                    q = ((c[0] + dx) % ncell, (c[1] + dy) % ncell, (c[2] + dz) % ncell)
+                    for j in grid.get(q, ()):
+                        d = p - pos[j]
+                        d -= box * np.round(d / box)
+                        if d @ d < ms2:
+                            ok = False
+                            break
+                    if not ok:
+                        break
+                if not ok:
+                    break
+            if not ok:
+                break
+        if ok:
+            pos[k] = p
+            grid.setdefault(c, []).append(k)
+            k += 1
+    vel = rng.normal(0.0, np.sqrt(temperature), size=(n, 3))
+    vel -= vel.mean(axis=0)
+    typ = (np.arange(n) % 2).astype(np.int32)
+    lj = LJParams(cutoff=lj_cutoff, epsilon=np.ones((2, 2)), sigma=np.ones((2, 2)))
+    er = EwaldRParams(alpha=alpha, k_electrostatic=1.0)
+    ek = EwaldKParams(alpha=alpha, kmax=(kmax, kmax, kmax), k_electrostatic=1.0)
+    return MDSystem(lo=np.zeros(3), hi=np.full(3, box), mass=np.ones(2), charge=np.array([1.0, -1.0]), pos=pos,
+                    vel=vel, type=typ, cutoff=rc, coef=coef, ghost_cutoff=rc * coef, dt=dt, lj=lj, ewald_r=er,
+                    ewald_k=ek, name=f"ions_N{n}_L{box:g}")
+
+
+def config_lj_4000(seed: int = 1) -> MDSystem:
+    """4000 LJ atoms, FCC 10^3 cells, rho* = 0.8442, T* = 0.72, rc 2.5, skin 0.3, dt 0.005."""
+    return fcc_lattice(10, 0.8442, 0.72, seed)
+
+
+def config_ions_8000(seed: int = 2) -> MDSystem:
+    """8000 ions (+-1) in L = 40, LJ rc 2.5, Ewald alpha 0.3, rc 10 (skin 0.3), kmax 8, T* = 1."""
+    return random_ions(8000, 40.0, seed)
+
+
+def config_lj_1m(seed: int = 3) -> MDSystem:
+    """1,048,576 LJ atoms, FCC 64^3 cells, rho* = 0.8442, T* = 0.72, rc 2.5, skin 0.3."""
+    return fcc_lattice(64, 0.8442, 0.72, seed)

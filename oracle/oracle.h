@@ -1,0 +1,87 @@
+/* oracle.h -- CPU FP64 restatement of CAVIAR's per-timestep particle path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This is the checker that the CUDA path is
+ * compared against (tests/, __graft_entry__.smoke, bench.py's cpu_baseline
+ * leg); the product (caviar_b200/) never links or calls it.
+ *
+ * Parity pinning: the restatement is checked bit-for-bit against the
+ * unmodified reference compiled from its own sources (oracle/_ref, see
+ * Makefile and ref_harness.cpp) and against the published Ewald golden
+ * forces (tests/golden/).  Every function cites the reference file:line it
+ * follows; paths are relative to the reference project root.
+ */
+#ifndef CAVIAR_ORACLE_H
+#define CAVIAR_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct orc_sys orc_sys;
+
+/* Rebuild policies of the Verlet list.
+ *  ORC_REBUILD_DISPLACEMENT: rebuild only when an atom moved more than half
+ *    the skin since the last build; positions are wrapped at rebuilds only.
+ *  ORC_REBUILD_REFERENCE: the reference's trigger -- any owned wrap, a change
+ *    of ghost count, or any owned/ghost displacement above half the skin
+ *    (md_simulator.cpp:487-502, neighborlist.cpp:91-139); wrap every step.
+ *  ORC_REBUILD_EVERY_STEP: Neighborlist `rebuild_test` (neighborlist.cpp:98-101). */
+enum { ORC_REBUILD_DISPLACEMENT = 0, ORC_REBUILD_REFERENCE = 1, ORC_REBUILD_EVERY_STEP = 2 };
+
+orc_sys *orc_create(const double lo[3], const double hi[3], const int bc[3],
+                    int n_types, const double *mass, const double *charge);
+void orc_destroy(orc_sys *s);
+
+int orc_set_atoms(orc_sys *s, int64_t n, const double *pos, const double *vel,
+                  const int32_t *type, const int32_t *mol);
+void orc_set_neighborlist(orc_sys *s, double cutoff, double cutoff_extra_coef,
+                          double ghost_cutoff, int all_atom_test);
+/* eps, sigma: n_types*n_types row-major; cutoff_list may be NULL. jump_tol <= 0 disables. */
+void orc_set_lj(orc_sys *s, double cutoff, const double *eps, const double *sigma,
+                const double *cutoff_list, int ignore_intra_molecule, double jump_tol);
+/* lambda may be NULL; cutoff < 0 keeps the reference's behaviour (no cutoff test). */
+void orc_set_ewald_r(orc_sys *s, double alpha, double k_electrostatic, const double *lambda,
+                     double cutoff);
+void orc_set_ewald_k(orc_sys *s, double alpha, int kx_max, int ky_max, int kz_max,
+                     double k_electrostatic);
+void orc_set_integrator(orc_sys *s, double dt, double k_b, int rebuild_policy);
+
+/* Md_simulator::setup (md_simulator.cpp:504-549): wrap, ghosts, list, forces. */
+int orc_setup(orc_sys *s);
+/* One velocity-Verlet step (md_simulator.cpp:555-668). */
+int orc_step(orc_sys *s);
+/* Build the list at the current positions (setup's wrap+ghost+build(true)) without forces. */
+int orc_build_list(orc_sys *s);
+/* Forces at the current positions with the current list (re_calculate_acc's force part). */
+int orc_compute_forces(orc_sys *s);
+
+/* Canonical pair set (id_a < id_b, shift of b), 5 int32 per pair, sorted.
+ * Returns the pair count; out may be NULL to only count. */
+int64_t orc_pairs(orc_sys *s, int32_t *out);
+int orc_get_state(const orc_sys *s, double *pos, double *vel, double *acc);
+int64_t orc_n_kvec_used(const orc_sys *s);
+/* S(k) of the used k-vectors from the last force call: 2 doubles (re, im) each. */
+int orc_get_sk(const orc_sys *s, double *out);
+
+/* Scalars, in this order:
+ *  0 virial (virialForce: LJ + Ewald-r, each pair once)
+ *  1 kinetic energy (COM-removed when all axes are periodic, kinetic_energy.cpp:58-72)
+ *  2 LJ energy of the linear force-shifted pair potential (the restatement's own)
+ *  3 Ewald real-space energy over the list pairs (the restatement's own)
+ *  4 Ewald k-space energy (electrostatic_ewald_k/energy.cpp:61-107)
+ *  5 Ewald self energy (energy.cpp:31-50)
+ *  6 number of list builds so far
+ *  7 number of ghosts at the last ghost exchange
+ *  8 degrees of freedom (kinetic_energy.cpp:680-718)
+ */
+#define ORC_N_SCALARS 9
+int orc_get_scalars(orc_sys *s, double *out);
+/* Evaluate energies (scalars 2..5) at the current positions and list. */
+int orc_energy(orc_sys *s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
