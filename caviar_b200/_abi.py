@@ -1,0 +1,244 @@
+"""ctypes binding of libcaviar_b200.so (the C ABI in include/caviar_b200.h).
+
+`Simulation` wraps one context.  There is no fallback: if the library or a
+CUDA device is missing, construction raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libcaviar_b200.so")
+
+OK = 0
+ERR = {1: "INVALID", 2: "CUDA", 3: "NAN", 4: "STATE", 5: "GEOMETRY", 6: "CAPACITY", 7: "NOMEM"}
+PREC_MIXED, PREC_FP64 = 0, 1
+REBUILD_DISPLACEMENT, REBUILD_REFERENCE, REBUILD_EVERY_STEP = 0, 1, 2
+TH_KEYS = ["step", "ke", "temperature", "e_lj", "e_ewald_r", "e_ewald_k", "e_self", "virial", "pressure", "builds"]
+N_THERMO = len(TH_KEYS)
+KT_PAIR, KT_KSPACE, KT_INTEGRATE, KT_BUILD = 0, 1, 2, 3
+
+# Every symbol declared in include/caviar_b200.h.
+EXPORTED = ["cvr_create", "cvr_destroy", "cvr_set_neighborlist", "cvr_set_lj", "cvr_set_ewald_r", "cvr_set_ewald_k",
+            "cvr_set_integrator", "cvr_set_precision", "cvr_set_state", "cvr_build_neighbors", "cvr_compute_forces",
+            "cvr_run", "cvr_get_state", "cvr_get_pairs", "cvr_get_sk", "cvr_get_scalars", "cvr_last_error",
+            "cvr_launch_count", "cvr_get_stream", "cvr_get_info", "cvr_set_kernel_timing", "cvr_kernel_time"]
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int32)
+_lib = None
+
+
+class CvrError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"CVR_ERR_{ERR.get(code, code)}: {msg}")
+        self.code = code
+
+
+def load(path: str = LIB_PATH):
+    """Load the library (raises if it is missing: there is no CPU path)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} not built; run python -m caviar_b200.build")
+    L = ctypes.CDLL(path)
+    vp = ctypes.c_void_p
+    L.cvr_create.argtypes = [ctypes.POINTER(vp), _dp, _dp, ctypes.POINTER(ctypes.c_int), ctypes.c_int, _dp, _dp,
+                             ctypes.c_int]
+    L.cvr_destroy.argtypes = [vp]
+    L.cvr_destroy.restype = None
+    L.cvr_set_neighborlist.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int]
+    L.cvr_set_lj.argtypes = [vp, ctypes.c_double, _dp, _dp, _dp, ctypes.c_int]
+    L.cvr_set_ewald_r.argtypes = [vp, ctypes.c_double, ctypes.c_double, _dp, ctypes.c_double]
+    L.cvr_set_ewald_k.argtypes = [vp, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double]
+    L.cvr_set_integrator.argtypes = [vp, ctypes.c_double, ctypes.c_double]
+    L.cvr_set_precision.argtypes = [vp, ctypes.c_int]
+    L.cvr_set_state.argtypes = [vp, ctypes.c_int64, vp, vp, vp, vp]
+    L.cvr_build_neighbors.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+    L.cvr_compute_forces.argtypes = [vp, vp, _dp]
+    L.cvr_run.argtypes = [vp, ctypes.c_int64, ctypes.c_int64, _dp]
+    L.cvr_get_state.argtypes = [vp, vp, vp, vp]
+    L.cvr_get_pairs.argtypes = [vp, _ip]
+    L.cvr_get_pairs.restype = ctypes.c_int64
+    L.cvr_get_sk.argtypes = [vp, _dp]
+    L.cvr_get_sk.restype = ctypes.c_int64
+    L.cvr_get_scalars.argtypes = [vp, _dp]
+    L.cvr_last_error.argtypes = [vp, ctypes.c_char_p, ctypes.c_size_t]
+    L.cvr_launch_count.argtypes = [vp]
+    L.cvr_launch_count.restype = ctypes.c_int64
+    L.cvr_get_stream.argtypes = [vp]
+    L.cvr_get_stream.restype = vp
+    L.cvr_get_info.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), ctypes.c_int]
+    L.cvr_set_kernel_timing.argtypes = [vp, ctypes.c_int]
+    L.cvr_kernel_time.argtypes = [vp, ctypes.c_int, _dp, ctypes.POINTER(ctypes.c_int64)]
+    _lib = L
+    return L
+
+
+def _d(a):
+    if a is None:
+        return None
+    return np.ascontiguousarray(a, np.float64).ctypes.data_as(_dp)
+
+
+def _ptr(a):
+    return None if a is None else ctypes.c_void_p(a.ctypes.data)
+
+
+class Simulation:
+    """One periodic system on one GPU, driven through the C ABI."""
+
+    def __init__(self, system=None, *, precision: int = PREC_MIXED, policy: int = REBUILD_DISPLACEMENT,
+                 device: int = 0, lo=None, hi=None, bc=(1, 1, 1), mass=None, charge=None):
+        self.L = load()
+        if system is not None:
+            lo, hi, bc, mass, charge = system.lo, system.hi, system.bc, system.mass, system.charge
+        lo = np.ascontiguousarray(lo, np.float64)
+        hi = np.ascontiguousarray(hi, np.float64)
+        mass = np.ascontiguousarray(mass, np.float64)
+        charge = np.ascontiguousarray(np.zeros_like(mass) if charge is None else charge, np.float64)
+        self.n_types = len(mass)
+        h = ctypes.c_void_p()
+        bca = (ctypes.c_int * 3)(*[int(b) for b in bc])
+        rc = self.L.cvr_create(ctypes.byref(h), _d(lo), _d(hi), bca, self.n_types, _d(mass), _d(charge), device)
+        if rc != OK:
+            raise CvrError(rc, "cvr_create failed")
+        self.h = h
+        self.n = 0
+        self._check(self.L.cvr_set_precision(self.h, precision))
+        if system is not None:
+            self.configure(system, policy)
+            self.set_state(system.pos, system.vel, system.type, system.mol)
+
+    # -- plumbing
+    def _check(self, rc):
+        if rc != OK:
+            buf = ctypes.create_string_buffer(512)
+            self.L.cvr_last_error(self.h, buf, 512)
+            raise CvrError(rc, buf.value.decode(errors="replace"))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.cvr_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- settings
+    def configure(self, s, policy: int = REBUILD_DISPLACEMENT):
+        self._check(self.L.cvr_set_neighborlist(self.h, s.cutoff, s.coef, s.ghost_cutoff, policy))
+        if s.lj is not None:
+            cl = None if s.lj.cutoff_list is None else s.lj.cutoff_list
+            self._check(self.L.cvr_set_lj(self.h, s.lj.cutoff, _d(s.lj.epsilon), _d(s.lj.sigma), _d(cl),
+                                          int(s.lj.ignore_intra_molecule)))
+        if s.ewald_r is not None:
+            self._check(self.L.cvr_set_ewald_r(self.h, s.ewald_r.alpha, s.ewald_r.k_electrostatic,
+                                               _d(s.ewald_r.lam), s.ewald_r.cutoff))
+        if s.ewald_k is not None:
+            kx, ky, kz = s.ewald_k.kmax
+            self._check(self.L.cvr_set_ewald_k(self.h, s.ewald_k.alpha, kx, ky, kz, s.ewald_k.k_electrostatic))
+        self._check(self.L.cvr_set_integrator(self.h, s.dt, s.k_b))
+
+    def set_state(self, pos, vel=None, typ=None, mol=None):
+        pos = np.ascontiguousarray(pos, np.float64)
+        n = pos.shape[0]
+        vel = None if vel is None else np.ascontiguousarray(vel, np.float64)
+        typ = np.ascontiguousarray(np.zeros(n, np.int32) if typ is None else typ, np.int32)
+        mol = None if mol is None else np.ascontiguousarray(mol, np.int32)
+        self._check(self.L.cvr_set_state(self.h, n, _ptr(pos), _ptr(vel), _ptr(typ), _ptr(mol)))
+        self.n = n
+
+    def set_state_ptr(self, n, pos_ptr, vel_ptr, type_ptr, mol_ptr=None):
+        """Host pointers (e.g. pinned torch tensors) without numpy copies."""
+        self._check(self.L.cvr_set_state(self.h, n, ctypes.c_void_p(pos_ptr), ctypes.c_void_p(vel_ptr),
+                                         ctypes.c_void_p(type_ptr), None if mol_ptr is None else ctypes.c_void_p(mol_ptr)))
+        self.n = n
+
+    # -- hot path
+    def build_neighbors(self, force: bool = True) -> bool:
+        r = ctypes.c_int(0)
+        self._check(self.L.cvr_build_neighbors(self.h, int(force), ctypes.byref(r)))
+        return bool(r.value)
+
+    def compute_forces(self):
+        acc = np.zeros((self.n, 3))
+        th = np.zeros(N_THERMO)
+        self._check(self.L.cvr_compute_forces(self.h, _ptr(acc), _d(th)))
+        return acc, dict(zip(TH_KEYS, th.tolist()))
+
+    def run(self, nsteps: int, thermo_every: int = 0):
+        nrec = nsteps // thermo_every if thermo_every > 0 else 0
+        th = np.zeros((max(nrec, 1), N_THERMO))
+        self._check(self.L.cvr_run(self.h, nsteps, thermo_every, th.ctypes.data_as(_dp)))
+        return th[:nrec]
+
+    def run_ptr(self, nsteps: int, thermo_every: int, thermo_ptr: Optional[int]):
+        self._check(self.L.cvr_run(self.h, nsteps, thermo_every,
+                                   None if thermo_ptr is None else ctypes.cast(thermo_ptr, _dp)))
+
+    # -- readback
+    def state(self):
+        pos = np.zeros((self.n, 3))
+        vel = np.zeros((self.n, 3))
+        acc = np.zeros((self.n, 3))
+        self._check(self.L.cvr_get_state(self.h, _ptr(pos), _ptr(vel), _ptr(acc)))
+        return pos, vel, acc
+
+    def get_state_ptr(self, pos_ptr, vel_ptr, acc_ptr):
+        self._check(self.L.cvr_get_state(self.h, ctypes.c_void_p(pos_ptr) if pos_ptr else None,
+                                         ctypes.c_void_p(vel_ptr) if vel_ptr else None,
+                                         ctypes.c_void_p(acc_ptr) if acc_ptr else None))
+
+    def pairs(self) -> np.ndarray:
+        m = self.L.cvr_get_pairs(self.h, None)
+        if m < 0:
+            self._check(int(-m))
+        out = np.zeros((m, 5), np.int32)
+        m2 = self.L.cvr_get_pairs(self.h, out.ctypes.data_as(_ip))
+        if m2 < 0:
+            self._check(int(-m2))
+        return out
+
+    def sk(self) -> np.ndarray:
+        m = self.L.cvr_get_sk(self.h, None)
+        out = np.zeros((max(m, 0), 2))
+        if m > 0:
+            self.L.cvr_get_sk(self.h, out.ctypes.data_as(_dp))
+        return out[:, 0] + 1j * out[:, 1]
+
+    def scalars(self) -> dict:
+        th = np.zeros(N_THERMO)
+        self._check(self.L.cvr_get_scalars(self.h, th.ctypes.data_as(_dp)))
+        return dict(zip(TH_KEYS, th.tolist()))
+
+    def info(self) -> dict:
+        v = (ctypes.c_int64 * 12)()
+        self._check(self.L.cvr_get_info(self.h, v, 12))
+        keys = ["n", "ncx", "ncy", "ncz", "cap", "builds", "tpa", "nk", "R", "max_count", "err", "step"]
+        return dict(zip(keys, list(v)))
+
+    @property
+    def launches(self) -> int:
+        return int(self.L.cvr_launch_count(self.h))
+
+    @property
+    def stream(self) -> int:
+        return int(self.L.cvr_get_stream(self.h) or 0)
+
+    def set_kernel_timing(self, on: bool):
+        self._check(self.L.cvr_set_kernel_timing(self.h, int(on)))
+
+    def kernel_time(self, kind: int):
+        ms = ctypes.c_double(0)
+        n = ctypes.c_int64(0)
+        self._check(self.L.cvr_kernel_time(self.h, kind, ctypes.byref(ms), ctypes.byref(n)))
+        return ms.value, n.value

@@ -1,0 +1,1199 @@
+// cvr_abi.cu -- host orchestration behind the C ABI of include/caviar_b200.h.
+//
+// One context = one periodic system resident in HBM.  A step is a fixed
+// sequence of stream launches:
+//   kick_drift -> [bin_count, scan x3, bin_scatter, rank, permute, build_list]
+//   -> pair (LJ + Ewald r) -> [sk_partial, sk_reduce, kforce] -> kick -> [thermo]
+// The bracketed build kernels exit at once unless kick_drift raised the
+// rebuild flag, so the host never waits on the device inside a run.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <array>
+#include <tuple>
+#include <vector>
+
+#include "../../include/caviar_b200.h"
+#include "cvr_build.cuh"
+#include "cvr_device.cuh"
+#include "cvr_force.cuh"
+
+using namespace cvr;
+
+namespace {
+
+constexpr int KCH = 64;  // atoms per S(k) chunk
+
+struct DBuf {
+  void *p = nullptr;
+  size_t bytes = 0;
+};
+
+struct KT {
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev;
+  size_t used = 0;
+  double ms = 0;
+  int64_t launches = 0;
+};
+
+}  // namespace
+
+struct cvr_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  // domain + types
+  double lo[3], hi[3], L[3];
+  int bc[3];
+  int n_types = 0;
+  std::vector<double> mass, charge;
+  // neighbour list
+  bool nl_set = false;
+  double cutoff = 0, coef = 1.12347, gc = 0;
+  int policy = CVR_REBUILD_DISPLACEMENT;
+  // LJ
+  bool lj_on = false;
+  double lj_cut = 0;
+  std::vector<double> eps, sig, cutl;
+  int ignore_intra = 0;
+  // Ewald r
+  bool ewr_on = false;
+  double ewr_alpha = 1, ewr_ke = 1, ewr_cut = -1;
+  std::vector<double> lam;
+  // Ewald k
+  bool ewk_on = false;
+  double ewk_alpha = 1, ewk_ke = 1;
+  int kmax[3] = {1, 1, 1};
+  // integrator
+  double dt = 0.001, k_b = 1.0;
+  int precision = CVR_PREC_MIXED;
+  // state
+  int64_t n = 0;
+  bool have_state = false, list_valid = false, setup_done = false, use_mol = false;
+  int64_t step = 0;
+  int R = 2, nc[3] = {1, 1, 1}, ncells = 1;
+  double w[3] = {1, 1, 1};
+  int tpa = 1, log2_tpa = 0, cap = 0, n_pad = 0;
+  // k space
+  int nk = 0, nruns = 0, kp = 2;
+  std::vector<int4> kint;
+  std::vector<double> fk;
+  std::vector<KRun> runs;
+  double e_self = 0, total_mass = 0;
+  // device memory
+  std::vector<std::pair<void **, size_t>> atom_bufs;
+  // per atom
+  double *x{}, *y{}, *z{}, *vx{}, *vy{}, *vz{};
+  void *ax{}, *ay{}, *az{}, *x4{};
+  float4 *xb{};
+  int *cell{}, *id{}, *type{}, *mol{};
+  int8_t *gcls{};
+  double *tx{}, *ty{}, *tz{}, *tvx{}, *tvy{}, *tvz{};
+  int *tid{}, *ttype{}, *tmol{}, *tcell{}, *slot_atom{}, *perm{};
+  double *stage{};
+  int *stage_i{};
+  int *ncount{};
+  // snapshot for replay after a list overflow
+  std::vector<std::pair<void *, void *>> snap_pairs;
+  std::vector<size_t> snap_bytes;
+  // cells
+  int *cell_count{}, *cell_start{}, *cell_fill{}, *block_sums{};
+  // list
+  uint32_t *nlist{};
+  size_t nlist_bytes = 0;
+  // flags: [flag, err, max_count, n_builds]
+  int *flags{};
+  double *d_mass_inv{}, *d_mass{}, *d_charge{};
+  void *d_coef{}, *d_offs{};
+  // partials
+  double *ev_part{}, *ke_part{}, *ek_part{};
+  int n_ev_blocks = 0, n_ke_blocks = 0, n_ek_blocks = 0;
+  double *d_thermo{};
+  size_t thermo_cap = 0;
+  // k space device
+  int4 *d_kint{};
+  double *d_fk{};
+  KRun *d_runs{};
+  double2 *d_kpartial{}, *d_sk{};
+  void *d_ak{};
+  int nchunks = 0;
+  // diagnostics
+  std::string err;
+  int64_t launches = 0;
+  double last_thermo[CVR_N_THERMO] = {0};
+  bool timing = false;
+  KT kt[CVR_N_KT];
+  std::vector<void *> all_allocs;
+};
+
+// ------------------------------------------------------------------ helpers
+namespace {
+
+int fail(cvr_ctx *c, int code, const std::string &msg) {
+  if (c) c->err = msg;
+  return code;
+}
+
+#define CVR_CUDA(ctx, call)                                                                        \
+  do {                                                                                             \
+    cudaError_t e_ = (call);                                                                       \
+    if (e_ != cudaSuccess) return fail((ctx), CVR_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+template <typename T>
+int dalloc(cvr_ctx *c, T **p, size_t count) {
+  if (*p) {
+    cudaFree(*p);
+    auto it = std::find(c->all_allocs.begin(), c->all_allocs.end(), (void *)*p);
+    if (it != c->all_allocs.end()) c->all_allocs.erase(it);
+    *p = nullptr;
+  }
+  if (count == 0) count = 1;
+  void *q = nullptr;
+  cudaError_t e = cudaMalloc(&q, count * sizeof(T));
+  if (e != cudaSuccess) return fail(c, CVR_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  cudaMemsetAsync(q, 0, count * sizeof(T), c->stream);
+  c->all_allocs.push_back(q);
+  *p = (T *)q;
+  return CVR_OK;
+}
+
+inline int grid_for(int64_t n, int block) { return (int)((n + block - 1) / block); }
+
+template <typename real>
+DevState<real> dev_state(cvr_ctx *c) {
+  DevState<real> s{};
+  s.n = (int)c->n;
+  s.n_pad = c->n_pad;
+  s.cap = c->cap;
+  s.tpa = c->tpa;
+  s.policy = c->policy;
+  s.n_types = c->n_types;
+  for (int d = 0; d < 3; ++d) {
+    s.box.lo[d] = c->lo[d];
+    s.box.hi[d] = c->hi[d];
+    s.box.L[d] = c->L[d];
+    s.box.gclo[d] = c->lo[d] + c->gc;  // x_llow = lower_global.x + ghost_cutoff
+    s.box.gchi[d] = c->hi[d] - c->gc;  // x_lupp = upper_global.x - ghost_cutoff
+    s.box.bc[d] = c->bc[d];
+    s.cells.nc[d] = c->nc[d];
+    s.cells.w[d] = c->w[d];
+    s.cells.inv_w[d] = 1.0 / c->w[d];
+  }
+  s.cells.ncells = c->ncells;
+  s.cells.R = c->R;
+  s.cells.S = 2 * c->R + 1;
+  const double rl = c->cutoff * c->coef;  // cutoff_extra = cutoff * cutoff_extra_coef
+  s.rl_sq = rl * rl;
+  s.rl_sq_lo = (float)(s.rl_sq * (1.0 - 1e-5));
+  s.rl_sq_hi = (float)(s.rl_sq * (1.0 + 1e-5));
+  const double half_skin = 0.5 * (rl - c->cutoff);  // threshold_distance_sq = 0.25 (rl - rc)^2
+  s.thr_sq = (float)(half_skin * half_skin);
+  s.x = c->x;
+  s.y = c->y;
+  s.z = c->z;
+  s.vx = c->vx;
+  s.vy = c->vy;
+  s.vz = c->vz;
+  s.ax = (real *)c->ax;
+  s.ay = (real *)c->ay;
+  s.az = (real *)c->az;
+  s.x4 = (typename V4<real>::t *)c->x4;
+  s.xb = c->xb;
+  s.cell = c->cell;
+  s.id = c->id;
+  s.type = c->type;
+  s.mol = c->mol;
+  s.gcls = c->gcls;
+  s.tx = c->tx;
+  s.ty = c->ty;
+  s.tz = c->tz;
+  s.tvx = c->tvx;
+  s.tvy = c->tvy;
+  s.tvz = c->tvz;
+  s.tid = c->tid;
+  s.ttype = c->ttype;
+  s.tmol = c->tmol;
+  s.tcell = c->tcell;
+  s.cell_count = c->cell_count;
+  s.cell_start = c->cell_start;
+  s.cell_fill = c->cell_fill;
+  s.slot_atom = c->slot_atom;
+  s.perm = c->perm;
+  s.block_sums = c->block_sums;
+  s.nlist = c->nlist;
+  s.ncount = c->ncount;
+  s.flag = c->flags;
+  s.err = c->flags + 1;
+  s.max_count = c->flags + 2;
+  s.n_builds = c->flags + 3;
+  s.mass_inv = c->d_mass_inv;
+  s.mass = c->d_mass;
+  return s;
+}
+
+// Event-bracketed launches for cvr_kernel_time.
+struct Bracket {
+  cvr_ctx *c;
+  int kind;
+  cudaEvent_t stop = nullptr;
+  Bracket(cvr_ctx *c_, int kind_) : c(c_), kind(kind_) {
+    if (!c->timing) return;
+    KT &k = c->kt[kind];
+    if (k.used == k.ev.size()) {
+      cudaEvent_t a, b;
+      cudaEventCreate(&a);
+      cudaEventCreate(&b);
+      k.ev.emplace_back(a, b);
+    }
+    cudaEventRecord(k.ev[k.used].first, c->stream);
+    stop = k.ev[k.used].second;
+    k.used++;
+    k.launches++;
+  }
+  ~Bracket() {
+    if (stop) cudaEventRecord(stop, c->stream);
+  }
+};
+
+void collect_timing(cvr_ctx *c) {
+  if (!c->timing) return;
+  cudaStreamSynchronize(c->stream);
+  for (auto &k : c->kt) {
+    for (size_t u = 0; u < k.used; ++u) {
+      float ms = 0;
+      if (cudaEventElapsedTime(&ms, k.ev[u].first, k.ev[u].second) == cudaSuccess) k.ms += ms;
+    }
+    k.used = 0;
+  }
+}
+
+// -------------------------------------------------------------- geometry
+int setup_cells(cvr_ctx *c) {
+  const double rl = c->cutoff * c->coef;
+  if (!(rl > 0)) return fail(c, CVR_ERR_INVALID, "neighbour list cutoff must be positive");
+  int64_t nct = 1;
+  for (int d = 0; d < 3; ++d) {
+    // cells at least rl/R wide (with a relative margin), so pairs within rl are <= R cells apart
+    int k = (int)std::floor(c->L[d] * c->R / (rl * (1.0 + 1e-10)));
+    k = std::max(1, std::min(k, 1024));
+    c->nc[d] = k;
+    c->w[d] = c->L[d] / k;
+    nct *= k;
+  }
+  if (nct > (int64_t)1 << 26) return fail(c, CVR_ERR_GEOMETRY, "too many cells");
+  c->ncells = (int)nct;
+  return CVR_OK;
+}
+
+int upload_tables(cvr_ctx *c) {
+  const int T = c->n_types;
+  const bool dbl = c->precision == CVR_PREC_FP64;
+  std::vector<PairCoef<double>> cd(T * T);
+  for (int a = 0; a < T; ++a)
+    for (int b = 0; b < T; ++b) {
+      PairCoef<double> &p = cd[a * T + b];
+      p = PairCoef<double>{};
+      p.lam = 1.0;
+      p.rc2 = -1.0;
+      if (c->lj_on) {
+        const double e = c->eps[a * T + b], s = c->sig[a * T + b];
+        const double rc = c->cutl.empty() ? c->lj_cut : c->cutl[a * T + b];
+        const double rc2 = rc * rc;
+        if (e != 0.0 && rc > 0) {  // lj.cpp:435-436 skips eps = 0
+          const double rcinv = 1.0 / rc2;
+          const double c2 = s * s * rcinv, c6 = c2 * c2 * c2, c12 = c6 * c6;
+          p.sig2 = s * s;
+          p.eps24 = 24.0 * e;
+          p.eps48 = 48.0 * e;
+          p.K = 4.0 * e * (12.0 * c12 * rcinv - 6.0 * c6 * rcinv);
+          p.rc2 = rc2;
+          const double g = 4.0 * e * (12.0 * c12 - 6.0 * c6);
+          p.e4 = 4.0 * e;
+          p.C1 = g / (2.0 * rc2);
+          p.C0 = -4.0 * e * (c12 - c6) - 0.5 * g;
+        }
+      }
+      if (c->ewr_on) {
+        p.qq = c->ewr_ke * c->charge[a] * c->charge[b];
+        if (!c->lam.empty()) p.lam = c->lam[a * T + b];
+      }
+    }
+  const int S = 2 * c->R + 1;
+  std::vector<double4> od(S * S * S);
+  for (int code = 0; code < S * S * S; ++code) {
+    const int dx = code % S - c->R, dy = (code / S) % S - c->R, dz = code / (S * S) - c->R;
+    od[code] = make_double4(dx * c->w[0], dy * c->w[1], dz * c->w[2], 0.0);
+  }
+  if (dbl) {
+    if (int r = dalloc(c, (PairCoef<double> **)&c->d_coef, T * T)) return r;
+    CVR_CUDA(c, cudaMemcpyAsync(c->d_coef, cd.data(), T * T * sizeof(PairCoef<double>), cudaMemcpyHostToDevice, c->stream));
+    if (int r = dalloc(c, (double4 **)&c->d_offs, S * S * S)) return r;
+    CVR_CUDA(c, cudaMemcpyAsync(c->d_offs, od.data(), od.size() * sizeof(double4), cudaMemcpyHostToDevice, c->stream));
+  } else {
+    std::vector<PairCoef<float>> cf(T * T);
+    for (int t = 0; t < T * T; ++t) {
+      const auto &p = cd[t];
+      cf[t] = PairCoef<float>{(float)p.sig2, (float)p.eps24, (float)p.eps48, (float)p.K, (float)p.rc2,
+                              (float)p.qq,   (float)p.e4,    (float)p.C0,    (float)p.C1, (float)p.lam};
+    }
+    std::vector<float4> of(S * S * S);
+    for (int code = 0; code < S * S * S; ++code) {
+      const int dx = code % S - c->R, dy = (code / S) % S - c->R, dz = code / (S * S) - c->R;
+      of[code] = make_float4(dx * (float)c->w[0], dy * (float)c->w[1], dz * (float)c->w[2], 0.f);
+    }
+    if (int r = dalloc(c, (PairCoef<float> **)&c->d_coef, T * T)) return r;
+    CVR_CUDA(c, cudaMemcpyAsync(c->d_coef, cf.data(), T * T * sizeof(PairCoef<float>), cudaMemcpyHostToDevice, c->stream));
+    if (int r = dalloc(c, (float4 **)&c->d_offs, S * S * S)) return r;
+    CVR_CUDA(c, cudaMemcpyAsync(c->d_offs, of.data(), of.size() * sizeof(float4), cudaMemcpyHostToDevice, c->stream));
+  }
+  std::vector<double> mi(T), m(T);
+  for (int t = 0; t < T; ++t) {
+    m[t] = c->mass[t];
+    mi[t] = (c->mass[t] == 0.0) ? 0.0 : 1.0 / c->mass[t];  // atom_data.cpp:582-585
+  }
+  if (int r = dalloc(c, &c->d_mass_inv, T)) return r;
+  if (int r = dalloc(c, &c->d_mass, T)) return r;
+  if (int r = dalloc(c, &c->d_charge, T)) return r;
+  CVR_CUDA(c, cudaMemcpyAsync(c->d_mass_inv, mi.data(), T * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CVR_CUDA(c, cudaMemcpyAsync(c->d_mass, m.data(), T * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CVR_CUDA(c, cudaMemcpyAsync(c->d_charge, c->charge.data(), T * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  return CVR_OK;
+}
+
+// k-vectors of the reference (initialize.cpp:184-222): kx, ky, kz nested over
+// [-kmax, kmax], zero skipped, f_k = exp(-k^2/(4 alpha^2)) / k^2; only the
+// first (2kx)(2ky)(2kz) are used.
+int setup_kspace(cvr_ctx *c) {
+  c->kint.clear();
+  c->fk.clear();
+  c->runs.clear();
+  if (!c->ewk_on) {
+    c->nk = 0;
+    return CVR_OK;
+  }
+  const double two_pi = 6.28318530717958647692;
+  const double lx_inv = 1.0 / c->L[0], ly_inv = 1.0 / c->L[1], lz_inv = 1.0 / c->L[2];
+  const double alpha_sq = c->ewk_alpha * c->ewk_alpha;
+  const double four_alpha2_inv = 1.0 / (4.0 * alpha_sq);
+  const int64_t used = (int64_t)(2 * c->kmax[0]) * (2 * c->kmax[1]) * (2 * c->kmax[2]);
+  for (int a = -c->kmax[0]; a <= c->kmax[0]; ++a)
+    for (int b = -c->kmax[1]; b <= c->kmax[1]; ++b)
+      for (int q = -c->kmax[2]; q <= c->kmax[2]; ++q) {
+        if ((int64_t)c->kint.size() >= used) break;
+        const double k0 = two_pi * a * lx_inv, k1 = two_pi * b * ly_inv, k2 = two_pi * q * lz_inv;
+        const double ksq = k0 * k0 + k1 * k1 + k2 * k2;
+        if (ksq == 0) continue;
+        c->kint.push_back(make_int4(a, b, q, 0));
+        c->fk.push_back((1.0 / ksq) * std::exp(-ksq * four_alpha2_inv));
+      }
+  c->nk = (int)c->kint.size();
+  for (int k = 0; k < c->nk; ++k) {
+    const int4 v = c->kint[k];
+    if (!c->runs.empty()) {
+      KRun &r = c->runs.back();
+      if (r.nx == v.x && r.ny == v.y && r.nz0 + r.len == v.z) {
+        r.len++;
+        continue;
+      }
+    }
+    c->runs.push_back(KRun{v.x, v.y, v.z, 1, k});
+  }
+  c->nruns = (int)c->runs.size();
+  c->kp = std::max(c->kmax[0], std::max(c->kmax[1], c->kmax[2])) + 1;
+  if (int r = dalloc(c, &c->d_kint, c->nk)) return r;
+  if (int r = dalloc(c, &c->d_fk, c->nk)) return r;
+  if (int r = dalloc(c, &c->d_runs, c->nruns)) return r;
+  if (int r = dalloc(c, &c->d_sk, c->nk)) return r;
+  if (c->precision == CVR_PREC_FP64) {
+    if (int r = dalloc(c, (double2 **)&c->d_ak, c->nk)) return r;
+  } else {
+    if (int r = dalloc(c, (float2 **)&c->d_ak, c->nk)) return r;
+  }
+  CVR_CUDA(c, cudaMemcpyAsync(c->d_kint, c->kint.data(), c->nk * sizeof(int4), cudaMemcpyHostToDevice, c->stream));
+  CVR_CUDA(c, cudaMemcpyAsync(c->d_fk, c->fk.data(), c->nk * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CVR_CUDA(c, cudaMemcpyAsync(c->d_runs, c->runs.data(), c->nruns * sizeof(KRun), cudaMemcpyHostToDevice, c->stream));
+  c->n_ek_blocks = grid_for(c->nk, 256);
+  if (int r = dalloc(c, &c->ek_part, c->n_ek_blocks)) return r;
+  return CVR_OK;
+}
+
+int alloc_atoms(cvr_ctx *c, int64_t n) {
+  const bool dbl = c->precision == CVR_PREC_FP64;
+  const size_t rs = dbl ? 8 : 4;
+  c->n = n;
+  c->n_pad = (int)((n + 31) / 32 * 32);
+  int r = 0;
+#define A(ptr, cnt) \
+  if ((r = dalloc(c, &c->ptr, (cnt)))) return r;
+  A(x, n) A(y, n) A(z, n) A(vx, n) A(vy, n) A(vz, n);
+  A(tx, n) A(ty, n) A(tz, n) A(tvx, n) A(tvy, n) A(tvz, n);
+  A(xb, n) A(cell, n) A(id, n) A(type, n) A(mol, n) A(gcls, n);
+  A(tid, n) A(ttype, n) A(tmol, n) A(tcell, n) A(slot_atom, n) A(perm, n);
+  A(ncount, n) A(stage, 6 * n) A(stage_i, 2 * n);
+#undef A
+  if ((r = dalloc(c, (unsigned char **)&c->ax, n * rs))) return r;
+  if ((r = dalloc(c, (unsigned char **)&c->ay, n * rs))) return r;
+  if ((r = dalloc(c, (unsigned char **)&c->az, n * rs))) return r;
+  if ((r = dalloc(c, (unsigned char **)&c->x4, n * 4 * rs))) return r;
+  // per-atom arrays that a replay after a list overflow restores
+  c->snap_pairs.clear();
+  c->snap_bytes.clear();
+  auto add = [&](void *p, size_t b) {
+    c->snap_pairs.emplace_back(p, nullptr);
+    c->snap_bytes.push_back(b);
+  };
+  add(c->x, n * 8); add(c->y, n * 8); add(c->z, n * 8);
+  add(c->vx, n * 8); add(c->vy, n * 8); add(c->vz, n * 8);
+  add(c->ax, n * rs); add(c->ay, n * rs); add(c->az, n * rs);
+  add(c->x4, n * 4 * rs); add(c->xb, n * 16); add(c->cell, n * 4); add(c->id, n * 4);
+  add(c->type, n * 4); add(c->mol, n * 4); add(c->gcls, n);
+  // partial-sum buffers
+  c->n_ke_blocks = grid_for(n, 256);
+  if ((r = dalloc(c, &c->ke_part, (size_t)c->n_ke_blocks * 4))) return r;
+  return CVR_OK;
+}
+
+int alloc_cells(cvr_ctx *c) {
+  int r;
+  if ((r = dalloc(c, &c->cell_count, c->ncells + 1))) return r;
+  if ((r = dalloc(c, &c->cell_start, c->ncells + 1))) return r;
+  if ((r = dalloc(c, &c->cell_fill, c->ncells + 1))) return r;
+  if ((r = dalloc(c, &c->block_sums, grid_for(c->ncells, 1024) + 1))) return r;
+  return CVR_OK;
+}
+
+int alloc_list(cvr_ctx *c, int cap) {
+  c->cap = (cap + c->tpa - 1) / c->tpa * c->tpa;
+  const size_t entries = (size_t)c->cap * c->n_pad;
+  int r;
+  if ((r = dalloc(c, &c->nlist, entries))) return r;
+  c->nlist_bytes = entries * 4;
+  const int blocks = grid_for(c->n * c->tpa, 128);
+  c->n_ev_blocks = blocks;
+  if ((r = dalloc(c, &c->ev_part, (size_t)blocks * 3))) return r;
+  return CVR_OK;
+}
+
+// ------------------------------------------------------------- launches
+template <typename real>
+void launch_build(cvr_ctx *c, int count_only) {
+  Bracket br(c, CVR_KT_BUILD);
+  DevState<real> s = dev_state<real>(c);
+  const int n = (int)c->n;
+  const int nb_scan = grid_for(c->ncells, 1024);
+  k_bin_count<real><<<grid_for(n, 256), 256, 0, c->stream>>>(s);
+  k_scan_local<<<nb_scan, 1024, 0, c->stream>>>(s.flag, c->cell_count, c->cell_start, c->block_sums, c->ncells);
+  k_scan_sums<<<1, 1024, 0, c->stream>>>(s.flag, c->block_sums, nb_scan, c->cell_start + c->ncells);
+  k_scan_add<<<nb_scan, 1024, 0, c->stream>>>(s.flag, c->cell_start, c->block_sums, c->ncells);
+  k_bin_scatter<real><<<grid_for(n, 256), 256, 0, c->stream>>>(s);
+  k_rank<real><<<grid_for(n, 256), 256, 0, c->stream>>>(s);
+  k_permute<real><<<grid_for(std::max<int64_t>(n, c->ncells), 256), 256, 0, c->stream>>>(s);
+  k_build_list<real><<<grid_for(n, 128), 128, 0, c->stream>>>(s, count_only, c->log2_tpa);
+  c->launches += 8;
+}
+
+template <typename real, int TPA, bool LJ, bool EWR, bool EV>
+void launch_pair_t(cvr_ctx *c) {
+  DevState<real> s = dev_state<real>(c);
+  EwrArgs<real> ew;
+  ew.alpha = (real)c->ewr_alpha;
+  ew.alpha2 = (real)(c->ewr_alpha * c->ewr_alpha);
+  ew.two_alpha_spi = (real)(2.0 * c->ewr_alpha * 0.56418958354775628695);  // 2 alpha / sqrt(pi)
+  ew.cut2 = (real)(c->ewr_cut >= 0 ? c->ewr_cut * c->ewr_cut : -1.0);
+  const int blocks = grid_for(c->n * TPA, 128);
+  k_pair<real, TPA, LJ, EWR, EV><<<blocks, 128, 0, c->stream>>>(
+      s, (const PairCoef<real> *)c->d_coef, (const typename V4<real>::t *)c->d_offs, ew, c->ignore_intra,
+      c->use_mol ? 1 : 0, c->ev_part);
+  c->launches++;
+}
+
+template <typename real, bool LJ, bool EWR, bool EV>
+void launch_pair_tpa(cvr_ctx *c) {
+  switch (c->tpa) {
+    case 1: launch_pair_t<real, 1, LJ, EWR, EV>(c); break;
+    case 8: launch_pair_t<real, 8, LJ, EWR, EV>(c); break;
+    default: launch_pair_t<real, 32, LJ, EWR, EV>(c); break;
+  }
+}
+
+template <typename real>
+void launch_pair(cvr_ctx *c, bool ev) {
+  Bracket br(c, CVR_KT_PAIR);
+  if (c->lj_on && c->ewr_on) {
+    ev ? launch_pair_tpa<real, true, true, true>(c) : launch_pair_tpa<real, true, true, false>(c);
+  } else if (c->lj_on) {
+    ev ? launch_pair_tpa<real, true, false, true>(c) : launch_pair_tpa<real, true, false, false>(c);
+  } else if (c->ewr_on) {
+    ev ? launch_pair_tpa<real, false, true, true>(c) : launch_pair_tpa<real, false, true, false>(c);
+  } else {
+    // no pair force field: accelerations start from zero
+    const size_t rs = sizeof(real);
+    cudaMemsetAsync(c->ax, 0, c->n * rs, c->stream);
+    cudaMemsetAsync(c->ay, 0, c->n * rs, c->stream);
+    cudaMemsetAsync(c->az, 0, c->n * rs, c->stream);
+    if (ev) cudaMemsetAsync(c->ev_part, 0, (size_t)c->n_ev_blocks * 3 * sizeof(double), c->stream);
+  }
+}
+
+template <typename real>
+KArgs<real> kargs(cvr_ctx *c) {
+  KArgs<real> a{};
+  a.nk = c->nk;
+  a.nruns = c->nruns;
+  for (int d = 0; d < 3; ++d) {
+    a.kmax[d] = c->kmax[d];
+    a.inv_L[d] = 1.0 / c->L[d];
+    a.two_pi_over_L[d] = (real)(6.28318530717958647692 / c->L[d]);
+  }
+  a.kp = c->kp;
+  a.kint = c->d_kint;
+  a.fk = c->d_fk;
+  a.runs = c->d_runs;
+  a.partial = c->d_kpartial;
+  a.sk = c->d_sk;
+  a.ak = (typename R2<real>::t *)c->d_ak;
+  a.e_partials = c->ek_part;
+  a.four_pi_over_v = 12.56637061435917295384 / (c->L[0] * c->L[1] * c->L[2]);
+  a.charge = c->d_charge;
+  a.k_e = c->ewk_ke;
+  a.nchunks = c->nchunks;
+  return a;
+}
+
+template <typename real>
+int launch_kspace(cvr_ctx *c) {
+  if (!c->ewk_on || c->nk == 0) return CVR_OK;
+  Bracket br(c, CVR_KT_KSPACE);
+  using c2 = typename R2<real>::t;
+  DevState<real> s = dev_state<real>(c);
+  KArgs<real> a = kargs<real>(c);
+  const size_t sm1 = (size_t)KCH * 3 * c->kp * sizeof(c2) + KCH * sizeof(real);
+  dim3 g1(grid_for(c->nk, 256), c->nchunks);
+  k_sk_partial<real, KCH><<<g1, 256, sm1, c->stream>>>(s, a);
+  k_sk_reduce<real><<<c->n_ek_blocks, 256, 0, c->stream>>>(s, a);
+  int tb = 128;
+  while (tb > 32 && (size_t)tb * 3 * c->kp * sizeof(c2) > 96 * 1024) tb /= 2;
+  const size_t sm3 = (size_t)tb * 3 * c->kp * sizeof(c2);
+  k_kforce<real><<<grid_for(c->n, tb), tb, sm3, c->stream>>>(s, a);
+  c->launches += 3;
+  return CVR_OK;
+}
+
+template <typename real>
+void set_smem_attrs(cvr_ctx *c) {
+  using c2 = typename R2<real>::t;
+  const size_t sm1 = (size_t)KCH * 3 * c->kp * sizeof(c2) + KCH * sizeof(real);
+  cudaFuncSetAttribute(k_sk_partial<real, KCH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(sm1, 48 * 1024));
+  cudaFuncSetAttribute(k_kforce<real>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024 + 1024);
+}
+
+template <typename real>
+void launch_thermo(cvr_ctx *c, double *out, double step) {
+  ThermoArgs t{};
+  t.ke_part = c->ke_part;
+  t.n_ke = c->n_ke_blocks;
+  t.ev_part = c->ev_part;
+  t.n_ev = c->n_ev_blocks;
+  t.ek_part = c->ek_part;
+  t.n_ek = (c->ewk_on && c->nk > 0) ? c->n_ek_blocks : 0;
+  t.volume = c->L[0] * c->L[1] * c->L[2];
+  t.k_b = c->k_b;
+  t.n_atoms = (double)c->n;
+  t.ek_coef = 2.0 * 3.14159265358979323846 * c->ewk_ke / t.volume;  // (2 pi / V) k_e sum f_k |S_k|^2
+  t.e_self = c->e_self;
+  const int bcsum = c->bc[0] + c->bc[1] + c->bc[2];
+  const int n_r_df = (bcsum == 0) ? 6 : (bcsum == 3 ? 3 : 6 - bcsum);  // atom_data.cpp:322-349
+  t.com_removed = (n_r_df >= 1 && n_r_df <= 3) ? 1 : 0;
+  t.dof = 3.0 * (double)c->n - n_r_df;
+  t.total_mass = c->total_mass;
+  t.n_builds = c->flags + 3;
+  t.step = step;
+  t.out = out;
+  k_thermo<<<1, 256, 0, c->stream>>>(t);
+  c->launches++;
+}
+
+template <typename real>
+int do_build(cvr_ctx *c, bool force) {
+  DevState<real> s = dev_state<real>(c);
+  if (force) {
+    const int one = 1;
+    CVR_CUDA(c, cudaMemcpyAsync(c->flags, &one, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  }
+  if (c->cap == 0) {
+    // size the list: count pass, then allocate
+    CVR_CUDA(c, cudaMemsetAsync(c->flags + 2, 0, sizeof(int), c->stream));
+    launch_build<real>(c, 1);
+    int mc = 0;
+    CVR_CUDA(c, cudaMemcpyAsync(&mc, c->flags + 2, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CVR_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (int r = alloc_list(c, std::max(8, (int)std::ceil(mc * 1.3) + 8))) return r;
+    const int one = 1;
+    CVR_CUDA(c, cudaMemcpyAsync(c->flags, &one, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  }
+  CVR_CUDA(c, cudaMemsetAsync(c->flags + 2, 0, sizeof(int), c->stream));
+  launch_build<real>(c, 0);
+  return CVR_OK;
+}
+
+int read_flags(cvr_ctx *c, int out[4]) {
+  CVR_CUDA(c, cudaMemcpyAsync(out, c->flags, 4 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CVR_CUDA(c, cudaStreamSynchronize(c->stream));
+  return CVR_OK;
+}
+
+template <typename real>
+int forces_now(cvr_ctx *c, bool ev) {
+  launch_pair<real>(c, ev);
+  if (int r = launch_kspace<real>(c)) return r;
+  return CVR_OK;
+}
+
+template <typename real>
+int setup_run(cvr_ctx *c) {
+  if (int r = do_build<real>(c, true)) return r;
+  CVR_CUDA(c, cudaMemsetAsync(c->flags, 0, sizeof(int), c->stream));
+  if (int r = forces_now<real>(c, false)) return r;
+  int f[4];
+  if (int r = read_flags(c, f)) return r;
+  if (f[1] & ERR_OVERFLOW) return fail(c, CVR_ERR_CAPACITY, "neighbour list overflow at setup");
+  c->list_valid = true;
+  c->setup_done = true;
+  return CVR_OK;
+}
+
+// Grow the list after an overflow: capacity from the largest count seen.
+int regrow(cvr_ctx *c) {
+  int f[4];
+  if (int r = read_flags(c, f)) return r;
+  const int want = std::max(c->cap * 5 / 4, (int)std::ceil(f[2] * 1.3) + 8);
+  if (int r = alloc_list(c, want)) return r;
+  const int zero = 0;
+  CVR_CUDA(c, cudaMemcpyAsync(c->flags + 1, &zero, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  return CVR_OK;
+}
+
+int snapshot(cvr_ctx *c, bool restore) {
+  for (size_t k = 0; k < c->snap_pairs.size(); ++k) {
+    auto &p = c->snap_pairs[k];
+    if (!p.second) {
+      void *q = nullptr;
+      cudaError_t e = cudaMalloc(&q, c->snap_bytes[k]);
+      if (e != cudaSuccess) return fail(c, CVR_ERR_NOMEM, "snapshot allocation failed");
+      c->all_allocs.push_back(q);
+      p.second = q;
+    }
+    if (restore)
+      CVR_CUDA(c, cudaMemcpyAsync(p.first, p.second, c->snap_bytes[k], cudaMemcpyDeviceToDevice, c->stream));
+    else
+      CVR_CUDA(c, cudaMemcpyAsync(p.second, p.first, c->snap_bytes[k], cudaMemcpyDeviceToDevice, c->stream));
+  }
+  return CVR_OK;
+}
+
+template <typename real>
+int run_impl(cvr_ctx *c, int64_t nsteps, int64_t every, double *thermo) {
+  if (!c->setup_done)
+    if (int r = setup_run<real>(c)) return r;
+  const int64_t nrec = (every > 0) ? nsteps / every : 0;
+  if ((size_t)nrec > c->thermo_cap) {
+    if (int r = dalloc(c, &c->d_thermo, (size_t)std::max<int64_t>(nrec, 1) * CVR_N_THERMO)) return r;
+    c->thermo_cap = (size_t)nrec;
+  }
+  if (int r = snapshot(c, false)) return r;
+  int f0[4];
+  if (int r = read_flags(c, f0)) return r;
+  const int64_t step0 = c->step;
+  for (int attempt = 0; attempt < 4; ++attempt) {
+    DevState<real> s = dev_state<real>(c);
+    const int nb = grid_for(c->n, 256);
+    int64_t rec = 0;
+    for (int64_t k = 0; k < nsteps; ++k) {
+      const bool th = every > 0 && ((k + 1) % every == 0);
+      {
+        Bracket br(c, CVR_KT_INTEGRATE);
+        k_kick_drift<real><<<nb, 256, 0, c->stream>>>(s, c->dt);
+      }
+      c->launches++;
+      launch_build<real>(c, 0);
+      if (int r = forces_now<real>(c, th)) return r;
+      {
+        Bracket br(c, CVR_KT_INTEGRATE);
+        if (th)
+          k_kick<real, true><<<nb, 256, 0, c->stream>>>(s, c->dt, c->ke_part);
+        else
+          k_kick<real, false><<<nb, 256, 0, c->stream>>>(s, c->dt, c->ke_part);
+      }
+      c->launches++;
+      if (th) {
+        launch_thermo<real>(c, c->d_thermo + rec * CVR_N_THERMO, (double)(step0 + k + 1));
+        ++rec;
+      }
+    }
+    int f[4];
+    if (int r = read_flags(c, f)) return r;
+    collect_timing(c);
+    if (f[1] & ERR_NAN) return fail(c, CVR_ERR_NAN, "NaN acceleration");
+    if (f[1] & ERR_OVERFLOW) {
+      // replay the call from the snapshot with a larger list
+      if (int r = snapshot(c, true)) return r;
+      if (int r = regrow(c)) return r;
+      CVR_CUDA(c, cudaMemcpyAsync(c->flags + 3, &f0[3], sizeof(int), cudaMemcpyHostToDevice, c->stream));
+      if (int r = do_build<real>(c, true)) return r;
+      CVR_CUDA(c, cudaMemsetAsync(c->flags, 0, sizeof(int), c->stream));
+      if (int r = forces_now<real>(c, false)) return r;
+      continue;
+    }
+    c->step = step0 + nsteps;
+    if (nrec > 0) {
+      if (thermo)
+        CVR_CUDA(c, cudaMemcpyAsync(thermo, c->d_thermo, (size_t)nrec * CVR_N_THERMO * sizeof(double),
+                                    cudaMemcpyDeviceToHost, c->stream));
+      CVR_CUDA(c, cudaMemcpyAsync(c->last_thermo, c->d_thermo + (nrec - 1) * CVR_N_THERMO,
+                                  CVR_N_THERMO * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+      CVR_CUDA(c, cudaStreamSynchronize(c->stream));
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(c, CVR_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+    return CVR_OK;
+  }
+  return fail(c, CVR_ERR_CAPACITY, "neighbour list overflow persists after regrowing");
+}
+
+template <typename real>
+int compute_impl(cvr_ctx *c, double *acc, double *thermo) {
+  if (!c->list_valid) {
+    if (int r = do_build<real>(c, true)) return r;
+    CVR_CUDA(c, cudaMemsetAsync(c->flags, 0, sizeof(int), c->stream));
+    c->list_valid = true;
+  }
+  if (int r = forces_now<real>(c, true)) return r;
+  DevState<real> s = dev_state<real>(c);
+  k_ke<real><<<c->n_ke_blocks, 256, 0, c->stream>>>(s, c->ke_part);
+  c->launches++;
+  if (c->thermo_cap == 0) {
+    if (int r = dalloc(c, &c->d_thermo, CVR_N_THERMO)) return r;
+    c->thermo_cap = 1;
+  }
+  launch_thermo<real>(c, c->d_thermo, (double)c->step);
+  CVR_CUDA(c, cudaMemcpyAsync(c->last_thermo, c->d_thermo, CVR_N_THERMO * sizeof(double), cudaMemcpyDeviceToHost,
+                              c->stream));
+  if (acc) {
+    k_gather_state<real><<<grid_for(c->n, 256), 256, 0, c->stream>>>(s, nullptr, nullptr, c->stage);
+    c->launches++;
+    CVR_CUDA(c, cudaMemcpyAsync(acc, c->stage, c->n * 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  }
+  int f[4];
+  if (int r = read_flags(c, f)) return r;
+  collect_timing(c);
+  if (f[1] & ERR_OVERFLOW) {
+    if (int r = regrow(c)) return r;
+    c->list_valid = false;
+    return compute_impl<real>(c, acc, thermo);
+  }
+  if (thermo) std::memcpy(thermo, c->last_thermo, sizeof(c->last_thermo));
+  c->setup_done = true;
+  return CVR_OK;
+}
+
+}  // namespace
+
+
+// ------------------------------------------------------------------ C ABI
+namespace {
+
+int choose_tpa(int64_t n) {
+  // enough lanes to fill 148 SMs (about 6e5 threads) without starving lanes
+  if (n * 32 <= 600000) return 32;
+  if (n * 8 <= 600000) return 8;
+  return 1;
+}
+
+int ensure_ready(cvr_ctx *c) {
+  if (!c->have_state) return fail(c, CVR_ERR_STATE, "cvr_set_state has not been called");
+  if (!c->nl_set) return fail(c, CVR_ERR_STATE, "cvr_set_neighborlist has not been called");
+  return CVR_OK;
+}
+
+// Re-derive everything that depends on the settings (cells, tables, k-set).
+int refresh(cvr_ctx *c) {
+  if (!c->have_state || !c->nl_set) return CVR_OK;
+  if (int r = setup_cells(c)) return r;
+  if (int r = alloc_cells(c)) return r;
+  if (int r = upload_tables(c)) return r;
+  if (int r = setup_kspace(c)) return r;
+  if (c->ewk_on && c->nk > 0) {
+    c->nchunks = grid_for(c->n, KCH);
+    if (int r = dalloc(c, &c->d_kpartial, (size_t)c->nchunks * c->nk)) return r;
+    if (c->precision == CVR_PREC_FP64)
+      set_smem_attrs<double>(c);
+    else
+      set_smem_attrs<float>(c);
+  }
+  c->list_valid = false;
+  c->setup_done = false;
+  return CVR_OK;
+}
+
+template <typename real>
+int pairs_impl(cvr_ctx *c, std::vector<std::array<int32_t, 5>> &out) {
+  const int64_t n = c->n;
+  std::vector<int> cnt(n), ids(n), cells(n);
+  std::vector<uint32_t> lst((size_t)c->cap * c->n_pad);
+  CVR_CUDA(c, cudaMemcpyAsync(cnt.data(), c->ncount, n * 4, cudaMemcpyDeviceToHost, c->stream));
+  CVR_CUDA(c, cudaMemcpyAsync(ids.data(), c->id, n * 4, cudaMemcpyDeviceToHost, c->stream));
+  CVR_CUDA(c, cudaMemcpyAsync(cells.data(), c->cell, n * 4, cudaMemcpyDeviceToHost, c->stream));
+  CVR_CUDA(c, cudaMemcpyAsync(lst.data(), c->nlist, lst.size() * 4, cudaMemcpyDeviceToHost, c->stream));
+  CVR_CUDA(c, cudaStreamSynchronize(c->stream));
+  const int S = 2 * c->R + 1, tpa = c->tpa;
+  const size_t stride = (size_t)c->n_pad * tpa;
+  auto fdiv = [](int a, int b) { return (a >= 0) ? a / b : -((-a + b - 1) / b); };
+  out.clear();
+  out.reserve((size_t)n * 40);
+  for (int64_t k = 0; k < n; ++k) {
+    const int ck = cells[k];
+    const int cxyz[3] = {ck % c->nc[0], (ck / c->nc[0]) % c->nc[1], ck / (c->nc[0] * c->nc[1])};
+    for (int e = 0; e < cnt[k]; ++e) {
+      const uint32_t v = lst[(size_t)(e / tpa) * stride + (size_t)k * tpa + (e % tpa)];
+      const int j = (int)(v & INDEX_MASK), code = (int)(v >> CODE_SHIFT);
+      const int dd[3] = {code % S - c->R, (code / S) % S - c->R, code / (S * S) - c->R};
+      int sh[3];
+      for (int d = 0; d < 3; ++d) sh[d] = fdiv(cxyz[d] + dd[d], c->nc[d]);
+      int a = ids[k], b = ids[j];
+      bool flip = a > b;
+      if (a == b) flip = std::make_tuple(sh[0], sh[1], sh[2]) < std::make_tuple(-sh[0], -sh[1], -sh[2]);
+      if (flip) {
+        std::swap(a, b);
+        for (int d = 0; d < 3; ++d) sh[d] = -sh[d];
+      }
+      out.push_back({a, b, sh[0], sh[1], sh[2]});
+    }
+  }
+  std::sort(out.begin(), out.end());
+  out.erase(std::unique(out.begin(), out.end()), out.end());
+  return CVR_OK;
+}
+
+}  // namespace
+
+#define DISPATCH(c, fn, ...) ((c)->precision == CVR_PREC_FP64 ? fn<double>(__VA_ARGS__) : fn<float>(__VA_ARGS__))
+
+extern "C" {
+
+int cvr_create(cvr_ctx **out, const double lo[3], const double hi[3], const int bc[3], int n_types,
+               const double *mass, const double *charge, int device) {
+  if (!out) return CVR_ERR_INVALID;
+  *out = nullptr;
+  if (!lo || !hi || !bc || !mass || n_types <= 0 || n_types > MAX_TYPES) return CVR_ERR_INVALID;
+  for (int d = 0; d < 3; ++d)
+    if (!(hi[d] > lo[d]) || (bc[d] != 0 && bc[d] != 1)) return CVR_ERR_INVALID;
+  if (cudaSetDevice(device) != cudaSuccess) return CVR_ERR_CUDA;
+  cvr_ctx *c = new cvr_ctx();
+  c->device = device;
+  for (int d = 0; d < 3; ++d) {
+    c->lo[d] = lo[d];
+    c->hi[d] = hi[d];
+    c->L[d] = hi[d] - lo[d];  // size_global = upper_global - lower_global (domain.cpp:470-477)
+    c->bc[d] = bc[d];
+  }
+  c->n_types = n_types;
+  c->mass.assign(mass, mass + n_types);
+  c->charge.assign(n_types, 0.0);
+  if (charge) c->charge.assign(charge, charge + n_types);
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete c;
+    return CVR_ERR_CUDA;
+  }
+  if (dalloc(c, &c->flags, 4) != CVR_OK) {
+    cudaStreamDestroy(c->stream);
+    delete c;
+    return CVR_ERR_NOMEM;
+  }
+  *out = c;
+  return CVR_OK;
+}
+
+void cvr_destroy(cvr_ctx *c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  for (void *p : c->all_allocs) cudaFree(p);
+  for (auto &k : c->kt)
+    for (auto &e : k.ev) {
+      cudaEventDestroy(e.first);
+      cudaEventDestroy(e.second);
+    }
+  cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+int cvr_set_neighborlist(cvr_ctx *c, double cutoff, double coef, double ghost_cutoff, int policy) {
+  if (!c) return CVR_ERR_INVALID;
+  if (!(cutoff > 0)) return fail(c, CVR_ERR_INVALID, "cutoff have to non-negative.");  // neighborlist.cpp:210
+  if (!(coef >= 1.0)) return fail(c, CVR_ERR_INVALID, "cutoff_extra_coef must be larger than 1.0");
+  if (policy < 0 || policy > 2) return fail(c, CVR_ERR_INVALID, "unknown rebuild policy");
+  cudaSetDevice(c->device);
+  c->cutoff = cutoff;
+  c->coef = coef;
+  c->gc = (ghost_cutoff > 0) ? ghost_cutoff : cutoff * coef;
+  c->policy = policy;
+  c->nl_set = true;
+  return refresh(c);
+}
+
+int cvr_set_lj(cvr_ctx *c, double cutoff, const double *eps, const double *sig, const double *cutl, int ignore_intra) {
+  if (!c || !eps || !sig) return CVR_ERR_INVALID;
+  if (cutoff < 0) return fail(c, CVR_ERR_INVALID, "Force field cutoff have to non-negative.");
+  const int T = c->n_types;
+  for (int t = 0; t < T * T; ++t) {
+    if (eps[t] < 0) return fail(c, CVR_ERR_INVALID, "Epsilon have to be non-negative.");
+    if (sig[t] < 0) return fail(c, CVR_ERR_INVALID, "Sigma have to be non-negative.");
+    if (cutl && cutl[t] < 0) return fail(c, CVR_ERR_INVALID, "cutoff_list have to be non-negative.");
+  }
+  cudaSetDevice(c->device);
+  c->lj_on = true;
+  c->lj_cut = cutoff;
+  c->eps.assign(eps, eps + T * T);
+  c->sig.assign(sig, sig + T * T);
+  c->cutl.clear();
+  if (cutl) c->cutl.assign(cutl, cutl + T * T);
+  c->ignore_intra = ignore_intra ? 1 : 0;
+  return refresh(c);
+}
+
+int cvr_set_ewald_r(cvr_ctx *c, double alpha, double ke, const double *lambda, double cutoff) {
+  if (!c) return CVR_ERR_INVALID;
+  if (alpha < 0) return fail(c, CVR_ERR_INVALID, "alpha have to non-negative.");
+  if (ke < 0) return fail(c, CVR_ERR_INVALID, "k_electrostatic has to be non-negative.");
+  cudaSetDevice(c->device);
+  c->ewr_on = true;
+  c->ewr_alpha = alpha;
+  c->ewr_ke = ke;
+  c->ewr_cut = cutoff;
+  c->lam.clear();
+  if (lambda) c->lam.assign(lambda, lambda + c->n_types * c->n_types);
+  return refresh(c);
+}
+
+int cvr_set_ewald_k(cvr_ctx *c, double alpha, int kx, int ky, int kz, double ke) {
+  if (!c) return CVR_ERR_INVALID;
+  if (alpha < 0) return fail(c, CVR_ERR_INVALID, "alpha have to non-negative.");
+  if (kx < 0 || ky < 0 || kz < 0) return fail(c, CVR_ERR_INVALID, "'k_max' have to non-negative.");
+  if (kx >= MAX_KMAX || ky >= MAX_KMAX || kz >= MAX_KMAX) return fail(c, CVR_ERR_INVALID, "k_max above 30 is not supported");
+  if (ke < 0) return fail(c, CVR_ERR_INVALID, "'k_electrostatic' has to be non-negative.");
+  cudaSetDevice(c->device);
+  c->ewk_on = true;
+  c->ewk_alpha = alpha;
+  c->kmax[0] = kx;
+  c->kmax[1] = ky;
+  c->kmax[2] = kz;
+  c->ewk_ke = ke;
+  return refresh(c);
+}
+
+int cvr_set_integrator(cvr_ctx *c, double dt, double k_b) {
+  if (!c) return CVR_ERR_INVALID;
+  if (!(dt >= 0)) return fail(c, CVR_ERR_INVALID, "expected 'dt' input");
+  if (!(k_b > 0)) return fail(c, CVR_ERR_INVALID, "k_b is not set.");
+  c->dt = dt;
+  c->k_b = k_b;
+  return CVR_OK;
+}
+
+int cvr_set_precision(cvr_ctx *c, int precision) {
+  if (!c) return CVR_ERR_INVALID;
+  if (precision != CVR_PREC_MIXED && precision != CVR_PREC_FP64) return fail(c, CVR_ERR_INVALID, "unknown precision");
+  if (c->have_state && precision != c->precision)
+    return fail(c, CVR_ERR_STATE, "precision must be chosen before cvr_set_state");
+  c->precision = precision;
+  return CVR_OK;
+}
+
+int cvr_set_state(cvr_ctx *c, int64_t n, const double *pos, const double *vel, const int32_t *type,
+                  const int32_t *mol) {
+  if (!c) return CVR_ERR_INVALID;
+  if (n <= 0 || n > (int64_t)INDEX_MASK || !pos || !type) return fail(c, CVR_ERR_INVALID, "bad atom arrays");
+  for (int64_t i = 0; i < n; ++i)
+    if (type[i] < 0 || type[i] >= c->n_types) return fail(c, CVR_ERR_INVALID, "atom type out of range");
+  cudaSetDevice(c->device);
+  if (n != c->n || !c->x) {
+    if (int r = alloc_atoms(c, n)) return r;
+    if (int r = dalloc(c, &c->stage, 9 * (size_t)n)) return r;
+    c->cap = 0;
+    c->tpa = choose_tpa(n);
+    c->log2_tpa = (c->tpa == 32) ? 5 : (c->tpa == 8 ? 3 : 0);
+  }
+  CVR_CUDA(c, cudaMemcpyAsync(c->stage, pos, (size_t)n * 3 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  if (vel)
+    CVR_CUDA(c, cudaMemcpyAsync(c->stage + 3 * n, vel, (size_t)n * 3 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CVR_CUDA(c, cudaMemcpyAsync(c->stage_i, type, (size_t)n * sizeof(int32_t), cudaMemcpyHostToDevice, c->stream));
+  if (mol) CVR_CUDA(c, cudaMemcpyAsync(c->stage_i + n, mol, (size_t)n * sizeof(int32_t), cudaMemcpyHostToDevice, c->stream));
+  c->have_state = true;
+  c->use_mol = mol != nullptr;
+  double q2 = 0, mt = 0;
+  for (int64_t i = 0; i < n; ++i) {
+    q2 += c->charge[type[i]] * c->charge[type[i]];
+    mt += c->mass[type[i]];
+  }
+  c->total_mass = mt;
+  c->e_self = c->ewk_on ? -0.56418958354775628695 * c->ewk_alpha * q2 * c->ewk_ke : 0.0;  // energy.cpp:49
+  if (c->precision == CVR_PREC_FP64) {
+    DevState<double> s = dev_state<double>(c);
+    k_scatter_state<double><<<grid_for(n, 256), 256, 0, c->stream>>>(s, c->stage, vel ? c->stage + 3 * n : nullptr,
+                                                                      c->stage_i, mol ? c->stage_i + n : nullptr);
+  } else {
+    DevState<float> s = dev_state<float>(c);
+    k_scatter_state<float><<<grid_for(n, 256), 256, 0, c->stream>>>(s, c->stage, vel ? c->stage + 3 * n : nullptr,
+                                                                    c->stage_i, mol ? c->stage_i + n : nullptr);
+  }
+  c->launches++;
+  CVR_CUDA(c, cudaMemsetAsync(c->flags, 0, 4 * sizeof(int), c->stream));
+  c->step = 0;
+  if (int r = refresh(c)) return r;
+  // e_self depends on the k-space settings; recompute after refresh
+  c->e_self = c->ewk_on ? -0.56418958354775628695 * c->ewk_alpha * q2 * c->ewk_ke : 0.0;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(c, CVR_ERR_CUDA, cudaGetErrorString(e));
+  return CVR_OK;
+}
+
+int cvr_build_neighbors(cvr_ctx *c, int force, int *rebuilt) {
+  if (!c) return CVR_ERR_INVALID;
+  if (int r = ensure_ready(c)) return r;
+  cudaSetDevice(c->device);
+  int f0[4];
+  if (int r = read_flags(c, f0)) return r;
+  if (force || !c->list_valid) {
+    if (int r = DISPATCH(c, do_build, c, true)) return r;
+  } else {
+    if (c->precision == CVR_PREC_FP64) {
+      k_check<double><<<grid_for(c->n, 256), 256, 0, c->stream>>>(dev_state<double>(c));
+    } else {
+      k_check<float><<<grid_for(c->n, 256), 256, 0, c->stream>>>(dev_state<float>(c));
+    }
+    c->launches++;
+    if (int r = DISPATCH(c, do_build, c, false)) return r;
+  }
+  CVR_CUDA(c, cudaMemsetAsync(c->flags, 0, sizeof(int), c->stream));
+  int f[4];
+  if (int r = read_flags(c, f)) return r;
+  collect_timing(c);
+  if (f[1] & ERR_OVERFLOW) {
+    if (int r = regrow(c)) return r;
+    if (int r = DISPATCH(c, do_build, c, true)) return r;
+    CVR_CUDA(c, cudaMemsetAsync(c->flags, 0, sizeof(int), c->stream));
+    if (int r = read_flags(c, f)) return r;
+    if (f[1] & ERR_OVERFLOW) return fail(c, CVR_ERR_CAPACITY, "neighbour list overflow");
+  }
+  c->list_valid = true;
+  if (rebuilt) *rebuilt = (f[3] != f0[3]) ? 1 : 0;
+  return CVR_OK;
+}
+
+int cvr_compute_forces(cvr_ctx *c, double *acc, double *thermo) {
+  if (!c) return CVR_ERR_INVALID;
+  if (int r = ensure_ready(c)) return r;
+  cudaSetDevice(c->device);
+  return DISPATCH(c, compute_impl, c, acc, thermo);
+}
+
+int cvr_run(cvr_ctx *c, int64_t nsteps, int64_t every, double *thermo) {
+  if (!c) return CVR_ERR_INVALID;
+  if (nsteps < 0 || every < 0) return fail(c, CVR_ERR_INVALID, "negative step count");
+  if (int r = ensure_ready(c)) return r;
+  cudaSetDevice(c->device);
+  return DISPATCH(c, run_impl, c, nsteps, every, thermo);
+}
+
+int cvr_get_state(cvr_ctx *c, double *pos, double *vel, double *acc) {
+  if (!c) return CVR_ERR_INVALID;
+  if (!c->have_state) return fail(c, CVR_ERR_STATE, "no state");
+  cudaSetDevice(c->device);
+  const int64_t n = c->n;
+  double *dp = c->stage, *dv = c->stage + 3 * n, *da = c->stage + 6 * n;
+  if (c->precision == CVR_PREC_FP64)
+    k_gather_state<double><<<grid_for(n, 256), 256, 0, c->stream>>>(dev_state<double>(c), dp, dv, da);
+  else
+    k_gather_state<float><<<grid_for(n, 256), 256, 0, c->stream>>>(dev_state<float>(c), dp, dv, da);
+  c->launches++;
+  if (pos) CVR_CUDA(c, cudaMemcpyAsync(pos, dp, n * 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  if (vel) CVR_CUDA(c, cudaMemcpyAsync(vel, dv, n * 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  if (acc) CVR_CUDA(c, cudaMemcpyAsync(acc, da, n * 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CVR_CUDA(c, cudaStreamSynchronize(c->stream));
+  return CVR_OK;
+}
+
+int64_t cvr_get_pairs(cvr_ctx *c, int32_t *out) {
+  if (!c) return -CVR_ERR_INVALID;
+  if (!c->list_valid || c->cap == 0) return -fail(c, CVR_ERR_STATE, "no neighbour list");
+  cudaSetDevice(c->device);
+  std::vector<std::array<int32_t, 5>> p;
+  int r = DISPATCH(c, pairs_impl, c, p);
+  if (r) return -r;
+  if (out) std::memcpy(out, p.data(), p.size() * sizeof(p[0]));
+  return (int64_t)p.size();
+}
+
+int64_t cvr_get_sk(cvr_ctx *c, double *out) {
+  if (!c) return -CVR_ERR_INVALID;
+  if (!c->ewk_on) return 0;
+  cudaSetDevice(c->device);
+  if (out) {
+    cudaError_t e = cudaMemcpyAsync(out, c->d_sk, (size_t)c->nk * sizeof(double2), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return -fail(c, CVR_ERR_CUDA, cudaGetErrorString(e));
+  }
+  return c->nk;
+}
+
+int cvr_get_scalars(cvr_ctx *c, double *thermo) {
+  if (!c || !thermo) return CVR_ERR_INVALID;
+  std::memcpy(thermo, c->last_thermo, sizeof(c->last_thermo));
+  return CVR_OK;
+}
+
+int cvr_last_error(const cvr_ctx *c, char *buf, size_t len) {
+  if (!c || !buf || len == 0) return CVR_ERR_INVALID;
+  std::snprintf(buf, len, "%s", c->err.c_str());
+  return CVR_OK;
+}
+
+int64_t cvr_launch_count(const cvr_ctx *c) { return c ? c->launches : -1; }
+
+void *cvr_get_stream(const cvr_ctx *c) { return c ? (void *)c->stream : nullptr; }
+
+int cvr_get_info(const cvr_ctx *c, int64_t *out, int len) {
+  if (!c || !out) return CVR_ERR_INVALID;
+  int flags[4] = {0, 0, 0, 0};
+  if (c->flags) {
+    cudaMemcpyAsync(flags, c->flags, sizeof(flags), cudaMemcpyDeviceToHost, c->stream);
+    cudaStreamSynchronize(c->stream);
+  }
+  const int64_t v[12] = {c->n, c->nc[0], c->nc[1], c->nc[2], c->cap, flags[3], c->tpa, c->nk, c->R, flags[2],
+                         flags[1], c->step};
+  for (int k = 0; k < len && k < 12; ++k) out[k] = v[k];
+  return CVR_OK;
+}
+
+int cvr_set_kernel_timing(cvr_ctx *c, int on) {
+  if (!c) return CVR_ERR_INVALID;
+  collect_timing(c);
+  c->timing = on != 0;
+  for (auto &k : c->kt) {
+    k.ms = 0;
+    k.launches = 0;
+  }
+  return CVR_OK;
+}
+
+int cvr_kernel_time(cvr_ctx *c, int kind, double *ms, int64_t *launches) {
+  if (!c || kind < 0 || kind >= CVR_N_KT) return CVR_ERR_INVALID;
+  collect_timing(c);
+  if (ms) *ms = c->kt[kind].ms;
+  if (launches) *launches = c->kt[kind].launches;
+  return CVR_OK;
+}
+
+}  // extern "C"

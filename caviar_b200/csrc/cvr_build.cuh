@@ -1,0 +1,338 @@
+// cvr_build.cuh -- Verlet-list build on sm_100a: PBC wrap, cell binning,
+// cell-ordered re-layout, and the pair search.
+//
+// Replaces, in the reference (CAVIAR; paths relative to its project root):
+//   Domain::fix_position                      src/caviar/objects/domain.cpp:418-468
+//   exchange_ghost_single_md_domain           src/caviar/objects/atom_data/exchange_ghost_single_md_domain.cpp:26-218
+//   Neighborlist::update_cell_list            src/caviar/objects/neighborlist.cpp:439-472
+//   Neighborlist::update_verlet_list_from_cell_list  neighborlist.cpp:515-573
+//
+// The reference materialises ghost copies of atoms near the faces and bins
+// owned + ghost atoms into cells of width rl.  Here no ghost is stored: an
+// image is (atom j, stencil offset d), and the list entry records d.  The
+// PAIR SET is nevertheless the reference's exactly: a pair (i, j, image s)
+// is listed iff the reference would list it from either end -- the image of
+// j exists as a reference ghost (ghost zones with the reference's
+// lower-zone-first rule) and |r_i - ghost_j|^2 < rl^2 in the reference's own
+// FP64 operation order, or the same with i and j swapped.  An FP32 prefilter
+// on cell-local coordinates decides every candidate that is more than a
+// 1e-5 relative guard band away from rl^2; the rest take the exact FP64 test.
+//
+// Every build kernel returns at once unless the step's rebuild flag is set,
+// so the whole sequence can sit in every step of a stream or graph.
+#pragma once
+#include "cvr_device.cuh"
+
+namespace cvr {
+
+__device__ __forceinline__ int ghost_val(double x, double gclo, double gchi, int bc) {
+  // exchange_ghost_single_md_domain.cpp:59-99: lower zone first, else upper, times bc
+  const int v = (x < gclo) ? -1 : ((x > gchi) ? 1 : 0);
+  return v * bc;
+}
+
+__device__ __forceinline__ int floor_div(int a, int b) {
+  const int q = a / b;
+  return (a % b != 0 && ((a < 0) != (b < 0))) ? q - 1 : q;
+}
+
+template <typename real>
+__device__ __forceinline__ void cell_xyz(const DevState<real> &s, int c, int &cx, int &cy, int &cz) {
+  cx = c % s.cells.nc[0];
+  const int t = c / s.cells.nc[0];
+  cy = t % s.cells.nc[1];
+  cz = t / s.cells.nc[1];
+}
+
+// Pass 1: wrap (Domain::fix_position: one if / else-if per periodic axis),
+// cell index, copy the atom to the temporaries, count atoms per cell.
+template <typename real>
+__global__ void k_bin_count(DevState<real> s) {
+  if (*s.flag == 0) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= s.n) return;
+  double p[3] = {s.x[i], s.y[i], s.z[i]};
+  int c[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    if (s.box.bc[d] == 1) {
+      if (p[d] < s.box.lo[d])
+        p[d] = __dadd_rn(p[d], s.box.L[d]);
+      else if (p[d] > s.box.hi[d])
+        p[d] = __dsub_rn(p[d], s.box.L[d]);
+    }
+    const double u = (p[d] - s.box.lo[d]) * s.cells.inv_w[d];
+    int ci = (u >= 0.0) ? (int)fmin(u, 2.0e9) : -1;  // floor for u >= 0; NaN lands in cell 0
+    ci = min(max(ci, 0), s.cells.nc[d] - 1);
+    c[d] = ci;
+  }
+  const int cell = c[0] + s.cells.nc[0] * (c[1] + s.cells.nc[1] * c[2]);
+  s.tx[i] = p[0];
+  s.ty[i] = p[1];
+  s.tz[i] = p[2];
+  s.tvx[i] = s.vx[i];
+  s.tvy[i] = s.vy[i];
+  s.tvz[i] = s.vz[i];
+  s.tid[i] = s.id[i];
+  s.ttype[i] = s.type[i];
+  s.tmol[i] = s.mol[i];
+  s.tcell[i] = cell;
+  atomicAdd(&s.cell_count[cell], 1);
+}
+
+// Exclusive scan of cell_count into cell_start, in three passes over blocks
+// of 1024 cells.  cell_start[ncells] = n.
+__device__ __forceinline__ int block_exclusive_scan_1024(int v, int *warp_tot, int &block_total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) warp_tot[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    int t = warp_tot[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, t, o);
+      if (lane >= o) t += y;
+    }
+    warp_tot[lane] = t;
+  }
+  __syncthreads();
+  block_total = warp_tot[31];
+  const int before = (warp > 0) ? warp_tot[warp - 1] : 0;
+  return before + x - v;
+}
+
+__global__ void __launch_bounds__(1024) k_scan_local(const int *__restrict__ flag, const int *__restrict__ in,
+                                                      int *__restrict__ out, int *__restrict__ block_sums, int m) {
+  if (*flag == 0) return;
+  __shared__ int wt[32];
+  const int i = blockIdx.x * 1024 + threadIdx.x;
+  const int v = (i < m) ? in[i] : 0;
+  int tot;
+  const int ex = block_exclusive_scan_1024(v, wt, tot);
+  if (i < m) out[i] = ex;
+  if (threadIdx.x == 0) block_sums[blockIdx.x] = tot;
+}
+
+__global__ void __launch_bounds__(1024) k_scan_sums(const int *__restrict__ flag, int *__restrict__ block_sums, int nb,
+                                                     int *__restrict__ total_out) {
+  if (*flag == 0) return;
+  __shared__ int wt[32];
+  __shared__ int carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (int base = 0; base < nb; base += 1024) {
+    const int i = base + threadIdx.x;
+    const int v = (i < nb) ? block_sums[i] : 0;
+    int tot;
+    const int ex = block_exclusive_scan_1024(v, wt, tot);
+    if (i < nb) block_sums[i] = ex + carry;
+    __syncthreads();
+    if (threadIdx.x == 0) carry += tot;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *total_out = carry;
+}
+
+__global__ void __launch_bounds__(1024) k_scan_add(const int *__restrict__ flag, int *__restrict__ out,
+                                                    const int *__restrict__ block_sums, int m) {
+  if (*flag == 0) return;
+  const int i = blockIdx.x * 1024 + threadIdx.x;
+  if (i < m) out[i] += block_sums[blockIdx.x];
+}
+
+// Pass 2: drop each atom into its cell's range (order inside a cell is
+// fixed by k_rank below, so the atomics here do not make the result depend
+// on scheduling).
+template <typename real>
+__global__ void k_bin_scatter(DevState<real> s) {
+  if (*s.flag == 0) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= s.n) return;
+  const int c = s.tcell[i];
+  const int slot = s.cell_start[c] + atomicAdd(&s.cell_fill[c], 1);
+  s.slot_atom[slot] = i;
+}
+
+// Pass 3: inside each cell, order atoms by id (deterministic layout).
+template <typename real>
+__global__ void k_rank(DevState<real> s) {
+  if (*s.flag == 0) return;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= s.n) return;
+  const int i = s.slot_atom[t];
+  const int c = s.tcell[i];
+  const int b = s.cell_start[c], e = s.cell_start[c + 1];
+  const int key = s.tid[i];
+  int rank = 0;
+  for (int u = b; u < e; ++u) rank += (s.tid[s.slot_atom[u]] < key) ? 1 : 0;
+  s.perm[b + rank] = i;
+}
+
+// Pass 4: gather into cell order, build the cell-local coordinates and the
+// ghost-zone classification, and clear the per-cell counters for next time.
+template <typename real>
+__global__ void k_permute(DevState<real> s) {
+  if (*s.flag == 0) return;
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < s.cells.ncells) {
+    s.cell_count[k] = 0;
+    s.cell_fill[k] = 0;
+  }
+  if (k >= s.n) return;
+  const int i = s.perm[k];
+  const double p[3] = {s.tx[i], s.ty[i], s.tz[i]};
+  s.x[k] = p[0];
+  s.y[k] = p[1];
+  s.z[k] = p[2];
+  s.vx[k] = s.tvx[i];
+  s.vy[k] = s.tvy[i];
+  s.vz[k] = s.tvz[i];
+  s.id[k] = s.tid[i];
+  const int ty = s.ttype[i];
+  s.type[k] = ty;
+  s.mol[k] = s.tmol[i];
+  const int c = s.tcell[i];
+  s.cell[k] = c;
+  int cc[3];
+  cell_xyz(s, c, cc[0], cc[1], cc[2]);
+  double loc[3];
+  int code = 0, mul = 1;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const double origin = s.box.lo[d] + (cc[d] + 0.5) * s.cells.w[d];
+    loc[d] = p[d] - origin;
+    code += (ghost_val(p[d], s.box.gclo[d], s.box.gchi[d], s.box.bc[d]) + 1) * mul;
+    mul *= 3;
+  }
+  typename V4<real>::t q;
+  q.x = (real)loc[0];
+  q.y = (real)loc[1];
+  q.z = (real)loc[2];
+  if constexpr (sizeof(real) == 4)
+    q.w = __int_as_float(ty);
+  else
+    q.w = (double)ty;
+  s.x4[k] = q;
+  s.xb[k] = make_float4((float)loc[0], (float)loc[1], (float)loc[2], 0.f);
+  s.gcls[k] = (int8_t)code;
+}
+
+// |pa - image(pb, shift)|^2 < rl^2 in the reference's FP64 order:
+// ghost = pb - val*L on shifted axes (val = -shift), dr = pa - ghost,
+// dr.dr = (dx*dx + dy*dy) + dz*dz, no fused multiply-add.
+__device__ __forceinline__ bool exact_within(const double pa[3], const double pb[3], const int sh[3], const DBox &b,
+                                             double rl_sq) {
+  double dr[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const double g = sh[d] ? __dsub_rn(pb[d], __dmul_rn((double)(-sh[d]), b.L[d])) : pb[d];
+    dr[d] = __dsub_rn(pa[d], g);
+  }
+  const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(dr[0], dr[0]), __dmul_rn(dr[1], dr[1])), __dmul_rn(dr[2], dr[2]));
+  return r2 < rl_sq;
+}
+
+// Does atom a (ghost-zone code gc) have a reference ghost at image shift sh?
+__device__ __forceinline__ bool has_image(int gcode, const int sh[3]) {
+  int v[3];
+  v[0] = gcode % 3 - 1;
+  v[1] = (gcode / 3) % 3 - 1;
+  v[2] = gcode / 9 - 1;
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+    if (sh[d] != 0 && v[d] != -sh[d]) return false;
+  return true;
+}
+
+// Pass 5: the pair search, one thread per atom over the (2R+1)^3 stencil.
+// count_only = 1 only counts (used to size the list before the first build).
+template <typename real>
+__global__ void __launch_bounds__(128) k_build_list(DevState<real> s, int count_only, int log2_tpa) {
+  if (*s.flag == 0) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (blockIdx.x == 0 && threadIdx.x == 0 && !count_only) atomicAdd(s.n_builds, 1);
+  int cnt = 0;
+  if (i < s.n) {
+    int cx, cy, cz;
+    cell_xyz(s, s.cell[i], cx, cy, cz);
+    const float4 xi = s.xb[i];
+    const double pi[3] = {s.x[i], s.y[i], s.z[i]};
+    const int gi = s.gcls[i];
+    const int R = s.cells.R, S = s.cells.S;
+    const int tpa = 1 << log2_tpa;
+    const size_t stride = (size_t)s.n_pad << log2_tpa;
+    uint32_t *row = s.nlist + ((size_t)i << log2_tpa);
+    const int nc0 = s.cells.nc[0], nc1 = s.cells.nc[1], nc2 = s.cells.nc[2];
+    for (int dz = -R; dz <= R; ++dz) {
+      const int sz = floor_div(cz + dz, nc2);
+      if (sz != 0 && !s.box.bc[2]) continue;
+      const int jz = cz + dz - sz * nc2;
+      for (int dy = -R; dy <= R; ++dy) {
+        const int sy = floor_div(cy + dy, nc1);
+        if (sy != 0 && !s.box.bc[1]) continue;
+        const int jy = cy + dy - sy * nc1;
+        for (int dx = -R; dx <= R; ++dx) {
+          const int sx = floor_div(cx + dx, nc0);
+          if (sx != 0 && !s.box.bc[0]) continue;
+          const int jx = cx + dx - sx * nc0;
+          const int cj = jx + nc0 * (jy + nc1 * jz);
+          const uint32_t code = (uint32_t)((dx + R) + S * ((dy + R) + S * (dz + R)));
+          const float ox = dx * (float)s.cells.w[0], oy = dy * (float)s.cells.w[1], oz = dz * (float)s.cells.w[2];
+          const int sh[3] = {sx, sy, sz};
+          const bool shifted = (sx | sy | sz) != 0;
+          const int jb = s.cell_start[cj], je = s.cell_start[cj + 1];
+          for (int j = jb; j < je; ++j) {
+            if (j == i && !shifted) continue;
+            const float4 xj = s.xb[j];
+            const float ddx = (xj.x - xi.x) + ox, ddy = (xj.y - xi.y) + oy, ddz = (xj.z - xi.z) + oz;
+            const float d2 = ddx * ddx + ddy * ddy + ddz * ddz;
+            if (!(d2 < s.rl_sq_hi)) continue;
+            bool inc;
+            if (!shifted) {
+              if (d2 <= s.rl_sq_lo) {
+                inc = true;
+              } else {
+                const double pj[3] = {s.x[j], s.y[j], s.z[j]};
+                inc = exact_within(pi, pj, sh, s.box, s.rl_sq);
+              }
+            } else {
+              const int gj = s.gcls[j];
+              const int msh[3] = {-sx, -sy, -sz};
+              const bool img_j = has_image(gj, sh);   // reference ghost of j at r_j + sL
+              const bool img_i = has_image(gi, msh);  // reference ghost of i at r_i - sL
+              if (!img_j && !img_i) {
+                inc = false;
+              } else if (d2 <= s.rl_sq_lo) {
+                inc = true;
+              } else {
+                const double pj[3] = {s.x[j], s.y[j], s.z[j]};
+                inc = (img_j && exact_within(pi, pj, sh, s.box, s.rl_sq)) ||
+                      (img_i && exact_within(pj, pi, msh, s.box, s.rl_sq));
+              }
+            }
+            if (inc) {
+              if (!count_only && cnt < s.cap)
+                row[(size_t)(cnt >> log2_tpa) * stride + (cnt & (tpa - 1))] = (uint32_t)j | (code << CODE_SHIFT);
+              ++cnt;
+            }
+          }
+        }
+      }
+    }
+    if (!count_only) s.ncount[i] = min(cnt, s.cap);
+    if (!count_only && cnt > s.cap) atomicOr(s.err, ERR_OVERFLOW);
+  }
+  // largest count, one atomic per warp
+  int m = cnt;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(s.max_count, m);
+}
+
+}  // namespace cvr

@@ -1,0 +1,82 @@
+// cvr_device.cuh -- device-side state shared by the sm_100a kernels.
+//
+// HBM layout (one periodic system, atoms kept in CELL ORDER, re-sorted at each
+// Verlet-list build):
+//   x,y,z / vx,vy,vz   FP64 SoA positions (unwrapped between builds) and velocities
+//   ax,ay,az           real SoA accelerations (real = float in the mixed form, double in FP64)
+//   x4                 real4 cell-local position (r - centre of the atom's build cell) with the
+//                      type in .w: the only per-neighbour gather of the pair kernel (16 B mixed)
+//   xb                 float4 cell-local position at the last build (rebuild trigger)
+//   cell,id,type,mol   int per atom; id = the caller's atom index
+//   nlist              uint32 entries j | (stencil offset code << 25), TPA-interleaved rows:
+//                      entry k of atom i at (k/TPA)*(n_pad*TPA) + i*TPA + k%TPA
+//   ncount             neighbours per atom
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace cvr {
+
+enum : int { ERR_NAN = 1, ERR_OVERFLOW = 2, ERR_GEOMETRY = 4 };
+constexpr int CODE_SHIFT = 25;
+constexpr unsigned INDEX_MASK = (1u << CODE_SHIFT) - 1u;
+constexpr int MAX_TYPES = 16;
+constexpr int MAX_KMAX = 31;
+
+template <typename real> struct V4;
+template <> struct V4<float> { using t = float4; };
+template <> struct V4<double> { using t = double4; };
+
+struct DBox {
+  double lo[3], hi[3], L[3];
+  double gclo[3], gchi[3];  // lower + ghost_cutoff, upper - ghost_cutoff (ghost zones)
+  int bc[3];
+};
+
+struct DCells {
+  int nc[3];
+  int ncells;
+  int R;  // stencil radius in cells
+  int S;  // 2R+1
+  double w[3], inv_w[3];
+};
+
+// Per type-pair constants of the fused pair kernel.
+template <typename real> struct PairCoef {
+  real sig2, eps24, eps48, K;  // LJ: c = r2inv*s6*(eps24 - eps48*s6) + K
+  real rc2;                    // LJ cutoff^2 (lj.cpp:417-420); < 0 disables LJ for the pair
+  real qq;                     // k_e q_i q_j (Ewald real space)
+  real e4, C0, C1;             // LJ energy: e4*(s6^2 - s6) + C1*r2 + C0
+  real lam;                    // Ewald same-molecule scaling lambda (1 if unset)
+};
+
+template <typename real> struct DevState {
+  int n, n_pad, cap, tpa, policy, n_types;
+  DBox box;
+  DCells cells;
+  double rl_sq;                 // (cutoff*coef)^2, FP64 list threshold
+  float rl_sq_lo, rl_sq_hi;     // FP32 guard band around rl_sq for the prefilter
+  float thr_sq;                 // (skin/2)^2 rebuild threshold
+  double *x, *y, *z, *vx, *vy, *vz;
+  real *ax, *ay, *az;
+  typename V4<real>::t *x4;
+  float4 *xb;
+  int *cell, *id, *type, *mol;
+  int8_t *gcls;                 // ghost-zone classification at build (x_val+1)+3(y_val+1)+9(z_val+1)
+  // rebuild temporaries
+  double *tx, *ty, *tz, *tvx, *tvy, *tvz;
+  int *tid, *ttype, *tmol, *tcell;
+  int *cell_count, *cell_start, *cell_fill, *slot_atom, *perm, *block_sums;
+  // list
+  uint32_t *nlist;
+  int *ncount;
+  // device flags
+  int *flag;       // rebuild requested for this step
+  int *err;        // sticky ERR_* bits
+  int *max_count;  // largest neighbour count at the last build
+  int *n_builds;
+  double *mass_inv;  // per type (device)
+  double *mass;      // per type (device)
+};
+
+}  // namespace cvr

@@ -1,0 +1,551 @@
+// cvr_force.cuh -- force, k-space and integrator kernels (sm_100a).
+//
+// Replaces, in the reference (CAVIAR; paths relative to its project root):
+//   force_field::Lj::calculate_acceleration            src/caviar/objects/force_field/lj.cpp:355-483
+//   Electrostatic_ewald_r::calculate_acceleration      src/caviar/objects/force_field/electrostatic_ewald_r.cpp:115-317
+//   Electrostatic_ewald_k::calculate_potential_k_coef_cmplx  .../electrostatic_ewald_k/initialize.cpp:117-146
+//   Electrostatic_ewald_k::calculate_acceleration      .../electrostatic_ewald_k.cpp:161-294
+//   k_space_energy / self_energy                       .../electrostatic_ewald_k/energy.cpp:31-116
+//   Md_simulator::integrate_velocity_verlet            src/caviar/objects/md_simulator.cpp:555-668
+//   Atom_data::kinetic_energy / finalize_temperature   src/caviar/objects/atom_data/kinetic_energy.cpp:30-202
+//
+// Structure differs from the reference on purpose: the reference runs a
+// half list with Newton's third law (scatter into j), which on a GPU needs
+// atomics and gives run-to-run different sums.  Here the list is full
+// (every pair in both atoms' rows) and each atom sums its own force in a
+// fixed order: no atomics, bit-reproducible.  LJ and Ewald real space share
+// one pass over the list.  Energies and virial are FP64 block sums.
+#pragma once
+#include "cvr_device.cuh"
+
+namespace cvr {
+
+template <typename real> struct R2;
+template <> struct R2<float> { using t = float2; };
+template <> struct R2<double> { using t = double2; };
+
+__device__ __forceinline__ float fast_rcp(float x) { return __fdividef(1.0f, x); }
+__device__ __forceinline__ double fast_rcp(double x) { return 1.0 / x; }
+__device__ __forceinline__ float fast_rsqrt(float x) { return rsqrtf(x); }
+__device__ __forceinline__ double fast_rsqrt(double x) { return rsqrt(x); }
+__device__ __forceinline__ float fast_exp(float x) { return __expf(x); }
+__device__ __forceinline__ double fast_exp(double x) { return exp(x); }
+__device__ __forceinline__ float erfc_r(float x) { return erfcf(x); }
+__device__ __forceinline__ double erfc_r(double x) { return erfc(x); }
+__device__ __forceinline__ int type_of(float w) { return __float_as_int(w); }
+__device__ __forceinline__ int type_of(double w) { return (int)w; }
+__device__ __forceinline__ void sincospi_r(float a, float *s, float *c) { sincospif(a, s, c); }
+__device__ __forceinline__ void sincospi_r(double a, double *s, double *c) { sincospi(a, s, c); }
+
+// Block-wide sum of NV doubles into out[blockIdx.x * NV + q] (fixed order).
+template <int NV>
+__device__ __forceinline__ void block_sum_store(double (&v)[NV], double *out) {
+  __shared__ double red[NV][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+  for (int q = 0; q < NV; ++q) {
+    double x = v[q];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    if (lane == 0) red[q][warp] = x;
+  }
+  __syncthreads();
+  if (warp == 0) {
+#pragma unroll
+    for (int q = 0; q < NV; ++q) {
+      double x = (lane < nw) ? red[q][lane] : 0.0;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+      if (lane == 0) out[(size_t)blockIdx.x * NV + q] = x;
+    }
+  }
+}
+
+template <typename real> struct EwrArgs {
+  real alpha, alpha2, two_alpha_spi;  // alpha, alpha^2, 2 alpha / sqrt(pi)
+  real cut2;                          // < 0: no cutoff (the reference)
+};
+
+// --------------------------------------------------------------- pair force
+// TPA lanes per atom stride through the atom's list row; lanes reduce with
+// shuffles.  use_mol enables the molecule tests (ignore_intra_molecule,
+// Ewald lambda).  EV adds energies + virial (FP64 per thread, FP64 block sums into
+// partials[block*3 + {e_lj, e_ewr, virial}]).
+template <typename real, int TPA, bool LJ, bool EWR, bool EV>
+__global__ void __launch_bounds__(128) k_pair(DevState<real> s, const PairCoef<real> *__restrict__ coef_g,
+                                              const typename V4<real>::t *__restrict__ offs_g, EwrArgs<real> ew,
+                                              int ignore_intra, int use_mol, double *__restrict__ partials) {
+  using real4 = typename V4<real>::t;
+  __shared__ PairCoef<real> coef[MAX_TYPES * MAX_TYPES];
+  __shared__ real4 offs[125];
+  const int T = s.n_types;
+  for (int t = threadIdx.x; t < T * T; t += blockDim.x) coef[t] = coef_g[t];
+  for (int t = threadIdx.x; t < s.cells.S * s.cells.S * s.cells.S; t += blockDim.x) offs[t] = offs_g[t];
+  __syncthreads();
+  if (*s.err) return;
+
+  const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = gid / TPA, lane = gid % TPA;
+  const bool valid = i < s.n;
+  real fx = 0, fy = 0, fz = 0;
+  double e_lj = 0, e_ew = 0, vir = 0;
+  int ti = 0;
+  if (valid) {
+    const real4 xi = s.x4[i];
+    ti = type_of(xi.w);
+    const int moli = use_mol ? s.mol[i] : 0;
+    const int cnt = s.ncount[i];
+    const uint32_t *row = s.nlist + (size_t)i * TPA + lane;
+    const size_t stride = (size_t)s.n_pad * TPA;
+    const PairCoef<real> *ci = coef + ti * T;
+    for (int k = lane, it = 0; k < cnt; k += TPA, ++it) {
+      const uint32_t e = __ldg(row + (size_t)it * stride);
+      const int j = (int)(e & INDEX_MASK);
+      const real4 o = offs[e >> CODE_SHIFT];
+      const real4 xj = s.x4[j];
+      const real dx = (xj.x - xi.x) + o.x;
+      const real dy = (xj.y - xi.y) + o.y;
+      const real dz = (xj.z - xi.z) + o.z;
+      const real r2 = dx * dx + dy * dy + dz * dz;
+      const int tj = type_of(xj.w);
+      const PairCoef<real> &pc = ci[tj];
+      const bool same_mol = use_mol && (moli == s.mol[j]);
+      real c = 0;
+      if (LJ) {
+        // lj.cpp:417-448: skip r^2 > rc^2 (rc2 < 0 when eps = 0 or excluded)
+        if (r2 <= pc.rc2 && !(same_mol && ignore_intra)) {
+          const real r2i = fast_rcp(r2);
+          const real s2 = pc.sig2 * r2i;
+          const real s6 = s2 * s2 * s2;
+          c = r2i * s6 * (pc.eps24 - pc.eps48 * s6) + pc.K;
+          if (EV) e_lj += (double)(pc.e4 * (s6 * s6 - s6) + pc.C1 * r2 + pc.C0);
+        }
+      }
+      if (EWR) {
+        // electrostatic_ewald_r.cpp:179-198: every list pair, coincident skipped
+        if (r2 > (real)0 && (ew.cut2 < (real)0 || r2 <= ew.cut2)) {
+          const real rinv = fast_rsqrt(r2);
+          const real r = r2 * rinv;
+          const real erfcv = erfc_r(ew.alpha * r);
+          const real sv = (ew.two_alpha_spi * fast_exp(-ew.alpha2 * r2) + erfcv * rinv) * (rinv * rinv);
+          const real lam = same_mol ? pc.lam : (real)1;
+          c -= lam * pc.qq * sv;
+          if (EV) e_ew += (double)(lam * pc.qq * erfcv * rinv);
+        }
+      }
+      fx += c * dx;
+      fy += c * dy;
+      fz += c * dz;
+      if (EV) vir -= (double)(c * r2);
+    }
+  }
+#pragma unroll
+  for (int o = TPA / 2; o > 0; o >>= 1) {
+    fx += __shfl_xor_sync(0xffffffffu, fx, o);
+    fy += __shfl_xor_sync(0xffffffffu, fy, o);
+    fz += __shfl_xor_sync(0xffffffffu, fz, o);
+  }
+  if (valid && lane == 0) {
+    const real mi = (real)s.mass_inv[ti];
+    s.ax[i] = fx * mi;
+    s.ay[i] = fy * mi;
+    s.az[i] = fz * mi;
+  }
+  if (EV) {
+    double v[3] = {0.5 * e_lj, 0.5 * e_ew, 0.5 * vir};  // full list: each pair twice
+    block_sum_store<3>(v, partials);
+  }
+}
+
+// ------------------------------------------------------------------ k space
+// k-vectors of the used set in the reference's enumeration order, grouped in
+// runs of consecutive nz at fixed (nx, ny).
+struct KRun {
+  int nx, ny, nz0, len, k0;
+};
+
+template <typename real> struct KArgs {
+  int nk, nruns, kmax[3], kp;  // kp = max kmax + 1 (table row length)
+  const int4 *kint;            // (nx, ny, nz, -) per used k
+  const double *fk;            // exp(-k^2/4a^2)/k^2 per used k
+  const KRun *runs;
+  double2 *partial;            // [nchunks][nk]
+  double2 *sk;                 // S(k)
+  typename R2<real>::t *ak;    // (4 pi / V) f_k conj(S_k)
+  double *e_partials;          // per block of k_sk_reduce
+  double inv_L[3];
+  real two_pi_over_L[3];
+  double four_pi_over_v;
+  double *charge;              // per type
+  double k_e;
+  int nchunks;
+};
+
+// Phase table of one atom: e^{i 2 pi m x_d / L_d}, m = 0..kmax_d, from the
+// fractional part of m x_d / L_d in FP64 (so |x| up to the box size costs no
+// phase accuracy), then sincospi in `real`.
+template <typename real>
+__device__ __forceinline__ typename R2<real>::t phase(double x_over_L, int m) {
+  const double u = (double)m * x_over_L;
+  const double f = u - rint(u);
+  real sn, cs;
+  sincospi_r((real)(2.0 * f), &sn, &cs);
+  typename R2<real>::t r;
+  r.x = cs;
+  r.y = sn;
+  return r;
+}
+
+template <typename T>
+__device__ __forceinline__ T cmul(T a, T b) {
+  T r;
+  r.x = a.x * b.x - a.y * b.y;
+  r.y = a.x * b.y + a.y * b.x;
+  return r;
+}
+template <typename T>
+__device__ __forceinline__ T conj_if(T a, bool c) {
+  if (c) a.y = -a.y;
+  return a;
+}
+
+// S(k) partial sums: one thread per k-vector, one block row per chunk of
+// KCH atoms whose phase tables sit in shared memory.  FP64 accumulation.
+template <typename real, int KCH>
+__global__ void __launch_bounds__(256) k_sk_partial(DevState<real> s, KArgs<real> a) {
+  using c2 = typename R2<real>::t;
+  extern __shared__ unsigned char smem_raw[];
+  c2 *tab = reinterpret_cast<c2 *>(smem_raw);  // [KCH][3][kp]
+  real *q = reinterpret_cast<real *>(tab + KCH * 3 * a.kp);
+  if (*s.err) return;
+  const int chunk = blockIdx.y;
+  const int a0 = chunk * KCH;
+  const int kp = a.kp;
+  for (int t = threadIdx.x; t < KCH * 3 * kp; t += blockDim.x) {
+    const int at = t / (3 * kp), rem = t % (3 * kp), d = rem / kp, m = rem % kp;
+    const int idx = a0 + at;
+    c2 v;
+    v.x = 0;
+    v.y = 0;
+    if (idx < s.n && m <= a.kmax[d]) {
+      const double x = (d == 0) ? s.x[idx] : ((d == 1) ? s.y[idx] : s.z[idx]);
+      v = phase<real>(x * a.inv_L[d], m);
+    }
+    tab[t] = v;
+  }
+  for (int t = threadIdx.x; t < KCH; t += blockDim.x) {
+    const int idx = a0 + t;
+    q[t] = (idx < s.n) ? (real)a.charge[s.type[idx]] : (real)0;
+  }
+  __syncthreads();
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= a.nk) return;
+  const int4 kn = a.kint[k];
+  const int mx = abs(kn.x), my = abs(kn.y), mz = abs(kn.z);
+  double sr = 0, si = 0;
+  const int na = min(KCH, s.n - a0);
+  for (int t = 0; t < na; ++t) {
+    const c2 *tb = tab + t * 3 * kp;
+    const c2 px = conj_if(tb[mx], kn.x < 0);
+    const c2 py = conj_if(tb[kp + my], kn.y < 0);
+    const c2 pz = conj_if(tb[2 * kp + mz], kn.z < 0);
+    const c2 p = cmul(cmul(px, py), pz);
+    sr += (double)(q[t] * p.x);
+    si += (double)(q[t] * p.y);
+  }
+  a.partial[(size_t)chunk * a.nk + k] = make_double2(sr, si);
+}
+
+// S(k) = sum of the chunk partials in chunk order; A_k for the force; FP64
+// k-space energy partials sum_k f_k |S_k|^2.
+template <typename real>
+__global__ void __launch_bounds__(256) k_sk_reduce(DevState<real> s, KArgs<real> a) {
+  if (*s.err) return;
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  double e = 0;
+  if (k < a.nk) {
+    double sr = 0, si = 0;
+    for (int c = 0; c < a.nchunks; ++c) {
+      const double2 p = a.partial[(size_t)c * a.nk + k];
+      sr += p.x;
+      si += p.y;
+    }
+    a.sk[k] = make_double2(sr, si);
+    const double f = a.fk[k];
+    const double cf = a.four_pi_over_v * f;
+    typename R2<real>::t A;
+    A.x = (real)(cf * sr);
+    A.y = (real)(-cf * si);
+    a.ak[k] = A;
+    e = f * (sr * sr + si * si);
+  }
+  double v[1] = {e};
+  block_sum_store<1>(v, a.e_partials);
+}
+
+// k-space force: one thread per atom, its own phase table in shared memory,
+// runs of nz at fixed (nx, ny) so each k costs one complex multiply.
+// F_i = k_e q_i sum_k k Im(A_k e^{i k.r_i}) (electrostatic_ewald_k.cpp:215-218).
+template <typename real>
+__global__ void __launch_bounds__(128) k_kforce(DevState<real> s, KArgs<real> a) {
+  using c2 = typename R2<real>::t;
+  extern __shared__ unsigned char smem_raw[];
+  const int kp = a.kp;
+  c2 *tab = reinterpret_cast<c2 *>(smem_raw) + (size_t)threadIdx.x * 3 * kp;
+  if (*s.err) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= s.n) return;
+  const double pd[3] = {s.x[i], s.y[i], s.z[i]};
+  for (int d = 0; d < 3; ++d)
+    for (int m = 0; m <= a.kmax[d]; ++m) tab[d * kp + m] = phase<real>(pd[d] * a.inv_L[d], m);
+  real fx = 0, fy = 0, fz = 0;
+  for (int r = 0; r < a.nruns; ++r) {
+    const KRun run = a.runs[r];
+    const c2 pxy = cmul(conj_if(tab[abs(run.nx)], run.nx < 0), conj_if(tab[kp + abs(run.ny)], run.ny < 0));
+    real tsum = 0;
+    for (int u = 0; u < run.len; ++u) {
+      const int nz = run.nz0 + u;
+      const c2 p = cmul(pxy, conj_if(tab[2 * kp + abs(nz)], nz < 0));
+      const c2 A = a.ak[run.k0 + u];
+      const real t = A.x * p.y + A.y * p.x;
+      tsum += t;
+      fz += (real)nz * t;
+    }
+    fx += (real)run.nx * tsum;
+    fy += (real)run.ny * tsum;
+  }
+  const int ti = s.type[i];
+  const real qm = (real)(a.k_e * a.charge[ti] * s.mass_inv[ti]);
+  s.ax[i] += qm * a.two_pi_over_L[0] * fx;
+  s.ay[i] += qm * a.two_pi_over_L[1] * fy;
+  s.az[i] += qm * a.two_pi_over_L[2] * fz;
+}
+
+// ------------------------------------------------------------- integrator
+// Velocity Verlet as kick (v += dt/2 a), drift (r += dt v), force, kick:
+// algebraically the reference's r += v dt + a dt^2/2, v += dt/2 (a + a_old)
+// (md_simulator.cpp:591-616) without storing a_old.  The first half also
+// writes the cell-local coordinates for the pair kernel and raises the
+// rebuild flag (neighborlist.cpp:91-139 / md_simulator.cpp:487-502).
+template <typename real>
+__global__ void __launch_bounds__(256) k_kick_drift(DevState<real> s, double dt) {
+  if (*s.err) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  bool need = false;
+  if (i < s.n) {
+    const double a0 = (double)s.ax[i], a1 = (double)s.ay[i], a2 = (double)s.az[i];
+    if (isnan(a0) || isnan(a1) || isnan(a2)) atomicOr(s.err, ERR_NAN);  // md_simulator.cpp:584-590
+    const double h = 0.5 * dt;
+    const double v0 = s.vx[i] + h * a0, v1 = s.vy[i] + h * a1, v2 = s.vz[i] + h * a2;
+    const double p[3] = {s.x[i] + dt * v0, s.y[i] + dt * v1, s.z[i] + dt * v2};
+    s.vx[i] = v0;
+    s.vy[i] = v1;
+    s.vz[i] = v2;
+    s.x[i] = p[0];
+    s.y[i] = p[1];
+    s.z[i] = p[2];
+    int cc[3];
+    cell_xyz(s, s.cell[i], cc[0], cc[1], cc[2]);
+    double loc[3];
+    int code = 0, mul = 1;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      loc[d] = p[d] - (s.box.lo[d] + (cc[d] + 0.5) * s.cells.w[d]);
+      if (s.policy == 1) {
+        if (s.box.bc[d] == 1 && (p[d] < s.box.lo[d] || p[d] > s.box.hi[d])) need = true;  // owned wrap
+        code += (ghost_val(p[d], s.box.gclo[d], s.box.gchi[d], s.box.bc[d]) + 1) * mul;
+        mul *= 3;
+      }
+    }
+    typename V4<real>::t q = s.x4[i];
+    q.x = (real)loc[0];
+    q.y = (real)loc[1];
+    q.z = (real)loc[2];
+    s.x4[i] = q;
+    const float4 b = s.xb[i];
+    const float ex = (float)loc[0] - b.x, ey = (float)loc[1] - b.y, ez = (float)loc[2] - b.z;
+    if (ex * ex + ey * ey + ez * ez > s.thr_sq) need = true;
+    if (s.policy == 1 && code != s.gcls[i]) need = true;  // ghost set changed
+    if (s.policy == 2) need = true;
+  }
+  if (__any_sync(0xffffffffu, need) && (threadIdx.x & 31) == 0) *s.flag = 1;
+}
+
+// Second half kick; KE partials (sum m v^2, sum m v) when KE.  Also clears
+// the step's rebuild flag: every reader of it has run by now.
+template <typename real, bool KE>
+__global__ void __launch_bounds__(256) k_kick(DevState<real> s, double dt, double *__restrict__ partials) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) *s.flag = 0;
+  if (*s.err) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double v[4] = {0, 0, 0, 0};
+  if (i < s.n) {
+    const double h = 0.5 * dt;
+    const double v0 = s.vx[i] + h * (double)s.ax[i];
+    const double v1 = s.vy[i] + h * (double)s.ay[i];
+    const double v2 = s.vz[i] + h * (double)s.az[i];
+    s.vx[i] = v0;
+    s.vy[i] = v1;
+    s.vz[i] = v2;
+    if (KE) {
+      const double m = s.mass[s.type[i]];
+      v[0] = m * (v0 * v0 + v1 * v1 + v2 * v2);
+      v[1] = m * v0;
+      v[2] = m * v1;
+      v[3] = m * v2;
+    }
+  }
+  if (KE) block_sum_store<4>(v, partials);
+}
+
+// KE partials without moving anything (thermo outside the step loop).
+template <typename real>
+__global__ void __launch_bounds__(256) k_ke(DevState<real> s, double *__restrict__ partials) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double v[4] = {0, 0, 0, 0};
+  if (i < s.n) {
+    const double m = s.mass[s.type[i]];
+    const double v0 = s.vx[i], v1 = s.vy[i], v2 = s.vz[i];
+    v[0] = m * (v0 * v0 + v1 * v1 + v2 * v2);
+    v[1] = m * v0;
+    v[2] = m * v1;
+    v[3] = m * v2;
+  }
+  block_sum_store<4>(v, partials);
+}
+
+// Rebuild check outside the step loop (cvr_build_neighbors with force = 0).
+template <typename real>
+__global__ void __launch_bounds__(256) k_check(DevState<real> s) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  bool need = false;
+  if (i < s.n) {
+    int cc[3];
+    cell_xyz(s, s.cell[i], cc[0], cc[1], cc[2]);
+    const double p[3] = {s.x[i], s.y[i], s.z[i]};
+    float e[3];
+    int code = 0, mul = 1;
+    const float4 b = s.xb[i];
+    const float bb[3] = {b.x, b.y, b.z};
+    for (int d = 0; d < 3; ++d) {
+      const double loc = p[d] - (s.box.lo[d] + (cc[d] + 0.5) * s.cells.w[d]);
+      e[d] = (float)loc - bb[d];
+      if (s.policy == 1) {
+        if (s.box.bc[d] == 1 && (p[d] < s.box.lo[d] || p[d] > s.box.hi[d])) need = true;
+        code += (ghost_val(p[d], s.box.gclo[d], s.box.gchi[d], s.box.bc[d]) + 1) * mul;
+        mul *= 3;
+      }
+    }
+    if (e[0] * e[0] + e[1] * e[1] + e[2] * e[2] > s.thr_sq) need = true;
+    if (s.policy == 1 && code != s.gcls[i]) need = true;
+    if (s.policy == 2) need = true;
+  }
+  if (__any_sync(0xffffffffu, need) && (threadIdx.x & 31) == 0) *s.flag = 1;
+}
+
+// ------------------------------------------------------------------ thermo
+struct ThermoArgs {
+  const double *ke_part;
+  int n_ke;
+  const double *ev_part;
+  int n_ev;
+  const double *ek_part;
+  int n_ek;
+  double total_mass, dof, volume, k_b, n_atoms, ek_coef, e_self;
+  int com_removed;
+  const int *n_builds;
+  double step;
+  double *out;  // CVR_N_THERMO doubles
+};
+
+__global__ void __launch_bounds__(256) k_thermo(ThermoArgs a) {
+  __shared__ double acc[8][256];
+  double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  for (int b = threadIdx.x; b < a.n_ke; b += blockDim.x)
+    for (int q = 0; q < 4; ++q) v[q] += a.ke_part[(size_t)b * 4 + q];
+  for (int b = threadIdx.x; b < a.n_ev; b += blockDim.x)
+    for (int q = 0; q < 3; ++q) v[4 + q] += a.ev_part[(size_t)b * 3 + q];
+  for (int b = threadIdx.x; b < a.n_ek; b += blockDim.x) v[7] += a.ek_part[b];
+  for (int q = 0; q < 8; ++q) acc[q][threadIdx.x] = v[q];
+  __syncthreads();
+  for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+    if ((int)threadIdx.x < st)
+      for (int q = 0; q < 8; ++q) acc[q][threadIdx.x] += acc[q][threadIdx.x + st];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const double mv2 = acc[0][0];
+    double ke = 0.5 * mv2;
+    if (a.com_removed && a.total_mass > 0) {
+      const double px = acc[1][0], py = acc[2][0], pz = acc[3][0];
+      ke -= 0.5 * (px * px + py * py + pz * pz) / a.total_mass;
+    }
+    const double temp = (a.dof > 0) ? 2.0 * ke / (a.k_b * a.dof) : 0.0;
+    const double vir = acc[6][0];
+    a.out[0] = a.step;
+    a.out[1] = ke;
+    a.out[2] = temp;
+    a.out[3] = acc[4][0];
+    a.out[4] = acc[5][0];
+    a.out[5] = a.ek_coef * acc[7][0];
+    a.out[6] = a.e_self;
+    a.out[7] = vir;
+    a.out[8] = a.n_atoms * a.k_b * temp / a.volume + vir / (3.0 * a.volume);
+    a.out[9] = (double)(*a.n_builds);
+  }
+}
+
+// Gather the cell-ordered state back to id order (AoS, host layout), with
+// positions wrapped once per axis like Domain::fix_position.
+template <typename real>
+__global__ void k_gather_state(DevState<real> s, double *__restrict__ pos, double *__restrict__ vel,
+                               double *__restrict__ acc) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= s.n) return;
+  const int o = s.id[k];
+  double p[3] = {s.x[k], s.y[k], s.z[k]};
+  for (int d = 0; d < 3; ++d)
+    if (s.box.bc[d] == 1) {
+      if (p[d] < s.box.lo[d])
+        p[d] = __dadd_rn(p[d], s.box.L[d]);
+      else if (p[d] > s.box.hi[d])
+        p[d] = __dsub_rn(p[d], s.box.L[d]);
+    }
+  if (pos) {
+    pos[3 * (size_t)o] = p[0];
+    pos[3 * (size_t)o + 1] = p[1];
+    pos[3 * (size_t)o + 2] = p[2];
+  }
+  if (vel) {
+    vel[3 * (size_t)o] = s.vx[k];
+    vel[3 * (size_t)o + 1] = s.vy[k];
+    vel[3 * (size_t)o + 2] = s.vz[k];
+  }
+  if (acc) {
+    acc[3 * (size_t)o] = (double)s.ax[k];
+    acc[3 * (size_t)o + 1] = (double)s.ay[k];
+    acc[3 * (size_t)o + 2] = (double)s.az[k];
+  }
+}
+
+// Scatter the caller's AoS state (id order) into the SoA arrays.
+template <typename real>
+__global__ void k_scatter_state(DevState<real> s, const double *__restrict__ pos, const double *__restrict__ vel,
+                                const int *__restrict__ typ, const int *__restrict__ mol) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= s.n) return;
+  s.x[i] = pos[3 * (size_t)i];
+  s.y[i] = pos[3 * (size_t)i + 1];
+  s.z[i] = pos[3 * (size_t)i + 2];
+  s.vx[i] = vel ? vel[3 * (size_t)i] : 0.0;
+  s.vy[i] = vel ? vel[3 * (size_t)i + 1] : 0.0;
+  s.vz[i] = vel ? vel[3 * (size_t)i + 2] : 0.0;
+  s.type[i] = typ[i];
+  s.mol[i] = mol ? mol[i] : -1;
+  s.id[i] = i;
+  s.ax[i] = 0;
+  s.ay[i] = 0;
+  s.az[i] = 0;
+}
+
+}  // namespace cvr

@@ -101,9 +101,11 @@ def maxwell_boltzmann(n: int, temperature: float, rng: np.random.Generator, mass
 
 
 def fcc_lattice(ncell: int, density: float, temperature: float, seed: int, cutoff: float = 2.5,
-                skin: float = 0.3, dt: float = 0.005) -> MDSystem:
+                skin: float = 0.3, dt: float = 0.005, jitter: float = 0.0) -> MDSystem:
     """Plain LJ fluid on an FCC lattice (4 atoms per cubic cell) in a periodic
-    cube, epsilon = sigma = m = 1, lattice offset a/4 from the faces."""
+    cube, epsilon = sigma = m = 1, lattice offset a/4 from the faces.  jitter > 0
+    displaces every atom uniformly in [-jitter, jitter]^3 (a perfect lattice has
+    zero net forces, which makes a poor force test)."""
     a = (4.0 / density) ** (1.0 / 3.0)
     L = ncell * a
     basis = np.array([[0, 0, 0], [0.5, 0.5, 0], [0.5, 0, 0.5], [0, 0.5, 0.5]], np.float64)
@@ -113,6 +115,8 @@ def fcc_lattice(ncell: int, density: float, temperature: float, seed: int, cutof
     n = pos.shape[0]
     rng = np.random.default_rng(seed)
     vel = maxwell_boltzmann(n, temperature, rng)
+    if jitter > 0:
+        pos = pos + rng.uniform(-jitter, jitter, size=pos.shape)
     coef = (cutoff + skin) / cutoff
     lj = LJParams(cutoff=cutoff, epsilon=np.ones((1, 1)), sigma=np.ones((1, 1)))
     return MDSystem(lo=np.zeros(3), hi=np.full(3, L), mass=np.ones(1), charge=np.zeros(1), pos=pos, vel=vel,

@@ -1,0 +1,165 @@
+/* caviar_b200.h -- C ABI of the B200 (sm_100a) MD timestep hot path.
+ *
+ * One opaque context per periodic system.  The context owns every device
+ * buffer and a CUDA stream; host pointers passed in are borrowed for the call
+ * only.  Every function returns CVR_OK (0) or a CVR_ERR_* code and never
+ * exits the process; cvr_last_error() gives the message.  A context is not
+ * thread safe: use one per host thread.
+ *
+ * Each entry point replaces one piece of the reference's object interface
+ * (CAVIAR, paths relative to its project root).  The reference shares state
+ * between objects through Atom_data's public vectors; here that state lives
+ * in the context, in HBM.
+ */
+#ifndef CAVIAR_B200_H
+#define CAVIAR_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------ status codes */
+#define CVR_OK 0
+#define CVR_ERR_INVALID 1   /* bad argument (reference: error->all on read/verify) */
+#define CVR_ERR_CUDA 2      /* CUDA runtime error */
+#define CVR_ERR_NAN 3       /* NaN acceleration (md_simulator.cpp:584-590) */
+#define CVR_ERR_STATE 4     /* wrong call order, e.g. cvr_run before cvr_set_state */
+#define CVR_ERR_GEOMETRY 5  /* box/cutoff combination the path cannot represent */
+#define CVR_ERR_CAPACITY 6  /* neighbour list or cell capacity exceeded and regrow failed */
+#define CVR_ERR_NOMEM 7     /* device allocation failed */
+
+/* ------------------------------------------------------------ option values */
+#define CVR_PREC_MIXED 0    /* FP32 pair/k-space math; FP64 positions, S(k), energy/virial sums */
+#define CVR_PREC_FP64 1     /* everything FP64 (the comparison form) */
+
+#define CVR_REBUILD_DISPLACEMENT 0 /* rebuild when an atom moved > skin/2 since the last build */
+#define CVR_REBUILD_REFERENCE 1    /* also on any owned wrap or ghost-set change (neighborlist.cpp:91-139) */
+#define CVR_REBUILD_EVERY_STEP 2   /* Neighborlist rebuild_test (neighborlist.cpp:98-101) */
+
+/* Thermo record written by cvr_run / cvr_get_scalars, in this order. */
+#define CVR_TH_STEP 0
+#define CVR_TH_KE 1        /* kinetic energy, COM removed when all axes are periodic (kinetic_energy.cpp:58-72) */
+#define CVR_TH_TEMP 2      /* 2 KE / (k_b dof)  (kinetic_energy.cpp:193-202) */
+#define CVR_TH_E_LJ 3      /* LJ energy of the linear force-shifted potential (lj.cpp:439-448) */
+#define CVR_TH_E_EWR 4     /* Ewald real-space energy over the list pairs */
+#define CVR_TH_E_K 5       /* Ewald k-space energy (electrostatic_ewald_k/energy.cpp:61-107) */
+#define CVR_TH_E_SELF 6    /* Ewald self energy (energy.cpp:31-50) */
+#define CVR_TH_VIRIAL 7    /* virialForce: LJ + Ewald-r, each pair once (lj.cpp:451-453) */
+#define CVR_TH_PRESSURE 8  /* N k_b T / V + virial / 3V (kinetic_energy.cpp:242-300) */
+#define CVR_TH_BUILDS 9    /* Verlet-list builds so far */
+#define CVR_N_THERMO 10
+
+typedef struct cvr_ctx cvr_ctx;
+
+/* Domain box + Atom_data type table.
+ * Replaces: Domain::read xmin..zmax/boundary_condition/generate (domain.cpp:206-266),
+ *           Atom_data add_type_mass / add_type_charge (atom_data.cpp:224-245, 574-595).
+ * lo, hi: box corners; bc: 1 periodic, 0 not; mass, charge: n_types each (host).
+ * device: CUDA ordinal. */
+int cvr_create(cvr_ctx **out, const double lo[3], const double hi[3], const int bc[3], int n_types,
+               const double *mass, const double *charge, int device);
+void cvr_destroy(cvr_ctx *ctx);
+
+/* Neighborlist basic: cutoff, cutoff_extra_coef (rl = cutoff * coef), and
+ * Atom_data ghost_cutoff; rebuild policy (CVR_REBUILD_*).
+ * Replaces: Neighborlist::read (neighborlist.cpp:193-251), init (:313-406),
+ *           update_is_needed (:91-139). */
+int cvr_set_neighborlist(cvr_ctx *ctx, double cutoff, double cutoff_extra_coef, double ghost_cutoff,
+                         int rebuild_policy);
+
+/* force_field lj: cutoff; epsilon, sigma: n_types*n_types row-major; cutoff_list:
+ * n_types*n_types or NULL; ignore_intra_molecule: 0/1.
+ * Replaces: Lj::read (lj.cpp:42-147), verify_settings (:149-353),
+ *           calculate_acceleration (:355-483). */
+int cvr_set_lj(cvr_ctx *ctx, double cutoff, const double *epsilon, const double *sigma,
+               const double *cutoff_list, int ignore_intra_molecule);
+
+/* force_field electrostatic_ewald_r: alpha, k_electrostatic; lambda: n_types^2
+ * same-molecule scaling or NULL; cutoff < 0 keeps the reference's behaviour of
+ * summing every list pair (electrostatic_ewald_r.cpp:142-226 has no cutoff test).
+ * Replaces: Electrostatic_ewald_r::read (:38-88), calculate_acceleration (:115-317). */
+int cvr_set_ewald_r(cvr_ctx *ctx, double alpha, double k_electrostatic, const double *lambda, double cutoff);
+
+/* force_field electrostatic_ewald_k: alpha, kx/ky/kz_max, k_electrostatic.
+ * Uses the reference's k-set: the first (2kx)(2ky)(2kz) vectors of the
+ * [-kmax,kmax]^3 \ {0} enumeration (initialize.cpp:184-222).
+ * Replaces: Electrostatic_ewald_k::read (:48-143), initialize (initialize.cpp:31-92),
+ *           calculate_potential_k_coef_cmplx (:117-146), calculate_acceleration (:161-294). */
+int cvr_set_ewald_k(cvr_ctx *ctx, double alpha, int kx_max, int ky_max, int kz_max, double k_electrostatic);
+
+/* md_simulator basic: dt; atom_data k_b.
+ * Replaces: Md_simulator::read dt / integrator_type velocity_verlet (md_simulator.cpp:58-233). */
+int cvr_set_integrator(cvr_ctx *ctx, double dt, double k_b);
+
+/* CVR_PREC_MIXED (default) or CVR_PREC_FP64.  No reference counterpart
+ * (the reference is FP64 only). */
+int cvr_set_precision(cvr_ctx *ctx, int precision);
+
+/* Atoms from HOST memory: pos, vel: n*3 (x,y,z per atom, = Vector<double> AoS);
+ * type: n; mol: n molecule indices or NULL (-1 = none).  Atom i gets id i.
+ * Replaces: Atom_data::add_atom (atom_data.cpp:487-521) / add_xyz_data_file
+ *           (atom_data/add_xyz_data_file.cpp:22-168). */
+int cvr_set_state(cvr_ctx *ctx, int64_t n, const double *pos, const double *vel, const int32_t *type,
+                  const int32_t *mol);
+
+/* Build the Verlet list at the current positions (force = 1), or only if the
+ * rebuild policy says so (force = 0).  *rebuilt (nullable) = 1 if it did.
+ * Replaces: Neighborlist::build (neighborlist.cpp:66-88). */
+int cvr_build_neighbors(cvr_ctx *ctx, int force, int *rebuilt);
+
+/* Accelerations of every enabled force field at the current positions and
+ * list, plus energies and virial.  acc: n*3 host (nullable), in id order;
+ * thermo: CVR_N_THERMO host (nullable).
+ * Replaces: Md_simulator::re_calculate_acc's force part (md_simulator.cpp:370-373),
+ *           Force_field::energy (force_field.h:36-50). */
+int cvr_compute_forces(cvr_ctx *ctx, double *acc, double *thermo);
+
+/* Advance nsteps velocity-Verlet steps (the first call also does setup:
+ * list + forces).  Every thermo_every steps (0 = never) a CVR_N_THERMO record
+ * is appended to thermo (host, nullable; capacity nsteps/thermo_every records).
+ * Replaces: Md_simulator::run / step (md_simulator.cpp:235-274, 382-485),
+ *           integrate_velocity_verlet (:555-668), setup (:504-549). */
+int cvr_run(cvr_ctx *ctx, int64_t nsteps, int64_t thermo_every, double *thermo);
+
+/* Current state to HOST memory in id order (each nullable): pos, vel, acc n*3.
+ * Positions are wrapped into the box the way Domain::fix_position does. */
+int cvr_get_state(cvr_ctx *ctx, double *pos, double *vel, double *acc);
+
+/* Canonical pair set of the current list: 5 int32 per pair
+ * (id_a < id_b, image shift sx, sy, sz of b), sorted.  Returns the count
+ * (< 0 on error); out may be NULL to count only.
+ * Replaces: reading Neighborlist::neighlist (neighborlist.h:88) + ghost ids. */
+int64_t cvr_get_pairs(cvr_ctx *ctx, int32_t *out);
+
+/* S(k) of the used k-vectors from the last force evaluation: 2 doubles
+ * (re, im) per vector (host).  Returns the count (< 0 on error).
+ * Replaces: reading Electrostatic_ewald_k::potential_k_coef_cmplx (electrostatic_ewald_k.h:83). */
+int64_t cvr_get_sk(cvr_ctx *ctx, double *out);
+
+/* Last thermo record (CVR_N_THERMO doubles, host). */
+int cvr_get_scalars(cvr_ctx *ctx, double *thermo);
+
+/* Diagnostics. */
+int cvr_last_error(const cvr_ctx *ctx, char *buf, size_t len);
+int64_t cvr_launch_count(const cvr_ctx *ctx);     /* kernels launched by this context so far */
+void *cvr_get_stream(const cvr_ctx *ctx);         /* the cudaStream_t the context launches on */
+int cvr_get_info(const cvr_ctx *ctx, int64_t *out, int len); /* n, cells x/y/z, list capacity, builds, ... */
+
+/* Kernel timing: when on, CUDA events bracket every launch of the named
+ * kernel class on the context's stream; cvr_kernel_time returns the summed
+ * milliseconds and the launch count since the last reset. */
+#define CVR_KT_PAIR 0      /* LJ + Ewald real-space pair force */
+#define CVR_KT_KSPACE 1    /* S(k) + k-space force */
+#define CVR_KT_INTEGRATE 2 /* velocity-Verlet kernels */
+#define CVR_KT_BUILD 3     /* binning + Verlet-list build */
+#define CVR_N_KT 4
+int cvr_set_kernel_timing(cvr_ctx *ctx, int on);
+int cvr_kernel_time(cvr_ctx *ctx, int kind, double *ms, int64_t *launches);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

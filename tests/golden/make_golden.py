@@ -1,0 +1,115 @@
+"""Generates the golden fixtures under tests/golden/ (run once, in a
+container that has the reference sources; the fixtures are committed so the
+GPU tests never need the reference at run time).
+
+1. ewald_n100.json -- the reference's own Ewald known-answer case
+   (benchmark/b2-ewald): 100 ions (type 0 q=-1, type 1 q=+1) in a 10^3
+   periodic box, alpha = 1.112583061, real-space cutoff 4.9, kmax 30, with
+   the published forces and total energy of benchmark/b2-ewald/espressopp/
+   ewald_result.dat.  Positions and types come from
+   benchmark/b2-ewald/caviar/ewald-n100.casl (`m1 add_atom aX at_position x y z`).
+
+2. ref_*.npz -- outputs of the unmodified reference (oracle/_ref/ref_harness,
+   compiled from the reference sources by oracle/Makefile) on small seeded
+   systems: accelerations, canonical pair set, virial, kinetic energy, S(k),
+   k-space and self energies, and a short trajectory.
+
+Usage:  python tests/golden/make_golden.py [/path/to/reference]
+"""
+import json
+import os
+import re
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from caviar_b200 import workloads as W  # noqa: E402
+from oracle import oracle as O  # noqa: E402
+
+
+def ewald_n100(ref_root: str) -> dict:
+    casl = os.path.join(ref_root, "benchmark", "b2-ewald", "caviar", "ewald-n100.casl")
+    dat = os.path.join(ref_root, "benchmark", "b2-ewald", "espressopp", "ewald_result.dat")
+    pos, typ = [], []
+    pat = re.compile(r"^\s*m1\s+add_atom\s+a([12])\s+at_position\s+(\S+)\s+(\S+)\s+(\S+)")
+    with open(casl) as f:
+        for line in f:
+            m = pat.match(line)
+            if m:
+                typ.append(int(m.group(1)) - 1)
+                pos.append([float(m.group(2)), float(m.group(3)), float(m.group(4))])
+    forces, energy = [], None
+    with open(dat) as f:
+        lines = f.read().splitlines()
+    for k, line in enumerate(lines):
+        if line.strip().startswith("total_energy"):
+            energy = float(lines[k + 1])
+        m = re.match(r"^\s*\{\s*(\S+)\s+(\S+)\s+(\S+)\s*\}", line)
+        if m:
+            forces.append([float(m.group(1)), float(m.group(2)), float(m.group(3))])
+    assert len(pos) == 100 and len(forces) == 100 and energy is not None
+    return {
+        "source": "benchmark/b2-ewald (caviar/ewald-n100.casl positions, espressopp/ewald_result.dat forces)",
+        "box": [0.0, 10.0], "alpha": 1.112583061, "rcut": 4.9, "kmax": 30,
+        "charge_by_type": [-1.0, 1.0], "mass_by_type": [1.0, 1.0],
+        "type": typ, "pos": pos, "force": forces, "total_energy": energy,
+    }
+
+
+def small_systems():
+    out = {}
+    # plain LJ, FCC 5^3 cells (500 atoms, L = 8.40 >= 2 rl), lattice jittered by 0.1
+    out["lj500"] = W.fcc_lattice(5, 0.8442, 0.72, seed=11, jitter=0.1)
+    # two-type LJ mixture with cutoff_list and Lorentz-Berthelot-like sigma
+    s = W.fcc_lattice(5, 0.8442, 1.0, seed=12, jitter=0.1)
+    s.type = (np.arange(s.n) % 3 == 0).astype(np.int32)
+    s.mass = np.array([1.0, 2.0])
+    s.charge = np.zeros(2)
+    s.lj = W.LJParams(cutoff=2.5, epsilon=np.array([[1.0, 0.75], [0.75, 0.5]]),
+                      sigma=np.array([[1.0, 0.94], [0.94, 0.88]]),
+                      cutoff_list=np.array([[2.5, 2.2], [2.2, 2.0]]))
+    s.name = "ljmix500"
+    out["ljmix500"] = s
+    # charged LJ + Ewald r + k (L = 16, rl = 5.15, kmax 4)
+    out["ions500"] = W.random_ions(500, 16.0, seed=13, rc=5.0, kmax=4, alpha=0.6)
+    return out
+
+
+def save_ref(name, s, nsteps=20):
+    f = O.run_reference(s, "forces")
+    r = O.run_reference(s, "run", nsteps=nsteps)
+    d = dict(
+        lo=s.lo, hi=s.hi, mass=s.mass, charge=s.charge, pos=s.pos, vel=s.vel, type=s.type,
+        cutoff=s.cutoff, coef=s.coef, ghost_cutoff=s.ghost_cutoff, dt=s.dt,
+        lj_cutoff=s.lj.cutoff if s.lj else -1.0,
+        lj_eps=s.lj.epsilon if s.lj else np.zeros((1, 1)),
+        lj_sigma=s.lj.sigma if s.lj else np.zeros((1, 1)),
+        lj_cutoff_list=s.lj.cutoff_list if (s.lj is not None and s.lj.cutoff_list is not None) else np.zeros((0, 0)),
+        ewr_alpha=s.ewald_r.alpha if s.ewald_r else -1.0,
+        ewk_alpha=s.ewald_k.alpha if s.ewald_k else -1.0,
+        ewk_kmax=np.array(s.ewald_k.kmax if s.ewald_k else (0, 0, 0)),
+        ref_acc=f["acc"], ref_pairs=f["pairs"], ref_virial=f["virial"], ref_ke=f["ke"],
+        ref_sk=f.get("sk", np.zeros(0)), ref_ek=f.get("ek_kspace", 0.0), ref_eself=f.get("ek_self", 0.0),
+        run_steps=nsteps, run_pos=r["pos"], run_vel=r["vel"], run_acc=r["acc"], run_ke=r["ke_trace"],
+        run_virial=r["vir_trace"],
+    )
+    np.savez_compressed(os.path.join(HERE, f"ref_{name}.npz"), **d)
+
+
+def main():
+    ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    g = ewald_n100(ref_root)
+    with open(os.path.join(HERE, "ewald_n100.json"), "w") as f:
+        json.dump(g, f, indent=0)
+    O.build(ref_root)
+    for name, s in small_systems().items():
+        save_ref(name, s)
+    print("golden fixtures written to", HERE)
+
+
+if __name__ == "__main__":
+    main()

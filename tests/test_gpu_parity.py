@@ -1,0 +1,187 @@
+"""GPU parity of the sm_100a path (through the C ABI) against the reference.
+
+Oracles: the unmodified reference's own outputs (tests/golden/ref_*.npz,
+produced by oracle/_ref built from the reference sources), the published
+Ewald known answer (tests/golden/ewald_n100.json), and the FP64 C
+restatement (oracle/) for cases without a fixture.
+
+Tolerances (stated here, used below):
+  * pair sets: bit-exact (same sorted canonical pair set);
+  * FP64 form: accelerations within 1e-12 relative (global), energies/virial 1e-11;
+  * mixed form: global relative force error ||dF|| / ||F|| <= 1e-5 and
+    per-atom max |dF_i| <= 1e-4 * rms|F|; energies/virial 1e-5 relative.
+"""
+import numpy as np
+import pytest
+
+from helpers import ewald_golden, force_errors, load_ref_fixture
+
+pytestmark = pytest.mark.gpu
+
+FIXTURES = ["lj500", "ljmix500", "ions500"]
+PRECS = ["mixed", "fp64"]
+
+
+def sim_for(abi, s, prec, policy=None):
+    p = abi.PREC_FP64 if prec == "fp64" else abi.PREC_MIXED
+    pol = abi.REBUILD_DISPLACEMENT if policy is None else policy
+    return abi.Simulation(s, precision=p, policy=pol)
+
+
+def check_forces(acc, ref, prec):
+    g, mx, _ = force_errors(acc, ref)
+    if prec == "fp64":
+        assert g < 1e-12, (g, mx)
+    else:
+        assert g <= 1e-5, (g, mx)
+        assert mx <= 1e-4, (g, mx)
+    return g, mx
+
+
+@pytest.mark.parametrize("prec", PRECS)
+@pytest.mark.parametrize("name", FIXTURES)
+def test_pair_set_bit_exact(cuda_lib, name, prec):
+    s, d = load_ref_fixture(name)
+    sim = sim_for(cuda_lib, s, prec)
+    sim.build_neighbors(True)
+    assert np.array_equal(sim.pairs(), d["ref_pairs"])
+
+
+@pytest.mark.parametrize("prec", PRECS)
+@pytest.mark.parametrize("name", FIXTURES)
+def test_forces_energy_virial_vs_reference(cuda_lib, oracle_lib, name, prec):
+    s, d = load_ref_fixture(name)
+    sim = sim_for(cuda_lib, s, prec)
+    acc, th = sim.compute_forces()
+    check_forces(acc, d["ref_acc"].reshape(-1, 3), prec)
+    tol = 1e-11 if prec == "fp64" else 1e-5
+    assert abs(th["virial"] - float(d["ref_virial"])) <= tol * abs(float(d["ref_virial"]))
+    assert abs(th["ke"] - float(d["ref_ke"])) <= 1e-12 * abs(float(d["ref_ke"]))
+    o = oracle_lib.Oracle(s)
+    o.setup()
+    e = o.energy()
+    scale = abs(e["e_lj"]) + abs(e["e_ewald_r"]) + 1.0
+    assert abs(th["e_lj"] - e["e_lj"]) <= tol * scale
+    assert abs(th["e_ewald_r"] - e["e_ewald_r"]) <= tol * scale
+    if s.ewald_k is not None:
+        assert abs(th["e_ewald_k"] - float(d["ref_ek"])) <= tol * abs(float(d["ref_ek"]))
+        assert abs(th["e_self"] - float(d["ref_eself"])) <= 1e-12 * abs(float(d["ref_eself"]))
+        sk = sim.sk()
+        ref_sk = d["ref_sk"][0::2] + 1j * d["ref_sk"][1::2]
+        assert np.abs(sk - ref_sk).max() <= (1e-11 if prec == "fp64" else 1e-5) * np.abs(ref_sk).max()
+
+
+@pytest.mark.parametrize("prec", PRECS)
+def test_golden_ewald_known_answer(cuda_lib, prec):
+    s, force, energy = ewald_golden()
+    sim = sim_for(cuda_lib, s, prec)
+    acc, th = sim.compute_forces()
+    check_forces(acc, force, prec)
+    e = th["e_ewald_r"] + th["e_ewald_k"] + th["e_self"]
+    assert abs(e - energy) <= (1e-10 if prec == "fp64" else 1e-5) * abs(energy)
+
+
+@pytest.mark.parametrize("prec", PRECS)
+@pytest.mark.parametrize("name", FIXTURES)
+def test_trajectory_vs_reference(cuda_lib, name, prec):
+    """20 velocity-Verlet steps under the reference's rebuild policy."""
+    s, d = load_ref_fixture(name)
+    sim = sim_for(cuda_lib, s, prec, policy=cuda_lib.REBUILD_REFERENCE)
+    sim.run(int(d["run_steps"]))
+    pos, vel, acc = sim.state()
+    L = s.box
+    dp = pos - d["run_pos"].reshape(-1, 3)
+    dp -= L * np.round(dp / L)
+    tol_p = 1e-9 if prec == "fp64" else 1e-5
+    assert np.abs(dp).max() < tol_p
+    g, _, _ = force_errors(acc, d["run_acc"].reshape(-1, 3))
+    assert g < (1e-8 if prec == "fp64" else 1e-4)
+
+
+def test_reference_policy_rebuild_count(cuda_lib, oracle_lib):
+    s, d = load_ref_fixture("lj500")
+    o = oracle_lib.Oracle(s, policy=oracle_lib.POLICY_REFERENCE)
+    o.setup()
+    o.step(int(d["run_steps"]))
+    sim = sim_for(cuda_lib, s, "fp64", policy=cuda_lib.REBUILD_REFERENCE)
+    sim.run(int(d["run_steps"]))
+    assert sim.info()["builds"] == int(o.scalars()["n_builds"])
+
+
+@pytest.mark.parametrize("prec", PRECS)
+def test_lj4000_vs_oracle(cuda_lib, oracle_lib, prec):
+    from caviar_b200 import workloads as W
+    s = W.fcc_lattice(10, 0.8442, 0.72, seed=1, jitter=0.1)
+    o = oracle_lib.Oracle(s)
+    o.setup()
+    sim = sim_for(cuda_lib, s, prec)
+    acc, th = sim.compute_forces()
+    assert np.array_equal(sim.pairs(), o.pairs())
+    check_forces(acc, o.state()[2], prec)
+
+
+def test_deterministic(cuda_lib):
+    from caviar_b200 import workloads as W
+    s = W.config_lj_4000()
+    out = []
+    for _ in range(2):
+        sim = sim_for(cuda_lib, s, "mixed")
+        sim.run(50)
+        out.append(sim.state())
+    for a, b in zip(*out):
+        assert np.array_equal(a, b)
+
+
+def test_edge_cases(cuda_lib):
+    from caviar_b200 import workloads as W
+    s = W.fcc_lattice(3, 0.8442, 0.5, seed=1)
+    one = s.copy()
+    one.pos, one.vel, one.type = s.pos[:1], s.vel[:1], s.type[:1]
+    sim = sim_for(cuda_lib, one, "mixed")
+    acc, _ = sim.compute_forces()
+    assert sim.pairs().shape == (0, 5) and np.all(acc == 0)
+    L = float(s.box[0])
+    two = s.copy()
+    two.pos = np.array([[0.5, 1.0, 1.0], [L - 0.5, 1.0, 1.0]])
+    two.vel = np.zeros((2, 3))
+    two.type = np.zeros(2, np.int32)
+    sim = sim_for(cuda_lib, two, "fp64")
+    acc, _ = sim.compute_forces()
+    assert sim.pairs().tolist() == [[0, 1, -1, 0, 0]]
+    assert acc[0, 0] > 0 and acc[1, 0] < 0
+    face = two.copy()
+    face.pos = np.array([[L, 1.0, 1.0], [L - 1.0, 1.0, 1.0]])
+    sim = sim_for(cuda_lib, face, "fp64")
+    sim.build_neighbors(True)
+    assert sim.pairs().shape[0] == 1
+
+
+def test_nan_is_reported(cuda_lib):
+    from caviar_b200 import workloads as W
+    s = W.fcc_lattice(3, 0.8442, 0.5, seed=1)
+    s.pos = s.pos.copy()
+    s.pos[1] = s.pos[0]  # coincident LJ atoms -> infinite / NaN force
+    sim = sim_for(cuda_lib, s, "mixed")
+    with pytest.raises(cuda_lib.CvrError) as e:
+        sim.run(2)
+    assert e.value.code == 3
+
+
+def test_list_overflow_regrows(cuda_lib, oracle_lib):
+    """Compress the atoms after the first build so the next build needs a
+    longer list than the first one sized: the list regrows and the pair set
+    still matches the oracle."""
+    from caviar_b200 import workloads as W
+    s = W.fcc_lattice(4, 0.3, 0.0, seed=1)
+    sim = sim_for(cuda_lib, s, "fp64")
+    sim.build_neighbors(True)
+    cap0 = sim.info()["cap"]
+    pos = s.lo + (s.pos - s.lo) * 0.6
+    sim.set_state(pos, np.zeros_like(pos), s.type)
+    sim.build_neighbors(True)
+    assert sim.info()["cap"] > cap0
+    s2 = s.copy()
+    s2.pos = pos
+    o = oracle_lib.Oracle(s2)
+    o.build_list()
+    assert np.array_equal(sim.pairs(), o.pairs())
