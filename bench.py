@@ -1,0 +1,381 @@
+#!/usr/bin/env python
+"""Throughput of the B200 MD timestep hot path (atom-steps/s).
+
+Headline workload (value): 1,048,576-atom LJ fluid (FCC 64^3 cells, rho* 0.8442,
+T* 0.72, rc 2.5 sigma, skin 0.3 sigma, dt 0.005), mixed precision (FP32 pair math,
+FP64 positions and sums).  The same line carries, for the metric's other
+halves: the FP64 GPU form of the same kernels, the 8000-ion Ewald electrolyte
+(L = 40, alpha 0.3, rc 10, kmax 8) in both precisions, and the relative force
+error of the mixed form against the FP64 form on identical states.
+
+A step is one velocity-Verlet step of the whole system (list maintenance,
+forces, integration).  Inputs (positions, list) are far larger than L2 for the
+headline workload, so no flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+N > 1 (under torchrun): every rank advances its own replica of the workload
+(the path does not shard; replicas only), timing is the max over ranks.
+`--impl reference` times the reference's own CPU implementation
+(oracle/_ref/ref_harness, the unmodified reference compiled from its sources)
+on the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "atom-steps/s: 1M LJ + 8K-ion Ewald, mixed vs FP64 GPU at ≤1e-5 rel force err"
+UNIT = "atom-steps/s"
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.p = None
+        self.f = None
+
+    def __enter__(self):
+        try:
+            self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except Exception:
+                self.p.kill()
+
+    def summary(self):
+        if not self.f:
+            return None
+        try:
+            self.f.seek(0)
+            rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+        except Exception:
+            return None
+        finally:
+            try:
+                os.unlink(self.f.name)
+            except Exception:
+                pass
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+            except (ValueError, IndexError):
+                continue
+            for k, nm in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profiled_traffic(name: str):
+    """dram bytes per launch of a kernel, from a committed ncu summary (profiles/)."""
+    path = os.path.join(ROOT, "profiles", name)
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.startswith("dram_bytes_per_launch_full_size:"):
+                    return float(line.split(":", 1)[1].split()[0])
+    except Exception:
+        pass
+    return None
+
+
+# ---------------------------------------------------------------- GPU arm
+
+def time_run(sim, torch, steps: int, warmup: int, dist=None, thermo_every: int = 0):
+    """Device time of exactly `steps` steps on the context's stream (CUDA
+    events), bracketed by barrier + synchronize; returns ms."""
+    stream = torch.cuda.ExternalStream(sim.stream)
+    sim.run(warmup)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    sim.run(steps, thermo_every)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    return e0.elapsed_time(e1)
+
+
+def max_over_ranks(x: float, dist, torch):
+    if dist is None:
+        return x
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def force_error(abi, s):
+    """Mixed-form accelerations against the FP64 form on the same state:
+    (global ||dF||/||F||, max_i |dF_i| / rms|F|)."""
+    a = abi.Simulation(s, precision=abi.PREC_MIXED)
+    b = abi.Simulation(s, precision=abi.PREC_FP64)
+    fa, _ = a.compute_forces()
+    fb, _ = b.compute_forces()
+    a.close()
+    b.close()
+    d = np.linalg.norm(fa - fb, axis=1)
+    nb = np.linalg.norm(fb, axis=1)
+    return float(np.linalg.norm(d) / np.linalg.norm(nb)), float(d.max() / np.sqrt(np.mean(nb ** 2)))
+
+
+def gpu_arm(args):
+    import torch
+    rank, world, local = dist_env()
+    dist = None
+    if world > 1:
+        import torch.distributed as td
+        torch.cuda.set_device(local)
+        td.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+        dist = td
+    else:
+        torch.cuda.set_device(0)
+    from caviar_b200 import build as B
+    B.build()
+    from caviar_b200 import _abi as abi
+    from caviar_b200 import workloads as W
+
+    steps, warmup = args.steps, max(3, args.warmup)
+    s_lj = W.config_lj_1m(seed=3 + rank)
+    n = s_lj.n
+
+    # --- headline: 1M LJ, mixed, device-resident inputs
+    sim = abi.Simulation(s_lj, precision=abi.PREC_MIXED, device=local)
+    sim.run(warmup)
+    l0 = sim.launches
+    b0 = sim.info()["builds"]
+    sim.set_kernel_timing(True)
+    with Clocks(local) as clk:
+        ms = time_run(sim, torch, steps, 0, dist)
+    launches = sim.launches - l0
+    pair_ms, pair_n = sim.kernel_time(abi.KT_PAIR)
+    build_ms, build_n = sim.kernel_time(abi.KT_BUILD)
+    integ_ms, integ_n = sim.kernel_time(abi.KT_INTEGRATE)
+    sim.set_kernel_timing(False)
+    info = sim.info()
+    builds = info["builds"] - b0
+    ms_max = max_over_ranks(ms, dist, torch)
+    value = world * n * steps / (ms_max / 1e3)
+
+    # --- e2e through the public API: host (pinned) buffers in, results out
+    pos_h = torch.from_numpy(np.ascontiguousarray(s_lj.pos)).pin_memory()
+    vel_h = torch.from_numpy(np.ascontiguousarray(s_lj.vel)).pin_memory()
+    typ_h = torch.from_numpy(np.ascontiguousarray(s_lj.type, np.int32)).pin_memory()
+    out_p = torch.empty((n, 3), dtype=torch.float64).pin_memory()
+    out_v = torch.empty((n, 3), dtype=torch.float64).pin_memory()
+    thermo = torch.empty((steps, abi.N_THERMO), dtype=torch.float64).pin_memory()
+    sim2 = abi.Simulation(s_lj, precision=abi.PREC_MIXED, device=local)
+    sim2.run(warmup)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    t0 = time.perf_counter()
+    sim2.set_state_ptr(n, pos_h.data_ptr(), vel_h.data_ptr(), typ_h.data_ptr())
+    sim2.run_ptr(steps, 1, thermo.data_ptr())
+    sim2.get_state_ptr(out_p.data_ptr(), out_v.data_ptr(), 0)
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(time.perf_counter() - t0, dist, torch)
+    e2e = world * n * steps / e2e_s
+    h2d = n * (3 * 8 + 3 * 8 + 4)
+    d2h = n * (3 * 8 + 3 * 8)
+    sim2.close()
+
+    # --- secondary lines: FP64 form, 8K ions, force error (rank 0 only)
+    sec = {}
+    if rank == 0:
+        sim64 = abi.Simulation(s_lj, precision=abi.PREC_FP64, device=local)
+        ms64 = time_run(sim64, torch, steps, warmup)
+        sec["lj_1m_fp64"] = {"value": n * steps / (ms64 / 1e3), "ms_per_step": ms64 / steps}
+        sim64.close()
+        s_ion = W.config_ions_8000(seed=2)
+        ion = {}
+        for nm, p in (("mixed", abi.PREC_MIXED), ("fp64", abi.PREC_FP64)):
+            si = abi.Simulation(s_ion, precision=p, device=local)
+            si.set_kernel_timing(True)
+            msi = time_run(si, torch, steps, warmup)
+            kms, kn = si.kernel_time(abi.KT_KSPACE)
+            pms, pn = si.kernel_time(abi.KT_PAIR)
+            ion[nm] = {"value": s_ion.n * steps / (msi / 1e3), "ms_per_step": msi / steps,
+                       "kspace_ms_per_step": kms / max(kn, 1), "pair_ms_per_step": pms / max(pn, 1)}
+            si.close()
+        sec["ions_8k_mixed"] = ion["mixed"]
+        sec["ions_8k_fp64"] = ion["fp64"]
+        sec["mixed_over_fp64"] = {"lj_1m": value / world / sec["lj_1m_fp64"]["value"],
+                                  "ions_8k": ion["mixed"]["value"] / ion["fp64"]["value"]}
+        g1, m1 = force_error(abi, W.fcc_lattice(64, 0.8442, 0.72, seed=3, jitter=0.1))
+        g2, m2 = force_error(abi, s_ion)
+        sec["force_rel_err_mixed_vs_fp64"] = {"lj_1m": {"global": g1, "max_over_rms": m1},
+                                              "ions_8k": {"global": g2, "max_over_rms": m2}}
+
+    # --- roofline of the dominant kernel (the pair kernel on the headline workload)
+    peak, peak_kind = measured_peaks()
+    real_b = 4
+    mean_cnt = info["list_entries"] / n
+    bytes_launch = n * (4 * real_b + 4 + 3 * real_b) + 4.0 * mean_cnt * n
+    pair_avg_ms = pair_ms / max(pair_n, 1)
+    achieved = bytes_launch / (pair_avg_ms / 1e3) / 1e9
+    traffic = profiled_traffic("pair_lj1m.txt")
+    sim.close()
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(s_lj, budget_s=args.cpu_budget)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps, "warmup": warmup,
+            "ms_per_step": ms_max / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "fp32 pair/k-space math, fp64 positions + S(k) + energy/virial sums",
+            "data": "synthetic (seeded FCC lattice + Maxwell-Boltzmann velocities)",
+            "config": {"workload": "LJ fluid N=1048576 (FCC 64^3, rho*=0.8442, T*=0.72, rc=2.5, skin=0.3, dt=0.005), "
+                                   "mixed precision", "n_atoms": n, "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (list ~%d MB, positions %d MB)" % (
+                           int(4 * mean_cnt * n / 1e6), int(n * 24 / 1e6)),
+                       "rebuild_policy": "displacement (skin/2)", "list_builds_in_window": builds,
+                       "mean_neighbours": mean_cnt},
+            "roofline": {"bound": "hbm", "kernel": "k_pair (LJ, full Verlet list)", "achieved": achieved,
+                         "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                         "peak_source": peak_kind, "bytes_per_launch": bytes_launch,
+                         "avg_launch_ms": pair_avg_ms, "launches": pair_n,
+                         "share_of_step": pair_ms / ms if ms > 0 else None},
+            "kernel_ms_per_step": {"pair": pair_ms / max(steps, 1), "build": build_ms / max(steps, 1),
+                                   "integrate": integ_ms / max(steps, 1)},
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d / steps, "d2h_bytes_per_step":
+                    d2h / steps + 8 * abi.N_THERMO,
+                    "note": "cvr_set_state from pinned host buffers + cvr_run (setup, K steps, per-step thermo "
+                            "record read back) + cvr_get_state to pinned host buffers"},
+            "gpu_launches": launches,
+            "cpu_baseline": cpu,
+            "clocks": clk.summary(),
+            "secondary": sec,
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+# ----------------------------------------------------- reference CPU arm
+
+def reference_step_time(s, max_steps: int, budget_s: float):
+    """Run the unmodified reference on `s` until `budget_s` seconds of steps
+    (at least 2, at most max_steps + 1) and return (seconds per step after the
+    first, steps timed, seconds of the first step, which includes setup)."""
+    from oracle import oracle as O
+    if not O.harness_available():
+        return None
+    r = O.run_reference(s, "run", nsteps=max_steps + 1, budget_s=budget_s, timeout=budget_s * 10 + 600)
+    k = int(r["steps_done"]) - 1
+    return float(r["wall_rest"]) / k, k, float(r["wall_first"])
+
+
+def cpu_baseline(s, budget_s: float = 20.0):
+    try:
+        res = reference_step_time(s, 1000, budget_s)
+    except Exception as e:  # pragma: no cover - reported, not hidden
+        return {"value": None, "unit": UNIT, "cores": 1, "kind": "reference", "sample": f"failed: {e}"}
+    if res is None:
+        return {"value": None, "unit": UNIT, "cores": 1, "kind": "reference", "sample": "harness not built"}
+    per, k, first = res
+    return {"value": s.n / per, "unit": UNIT, "cores": 1, "kind": "reference",
+            "sample": f"{k} velocity-Verlet steps of the same {s.n}-atom system after a setup step "
+                      f"({first:.1f} s); serial reference (its OpenMP build does not compile)"}
+
+
+def reference_arm(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    from caviar_b200 import workloads as W
+    from oracle import oracle as O
+    s = W.config_lj_1m(seed=3)
+    if not O.harness_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_harness not built"}), flush=True)
+        return
+    # warm-up is the reference's setup step plus W steps is too long for 1M
+    # atoms at ~5 s/step; time a bounded number of whole steps instead.
+    budget = max(20.0, args.cpu_budget * 3)
+    per, k, first = reference_step_time(s, args.steps, budget)
+    value = s.n / per
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": k, "warmup": 1,
+            "ms_per_step": per * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "fp64", "data": "synthetic (seeded FCC lattice + Maxwell-Boltzmann velocities)",
+            "config": {"workload": "LJ fluid N=1048576 (FCC 64^3, rho*=0.8442, T*=0.72, rc=2.5, skin=0.3, "
+                                   "dt=0.005)", "n_atoms": s.n, "parallelism": "serial CPU"},
+            "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
+                             "sample": f"{k} steps after one setup step ({first:.1f} s); unmodified reference "
+                                       "compiled from its own sources, serial"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=500)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--cpu-budget", type=float, default=20.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        gpu_arm(args)
+
+
+if __name__ == "__main__":
+    main()

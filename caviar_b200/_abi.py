@@ -221,9 +221,10 @@ class Simulation:
         return dict(zip(TH_KEYS, th.tolist()))
 
     def info(self) -> dict:
-        v = (ctypes.c_int64 * 12)()
-        self._check(self.L.cvr_get_info(self.h, v, 12))
-        keys = ["n", "ncx", "ncy", "ncz", "cap", "builds", "tpa", "nk", "R", "max_count", "err", "step"]
+        v = (ctypes.c_int64 * 13)()
+        self._check(self.L.cvr_get_info(self.h, v, 13))
+        keys = ["n", "ncx", "ncy", "ncz", "cap", "builds", "tpa", "nk", "R", "max_count", "err", "step",
+                "list_entries"]
         return dict(zip(keys, list(v)))
 
     @property

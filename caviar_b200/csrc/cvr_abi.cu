@@ -1171,9 +1171,16 @@ int cvr_get_info(const cvr_ctx *c, int64_t *out, int len) {
     cudaMemcpyAsync(flags, c->flags, sizeof(flags), cudaMemcpyDeviceToHost, c->stream);
     cudaStreamSynchronize(c->stream);
   }
-  const int64_t v[12] = {c->n, c->nc[0], c->nc[1], c->nc[2], c->cap, flags[3], c->tpa, c->nk, c->R, flags[2],
-                         flags[1], c->step};
-  for (int k = 0; k < len && k < 12; ++k) out[k] = v[k];
+  int64_t entries = 0;
+  if (len > 12 && c->ncount && c->list_valid) {
+    std::vector<int> cnt(c->n);
+    cudaMemcpyAsync(cnt.data(), c->ncount, c->n * sizeof(int), cudaMemcpyDeviceToHost, c->stream);
+    cudaStreamSynchronize(c->stream);
+    for (int v : cnt) entries += v;
+  }
+  const int64_t v[13] = {c->n, c->nc[0], c->nc[1], c->nc[2], c->cap, flags[3], c->tpa, c->nk, c->R, flags[2],
+                         flags[1], c->step, entries};
+  for (int k = 0; k < len && k < 13; ++k) out[k] = v[k];
   return CVR_OK;
 }
 

@@ -146,7 +146,10 @@ int cvr_get_scalars(cvr_ctx *ctx, double *thermo);
 int cvr_last_error(const cvr_ctx *ctx, char *buf, size_t len);
 int64_t cvr_launch_count(const cvr_ctx *ctx);     /* kernels launched by this context so far */
 void *cvr_get_stream(const cvr_ctx *ctx);         /* the cudaStream_t the context launches on */
-int cvr_get_info(const cvr_ctx *ctx, int64_t *out, int len); /* n, cells x/y/z, list capacity, builds, ... */
+/* out[0..len): n, cells x, y, z, list capacity per atom, list builds, lanes
+ * per atom, k-vectors, stencil radius, largest neighbour count, error bits,
+ * step, total list entries (index 12 costs a device-to-host copy). */
+int cvr_get_info(const cvr_ctx *ctx, int64_t *out, int len);
 
 /* Kernel timing: when on, CUDA events bracket every launch of the named
  * kernel class on the context's stream; cvr_kernel_time returns the summed

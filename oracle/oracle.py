@@ -269,9 +269,10 @@ def harness_available() -> bool:
 
 
 def run_reference(system, mode: str = "forces", nsteps: int = 0, rebuild_test: bool = False,
-                  timeout: Optional[float] = None) -> Dict[str, np.ndarray]:
+                  timeout: Optional[float] = None, budget_s: float = 0.0) -> Dict[str, np.ndarray]:
     """Run the unmodified reference on `system` ("forces" or "run") and return
-    its FP64 output blocks plus the harness's own wall time."""
+    its FP64 output blocks plus the harness's own wall time.  budget_s > 0
+    stops a run after the step that crosses the budget (at least 2 steps)."""
     if not harness_available():
         raise FileNotFoundError(f"reference harness not built: {HARNESS_PATH}")
     with tempfile.TemporaryDirectory() as d:
@@ -281,7 +282,7 @@ def run_reference(system, mode: str = "forces", nsteps: int = 0, rebuild_test: b
         with open(script, "w") as f:
             f.write(casl_script(system, nsteps, rebuild_test))
         write_state(state, system)
-        args = [HARNESS_PATH, script, state, mode, out] + ([str(nsteps)] if mode == "run" else [])
+        args = [HARNESS_PATH, script, state, mode, out] + ([str(nsteps), repr(float(budget_s))] if mode == "run" else [])
         t0 = time.perf_counter()
         p = subprocess.run(args, cwd=d, capture_output=True, text=True, timeout=timeout)
         wall = time.perf_counter() - t0

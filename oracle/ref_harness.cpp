@@ -5,7 +5,7 @@
 //
 // Usage:
 //   ref_harness <script.casl> <state.bin> forces <out.bin>
-//   ref_harness <script.casl> <state.bin> run    <out.bin> <nsteps>
+//   ref_harness <script.casl> <state.bin> run    <out.bin> <nsteps> [budget_seconds]
 //
 // The CASL script defines the objects (domain box, atom_data basic,
 // neighborlist basic, force fields, md_simulator basic) with the reference's
@@ -22,7 +22,8 @@
 // "run" calls Md_simulator::step(i) for i in [0, nsteps) (md_simulator.cpp:
 // 376-485) and dumps the final owned state plus per-step kinetic energy and
 // virial, and the wall time of the first step (which includes setup) and of
-// the remaining steps.
+// the remaining steps.  With a budget, it stops after the first step whose end
+// exceeds the budget (at least two steps) and reports how many ran.
 //
 // state.bin (little endian):
 //   int64 n; then n records of { int32 type; int32 mol; double pos[3]; double vel[3]; }
@@ -183,6 +184,7 @@ int main(int argc, char **argv)
   }
   const std::string mode = argv[3];
   const int64_t nsteps = (argc > 5) ? std::atoll(argv[5]) : 0;
+  const double budget = (argc > 6) ? std::atof(argv[6]) : 0.0;
 
   char arg0[] = "ref_harness";
   char arg1[] = "-i";
@@ -286,6 +288,7 @@ int main(int argc, char **argv)
   {
     std::vector<double> ke, vir;
     double t_first = 0, t_rest = 0;
+    int64_t done = 0;
     for (int64_t s = 0; s < nsteps; ++s)
     {
       const double t0 = now_s();
@@ -297,12 +300,16 @@ int main(int argc, char **argv)
         t_rest += t1 - t0;
       ke.push_back(ad->kinetic_energy());
       vir.push_back(ad->virialForce);
+      ++done;
+      if (budget > 0 && s >= 1 && t_first + t_rest > budget)
+        break;
     }
     dump_owned();
     out.block("ke_trace", ke.data(), (int64_t)ke.size(), 8);
     out.block("vir_trace", vir.data(), (int64_t)vir.size(), 8);
     out.scalar("wall_first", t_first);
     out.scalar("wall_rest", t_rest);
+    out.scalar("steps_done", (double)done);
     out.scalar("n_ghost", (double)ad->atom_struct_ghost.position.size());
   }
   else
