@@ -26,7 +26,8 @@ KT_PAIR, KT_KSPACE, KT_INTEGRATE, KT_BUILD = 0, 1, 2, 3
 EXPORTED = ["cvr_create", "cvr_destroy", "cvr_set_neighborlist", "cvr_set_lj", "cvr_set_ewald_r", "cvr_set_ewald_k",
             "cvr_set_integrator", "cvr_set_precision", "cvr_set_state", "cvr_build_neighbors", "cvr_compute_forces",
             "cvr_run", "cvr_get_state", "cvr_get_pairs", "cvr_get_sk", "cvr_get_scalars", "cvr_last_error",
-            "cvr_launch_count", "cvr_get_stream", "cvr_get_info", "cvr_set_kernel_timing", "cvr_kernel_time"]
+            "cvr_launch_count", "cvr_get_stream", "cvr_get_info", "cvr_set_kernel_timing", "cvr_kernel_time",
+            "cvr_structure_factor_noalloc"]
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int32)

@@ -9,7 +9,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libcaviar_b200.so")
-SOURCES = [os.path.join(HERE, "csrc", "cvr_abi.cu")]
+SOURCES = [os.path.join(HERE, "csrc", "cvr_abi.cu"), os.path.join(HERE, "csrc", "cvr_noalloc.cu")]
 DEPS = SOURCES + [os.path.join(HERE, "csrc", f) for f in ("cvr_device.cuh", "cvr_build.cuh", "cvr_force.cuh")] + [
     os.path.join(ROOT, "include", "caviar_b200.h")]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

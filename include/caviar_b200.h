@@ -162,6 +162,39 @@ int cvr_get_info(const cvr_ctx *ctx, int64_t *out, int len);
 int cvr_set_kernel_timing(cvr_ctx *ctx, int on);
 int cvr_kernel_time(cvr_ctx *ctx, int kind, double *ms, int64_t *launches);
 
+/* ---------------------------------------------------------- no allocation */
+/* Capacity, in complex doubles (16 B each), of the fixed device array behind
+ * cvr_structure_factor_noalloc: 262144 = 4 MiB per GPU that loads the library. */
+#define CVR_NOALLOC_SK_SCRATCH 262144
+
+/* Ewald structure factor S(k) = sum_j q_j exp(i k.r_j), k = 2 pi (nx/Lx, ny/Ly, nz/Lz)
+ * over the reference's k-set (the first (2kx)(2ky)(2kz) vectors of the
+ * [-kmax, kmax]^3 \ {0} enumeration), for callers that cannot allocate device
+ * memory: it calls no cudaMalloc, cudaFree or allocating library routine.
+ * No counterpart in the reference (there S(k) lives inside Electrostatic_ewald_k).
+ *
+ * Callers that need it run inside a host program whose allocator owns the
+ * GPU's memory (a framework's caching allocator, an engine that reserves its
+ * pool up front), are plug-ins forbidden to allocate after start-up, or cannot
+ * afford the device-wide synchronisation of cudaMalloc/cudaFree mid-run.
+ *
+ * pos: DEVICE, n*3 doubles (x, y, z per atom); q: DEVICE, n charges;
+ * box_len: HOST, 3 box lengths; sk: DEVICE, 2*(2kx)(2ky)(2kz) doubles (re, im)
+ * written in k-set order; stream: cudaStream_t (NULL = default stream);
+ * err/err_len: optional host buffer for a message.  Launches on the current
+ * device and returns without synchronising.
+ *
+ * Scratch: the chunk partial sums use one fixed device array of
+ * CVR_NOALLOC_SK_SCRATCH complex doubles per GPU, held until process exit.
+ * More k-vectors than that -> CVR_ERR_CAPACITY; k_max above 30 -> CVR_ERR_INVALID.
+ * The first call on each device looks up that array's device address; make it
+ * before any stream capture.  All calls share the array and it keeps the last
+ * call's contents (every partial is written before it is read, so nothing
+ * needs clearing); calls whose kernels overlap on the GPU race on it. */
+int cvr_structure_factor_noalloc(const double *pos, const double *q, int64_t n, const double box_len[3],
+                                 int kx_max, int ky_max, int kz_max, double *sk, void *stream, char *err,
+                                 size_t err_len);
+
 #ifdef __cplusplus
 }
 #endif
