@@ -116,14 +116,22 @@ struct cvr_ctx {
   double *d_fk{};
   KRun *d_runs{};
   double2 *d_kpartial{}, *d_sk{};
-  void *d_ak{};
+  void *d_ak{}, *d_fpart{};
   int nchunks = 0;
+  int kf_threads = 128, kf_slices = 1, kf_runs_per_slice = 1;
   // diagnostics
   std::string err;
   int64_t launches = 0;
   double last_thermo[CVR_N_THERMO] = {0};
   bool timing = false;
   KT kt[CVR_N_KT];
+  // CUDA graphs of one step (plain, thermo); rebuilt when buffers move
+  bool use_graphs = true;
+  int64_t epoch = 0, graph_epoch = -1;
+  cudaGraphExec_t g_step[2] = {nullptr, nullptr};
+  int64_t graph_kernels[2] = {0, 0};
+  long long *counters{};
+  long long counter_src[2] = {0, 0};
   std::vector<void *> all_allocs;
 };
 
@@ -156,6 +164,7 @@ int dalloc(cvr_ctx *c, T **p, size_t count) {
   cudaMemsetAsync(q, 0, count * sizeof(T), c->stream);
   c->all_allocs.push_back(q);
   *p = (T *)q;
+  c->epoch++;
   return CVR_OK;
 }
 
@@ -490,11 +499,14 @@ void launch_build(cvr_ctx *c, int count_only) {
   k_bin_scatter<real><<<grid_for(n, 256), 256, 0, c->stream>>>(s);
   k_rank<real><<<grid_for(n, 256), 256, 0, c->stream>>>(s);
   k_permute<real><<<grid_for(std::max<int64_t>(n, c->ncells), 256), 256, 0, c->stream>>>(s);
-  k_build_list<real><<<grid_for(n, 128), 128, 0, c->stream>>>(s, count_only, c->log2_tpa);
+  if ((int64_t)n * 32 <= 4 * 1024 * 1024)  // small systems: one warp per atom fills the GPU
+    k_build_list_warp<real><<<grid_for((int64_t)n * 32, 128), 128, 0, c->stream>>>(s, count_only, c->log2_tpa);
+  else
+    k_build_list<real><<<grid_for(n, 128), 128, 0, c->stream>>>(s, count_only, c->log2_tpa);
   c->launches += 8;
 }
 
-template <typename real, int TPA, bool LJ, bool EWR, bool EV>
+template <typename real, int TPA, bool LJ, bool EWR, bool EV, bool ONE_TYPE>
 void launch_pair_t(cvr_ctx *c) {
   DevState<real> s = dev_state<real>(c);
   EwrArgs<real> ew;
@@ -503,7 +515,7 @@ void launch_pair_t(cvr_ctx *c) {
   ew.two_alpha_spi = (real)(2.0 * c->ewr_alpha * 0.56418958354775628695);  // 2 alpha / sqrt(pi)
   ew.cut2 = (real)(c->ewr_cut >= 0 ? c->ewr_cut * c->ewr_cut : -1.0);
   const int blocks = grid_for(c->n * TPA, 128);
-  k_pair<real, TPA, LJ, EWR, EV><<<blocks, 128, 0, c->stream>>>(
+  k_pair<real, TPA, LJ, EWR, EV, ONE_TYPE><<<blocks, 128, 0, c->stream>>>(
       s, (const PairCoef<real> *)c->d_coef, (const typename V4<real>::t *)c->d_offs, ew, c->ignore_intra,
       c->use_mol ? 1 : 0, c->ev_part);
   c->launches++;
@@ -511,10 +523,12 @@ void launch_pair_t(cvr_ctx *c) {
 
 template <typename real, bool LJ, bool EWR, bool EV>
 void launch_pair_tpa(cvr_ctx *c) {
+  // one type pair, no molecule tests: LJ constants in registers
+  const bool one = LJ && !EWR && c->n_types == 1 && !c->use_mol;
   switch (c->tpa) {
-    case 1: launch_pair_t<real, 1, LJ, EWR, EV>(c); break;
-    case 8: launch_pair_t<real, 8, LJ, EWR, EV>(c); break;
-    default: launch_pair_t<real, 32, LJ, EWR, EV>(c); break;
+    case 1: one ? launch_pair_t<real, 1, LJ, EWR, EV, true>(c) : launch_pair_t<real, 1, LJ, EWR, EV, false>(c); break;
+    case 8: one ? launch_pair_t<real, 8, LJ, EWR, EV, true>(c) : launch_pair_t<real, 8, LJ, EWR, EV, false>(c); break;
+    default: one ? launch_pair_t<real, 32, LJ, EWR, EV, true>(c) : launch_pair_t<real, 32, LJ, EWR, EV, false>(c); break;
   }
 }
 
@@ -573,11 +587,15 @@ int launch_kspace(cvr_ctx *c) {
   dim3 g1(grid_for(c->nk, 256), c->nchunks);
   k_sk_partial<real, KCH><<<g1, 256, sm1, c->stream>>>(s, a);
   k_sk_reduce<real><<<c->n_ek_blocks, 256, 0, c->stream>>>(s, a);
-  int tb = 128;
-  while (tb > 32 && (size_t)tb * 3 * c->kp * sizeof(c2) > 96 * 1024) tb /= 2;
+  const int tb = c->kf_threads;
   const size_t sm3 = (size_t)tb * 3 * c->kp * sizeof(c2);
-  k_kforce<real><<<grid_for(c->n, tb), tb, sm3, c->stream>>>(s, a);
+  dim3 g3(grid_for(c->n, tb), c->kf_slices);
+  k_kforce<real><<<g3, tb, sm3, c->stream>>>(s, a, c->kf_runs_per_slice, (real *)c->d_fpart);
   c->launches += 3;
+  if (c->kf_slices > 1) {
+    k_kforce_reduce<real><<<grid_for(c->n, 256), 256, 0, c->stream>>>(s, a, c->kf_slices, (const real *)c->d_fpart);
+    c->launches++;
+  }
   return CVR_OK;
 }
 
@@ -590,7 +608,7 @@ void set_smem_attrs(cvr_ctx *c) {
 }
 
 template <typename real>
-void launch_thermo(cvr_ctx *c, double *out, double step) {
+void launch_thermo(cvr_ctx *c, double *out) {
   ThermoArgs t{};
   t.ke_part = c->ke_part;
   t.n_ke = c->n_ke_blocks;
@@ -609,7 +627,7 @@ void launch_thermo(cvr_ctx *c, double *out, double step) {
   t.dof = 3.0 * (double)c->n - n_r_df;
   t.total_mass = c->total_mass;
   t.n_builds = c->flags + 3;
-  t.step = step;
+  t.counters = c->counters;
   t.out = out;
   k_thermo<<<1, 256, 0, c->stream>>>(t);
   c->launches++;
@@ -693,6 +711,91 @@ int snapshot(cvr_ctx *c, bool restore) {
   return CVR_OK;
 }
 
+// The kernels of one step after the position update: list build (gated by
+// the device flag), forces, second kick, optional thermo record.
+template <typename real>
+int launch_step_tail(cvr_ctx *c, bool th) {
+  DevState<real> s = dev_state<real>(c);
+  if (int r = forces_now<real>(c, th)) return r;
+  const int nb = grid_for(c->n, 256);
+  {
+    Bracket br(c, CVR_KT_INTEGRATE);
+    if (th)
+      k_kick<real, true><<<nb, 256, 0, c->stream>>>(s, c->dt, c->ke_part, c->counters);
+    else
+      k_kick<real, false><<<nb, 256, 0, c->stream>>>(s, c->dt, c->ke_part, c->counters);
+  }
+  c->launches++;
+  if (th) launch_thermo<real>(c, c->d_thermo);
+  return CVR_OK;
+}
+
+template <typename real>
+void launch_kick_drift(cvr_ctx *c) {
+  Bracket br(c, CVR_KT_INTEGRATE);
+  k_kick_drift<real><<<grid_for(c->n, 256), 256, 0, c->stream>>>(dev_state<real>(c), c->dt);
+  c->launches++;
+}
+
+void destroy_graphs(cvr_ctx *c) {
+  for (auto &g : c->g_step)
+    if (g) {
+      cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
+  c->graph_epoch = -1;
+}
+
+// One CUDA graph per step kind (plain, thermo):
+//   [kick_drift, set condition] -> IF(rebuild flag) {list build} -> [forces, kick, thermo]
+// The build nodes sit in the body of a conditional node whose value a one-thread
+// kernel sets from the device flag, so a step without a rebuild launches none
+// of them.  Kernel parameters are baked in: the graphs are rebuilt whenever a
+// device buffer moves (epoch).
+template <typename real>
+int build_graphs(cvr_ctx *c) {
+  destroy_graphs(c);
+  const int64_t launches0 = c->launches;
+  for (int th = 0; th < 2; ++th) {
+    cudaGraph_t g = nullptr, pre = nullptr, post = nullptr, body_out = nullptr;
+    CVR_CUDA(c, cudaGraphCreate(&g, 0));
+    cudaGraphConditionalHandle h;
+    CVR_CUDA(c, cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
+    CVR_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    launch_kick_drift<real>(c);
+    k_set_rebuild_condition<<<1, 1, 0, c->stream>>>(c->flags, h);
+    CVR_CUDA(c, cudaStreamEndCapture(c->stream, &pre));
+    cudaGraphNode_t n_pre, n_cond, n_post;
+    CVR_CUDA(c, cudaGraphAddChildGraphNode(&n_pre, g, nullptr, 0, pre));
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeIf;
+    cp.conditional.size = 1;
+    CVR_CUDA(c, cudaGraphAddNode(&n_cond, g, &n_pre, 1, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    CVR_CUDA(c, cudaStreamBeginCaptureToGraph(c->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    launch_build<real>(c, 0);
+    CVR_CUDA(c, cudaStreamEndCapture(c->stream, &body_out));
+    CVR_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    const int r = launch_step_tail<real>(c, th != 0);
+    CVR_CUDA(c, cudaStreamEndCapture(c->stream, &post));
+    if (r) return r;
+    CVR_CUDA(c, cudaGraphAddChildGraphNode(&n_post, g, &n_cond, 1, post));
+    CVR_CUDA(c, cudaGraphInstantiate(&c->g_step[th], g, 0));
+    cudaGraphDestroy(pre);
+    cudaGraphDestroy(post);
+    cudaGraphDestroy(g);
+  }
+  // kernels per step outside the conditional body, for the launch count
+  const int64_t captured = c->launches - launches0;  // both graphs + 8 build kernels each
+  c->launches = launches0;
+  c->graph_kernels[0] = 0;
+  (void)captured;
+  c->graph_epoch = c->epoch;
+  return CVR_OK;
+}
+
 template <typename real>
 int run_impl(cvr_ctx *c, int64_t nsteps, int64_t every, double *thermo) {
   if (!c->setup_done)
@@ -707,34 +810,32 @@ int run_impl(cvr_ctx *c, int64_t nsteps, int64_t every, double *thermo) {
   if (int r = read_flags(c, f0)) return r;
   const int64_t step0 = c->step;
   for (int attempt = 0; attempt < 4; ++attempt) {
-    DevState<real> s = dev_state<real>(c);
-    const int nb = grid_for(c->n, 256);
-    int64_t rec = 0;
+    c->counter_src[0] = step0;
+    c->counter_src[1] = 0;
+    CVR_CUDA(c, cudaMemcpyAsync(c->counters, c->counter_src, sizeof(c->counter_src), cudaMemcpyHostToDevice,
+                                c->stream));
+    const bool graphs = c->use_graphs && !c->timing;
+    if (graphs && c->graph_epoch != c->epoch)
+      if (int r = build_graphs<real>(c)) return r;
+    const int64_t launches0 = c->launches;
     for (int64_t k = 0; k < nsteps; ++k) {
       const bool th = every > 0 && ((k + 1) % every == 0);
-      {
-        Bracket br(c, CVR_KT_INTEGRATE);
-        k_kick_drift<real><<<nb, 256, 0, c->stream>>>(s, c->dt);
-      }
-      c->launches++;
-      launch_build<real>(c, 0);
-      if (int r = forces_now<real>(c, th)) return r;
-      {
-        Bracket br(c, CVR_KT_INTEGRATE);
-        if (th)
-          k_kick<real, true><<<nb, 256, 0, c->stream>>>(s, c->dt, c->ke_part);
-        else
-          k_kick<real, false><<<nb, 256, 0, c->stream>>>(s, c->dt, c->ke_part);
-      }
-      c->launches++;
-      if (th) {
-        launch_thermo<real>(c, c->d_thermo + rec * CVR_N_THERMO, (double)(step0 + k + 1));
-        ++rec;
+      if (graphs) {
+        CVR_CUDA(c, cudaGraphLaunch(c->g_step[th ? 1 : 0], c->stream));
+      } else {
+        launch_kick_drift<real>(c);
+        launch_build<real>(c, 0);
+        if (int r = launch_step_tail<real>(c, th)) return r;
       }
     }
     int f[4];
     if (int r = read_flags(c, f)) return r;
     collect_timing(c);
+    if (graphs) {
+      // kernel nodes executed: per step kick_drift + condition + tail; 8 per rebuild
+      const int tail = 1 + (c->lj_on || c->ewr_on ? 1 : 0) + ((c->ewk_on && c->nk > 0) ? (c->kf_slices > 1 ? 4 : 3) : 0);
+      c->launches = launches0 + nsteps * (2 + tail) + nrec + 8 * (int64_t)(f[3] - f0[3]);
+    }
     if (f[1] & ERR_NAN) return fail(c, CVR_ERR_NAN, "NaN acceleration");
     if (f[1] & ERR_OVERFLOW) {
       // replay the call from the snapshot with a larger list
@@ -777,7 +878,10 @@ int compute_impl(cvr_ctx *c, double *acc, double *thermo) {
     if (int r = dalloc(c, &c->d_thermo, CVR_N_THERMO)) return r;
     c->thermo_cap = 1;
   }
-  launch_thermo<real>(c, c->d_thermo, (double)c->step);
+  c->counter_src[0] = c->step;
+  c->counter_src[1] = 0;
+  CVR_CUDA(c, cudaMemcpyAsync(c->counters, c->counter_src, sizeof(c->counter_src), cudaMemcpyHostToDevice, c->stream));
+  launch_thermo<real>(c, c->d_thermo);
   CVR_CUDA(c, cudaMemcpyAsync(c->last_thermo, c->d_thermo, CVR_N_THERMO * sizeof(double), cudaMemcpyDeviceToHost,
                               c->stream));
   if (acc) {
@@ -827,6 +931,20 @@ int refresh(cvr_ctx *c) {
   if (c->ewk_on && c->nk > 0) {
     c->nchunks = grid_for(c->n, KCH);
     if (int r = dalloc(c, &c->d_kpartial, (size_t)c->nchunks * c->nk)) return r;
+    // k-force launch shape: threads per block bounded by the phase tables'
+    // shared memory, k-runs split into slices until ~8 blocks per SM exist
+    const size_t c2b = (c->precision == CVR_PREC_FP64) ? 16 : 8;
+    int tb = 128;
+    while (tb > 32 && (size_t)tb * 3 * c->kp * c2b > 96 * 1024) tb /= 2;
+    c->kf_threads = tb;
+    const int atom_blocks = grid_for(c->n, tb);
+    int slices = std::max(1, std::min(c->nruns, (8 * 148 + atom_blocks - 1) / atom_blocks));
+    c->kf_runs_per_slice = (c->nruns + slices - 1) / slices;
+    c->kf_slices = (c->nruns + c->kf_runs_per_slice - 1) / c->kf_runs_per_slice;
+    if (c->kf_slices > 1) {
+      const size_t bytes = (size_t)c->kf_slices * 3 * c->n * ((c->precision == CVR_PREC_FP64) ? 8 : 4);
+      if (int r = dalloc(c, (unsigned char **)&c->d_fpart, bytes)) return r;
+    }
     if (c->precision == CVR_PREC_FP64)
       set_smem_attrs<double>(c);
     else
@@ -906,7 +1024,7 @@ int cvr_create(cvr_ctx **out, const double lo[3], const double hi[3], const int 
     delete c;
     return CVR_ERR_CUDA;
   }
-  if (dalloc(c, &c->flags, 4) != CVR_OK) {
+  if (dalloc(c, &c->flags, 4) != CVR_OK || dalloc(c, &c->counters, 2) != CVR_OK) {
     cudaStreamDestroy(c->stream);
     delete c;
     return CVR_ERR_NOMEM;
@@ -919,6 +1037,7 @@ void cvr_destroy(cvr_ctx *c) {
   if (!c) return;
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
+  destroy_graphs(c);
   for (void *p : c->all_allocs) cudaFree(p);
   for (auto &k : c->kt)
     for (auto &e : k.ev) {

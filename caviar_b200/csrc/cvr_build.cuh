@@ -219,7 +219,7 @@ __global__ void k_permute(DevState<real> s) {
   else
     q.w = (double)ty;
   s.x4[k] = q;
-  s.xb[k] = make_float4((float)loc[0], (float)loc[1], (float)loc[2], 0.f);
+  s.xb[k] = make_float4((float)loc[0], (float)loc[1], (float)loc[2], __int_as_float(cc[0]));
   s.gcls[k] = (int8_t)code;
 }
 
@@ -250,8 +250,114 @@ __device__ __forceinline__ bool has_image(int gcode, const int sh[3]) {
   return true;
 }
 
+// One candidate of the pair search: FP32 prefilter on cell-local
+// coordinates, exact FP64 reference test near the threshold.
+template <typename real>
+__device__ __forceinline__ bool in_list(const DevState<real> &s, int i, const float4 &xi, const double (&pi)[3],
+                                        int gi, int j, const float4 &xj, int dx, int dy, int dz, int sx, int sy,
+                                        int sz) {
+  const bool shifted = (sx | sy | sz) != 0;
+  if (j == i && !shifted) return false;
+  const float ddx = (xj.x - xi.x) + dx * (float)s.cells.w[0];
+  const float ddy = (xj.y - xi.y) + dy * (float)s.cells.w[1];
+  const float ddz = (xj.z - xi.z) + dz * (float)s.cells.w[2];
+  const float d2 = ddx * ddx + ddy * ddy + ddz * ddz;
+  if (!(d2 < s.rl_sq_hi)) return false;
+  const int sh[3] = {sx, sy, sz};
+  if (!shifted) {
+    if (d2 <= s.rl_sq_lo) return true;
+    const double pj[3] = {s.x[j], s.y[j], s.z[j]};
+    return exact_within(pi, pj, sh, s.box, s.rl_sq);
+  }
+  const int gj = s.gcls[j];
+  const int msh[3] = {-sx, -sy, -sz};
+  const bool img_j = has_image(gj, sh);   // reference ghost of j at r_j + sL
+  const bool img_i = has_image(gi, msh);  // reference ghost of i at r_i - sL
+  if (!img_j && !img_i) return false;
+  if (d2 <= s.rl_sq_lo) return true;
+  const double pj[3] = {s.x[j], s.y[j], s.z[j]};
+  return (img_j && exact_within(pi, pj, sh, s.box, s.rl_sq)) || (img_i && exact_within(pj, pi, msh, s.box, s.rl_sq));
+}
+
+__device__ __forceinline__ uint32_t list_entry(int j, int dx, int dy, int dz, int R, int S) {
+  const uint32_t code = (uint32_t)((dx + R) + S * ((dy + R) + S * (dz + R)));
+  return (uint32_t)j | (code << CODE_SHIFT);
+}
+
+template <typename real>
+__device__ __forceinline__ void consider(const DevState<real> &s, int i, const float4 &xi, const double (&pi)[3],
+                                         int gi, int j, const float4 &xj, int dx, int dy, int dz, int sx, int sy,
+                                         int sz, int &cnt, uint32_t *row, size_t stride, int log2_tpa, int count_only) {
+  if (in_list(s, i, xi, pi, gi, j, xj, dx, dy, dz, sx, sy, sz)) {
+    if (!count_only && cnt < s.cap)
+      row[(size_t)(cnt >> log2_tpa) * stride + (cnt & ((1 << log2_tpa) - 1))] =
+          list_entry(j, dx, dy, dz, s.cells.R, s.cells.S);
+    ++cnt;
+  }
+}
+
+// The same search with one WARP per atom, for systems too small to fill the
+// GPU with one thread per atom: the 32 lanes take consecutive candidates of a
+// stencil row, and a ballot keeps the accepted ones in candidate order, so
+// the list is identical to the one-thread-per-atom build.
+template <typename real>
+__global__ void __launch_bounds__(128) k_build_list_warp(DevState<real> s, int count_only, int log2_tpa) {
+  if (*s.flag == 0) return;
+  if (blockIdx.x == 0 && threadIdx.x == 0 && !count_only) atomicAdd(s.n_builds, 1);
+  const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (i >= s.n) return;  // whole warp leaves together
+  int cx, cy, cz;
+  cell_xyz(s, s.cell[i], cx, cy, cz);
+  const float4 xi = s.xb[i];
+  const double pi[3] = {s.x[i], s.y[i], s.z[i]};
+  const int gi = s.gcls[i];
+  const int R = s.cells.R, S = s.cells.S;
+  const size_t stride = (size_t)s.n_pad << log2_tpa;
+  uint32_t *row = s.nlist + ((size_t)i << log2_tpa);
+  const int nc0 = s.cells.nc[0], nc1 = s.cells.nc[1], nc2 = s.cells.nc[2];
+  const unsigned lt = (1u << lane) - 1u;
+  int cnt = 0;
+  for (int dz = -R; dz <= R; ++dz) {
+    const int sz = floor_div(cz + dz, nc2);
+    if (sz != 0 && !s.box.bc[2]) continue;
+    const int jz = cz + dz - sz * nc2;
+    for (int dy = -R; dy <= R; ++dy) {
+      const int sy = floor_div(cy + dy, nc1);
+      if (sy != 0 && !s.box.bc[1]) continue;
+      const int jy = cy + dy - sy * nc1;
+      const int rowbase = nc0 * (jy + nc1 * jz);
+      for (int dx = -R; dx <= R; ++dx) {
+        const int sx = floor_div(cx + dx, nc0);
+        if (sx != 0 && !s.box.bc[0]) continue;
+        const int cj = cx + dx - sx * nc0 + rowbase;
+        const int jb = s.cell_start[cj], je = s.cell_start[cj + 1];
+        for (int base = jb; base < je; base += 32) {
+          const int j = base + lane;
+          const bool ok = (j < je) && in_list(s, i, xi, pi, gi, j, s.xb[min(j, je - 1)], dx, dy, dz, sx, sy, sz);
+          const unsigned m = __ballot_sync(0xffffffffu, ok);
+          if (ok && !count_only) {
+            const int k = cnt + __popc(m & lt);
+            if (k < s.cap) row[(size_t)(k >> log2_tpa) * stride + (k & ((1 << log2_tpa) - 1))] = list_entry(j, dx, dy, dz, R, S);
+          }
+          cnt += __popc(m);
+        }
+      }
+    }
+  }
+  if (lane == 0) {
+    if (!count_only) s.ncount[i] = min(cnt, s.cap);
+    if (!count_only && cnt > s.cap) atomicOr(s.err, ERR_OVERFLOW);
+    atomicMax(s.max_count, cnt);
+  }
+}
+
 // Pass 5: the pair search, one thread per atom over the (2R+1)^3 stencil.
-// count_only = 1 only counts (used to size the list before the first build).
+// Each stencil row (fixed dy, dz) is at most two contiguous atom ranges (a
+// periodic wrap in x splits it); candidates are read four at a time, and a
+// candidate's cell x index comes from xb.w.  Rows of boxes narrower than the
+// stencil (nc_x < 2R+1) take the cell-by-cell path.  count_only = 1 only
+// counts (used to size the list before the first build).
 template <typename real>
 __global__ void __launch_bounds__(128) k_build_list(DevState<real> s, int count_only, int log2_tpa) {
   if (*s.flag == 0) return;
@@ -265,10 +371,10 @@ __global__ void __launch_bounds__(128) k_build_list(DevState<real> s, int count_
     const double pi[3] = {s.x[i], s.y[i], s.z[i]};
     const int gi = s.gcls[i];
     const int R = s.cells.R, S = s.cells.S;
-    const int tpa = 1 << log2_tpa;
     const size_t stride = (size_t)s.n_pad << log2_tpa;
     uint32_t *row = s.nlist + ((size_t)i << log2_tpa);
     const int nc0 = s.cells.nc[0], nc1 = s.cells.nc[1], nc2 = s.cells.nc[2];
+    const bool rows = nc0 >= S;
     for (int dz = -R; dz <= R; ++dz) {
       const int sz = floor_div(cz + dz, nc2);
       if (sz != 0 && !s.box.bc[2]) continue;
@@ -277,50 +383,42 @@ __global__ void __launch_bounds__(128) k_build_list(DevState<real> s, int count_
         const int sy = floor_div(cy + dy, nc1);
         if (sy != 0 && !s.box.bc[1]) continue;
         const int jy = cy + dy - sy * nc1;
-        for (int dx = -R; dx <= R; ++dx) {
-          const int sx = floor_div(cx + dx, nc0);
-          if (sx != 0 && !s.box.bc[0]) continue;
-          const int jx = cx + dx - sx * nc0;
-          const int cj = jx + nc0 * (jy + nc1 * jz);
-          const uint32_t code = (uint32_t)((dx + R) + S * ((dy + R) + S * (dz + R)));
-          const float ox = dx * (float)s.cells.w[0], oy = dy * (float)s.cells.w[1], oz = dz * (float)s.cells.w[2];
-          const int sh[3] = {sx, sy, sz};
-          const bool shifted = (sx | sy | sz) != 0;
-          const int jb = s.cell_start[cj], je = s.cell_start[cj + 1];
-          for (int j = jb; j < je; ++j) {
-            if (j == i && !shifted) continue;
-            const float4 xj = s.xb[j];
-            const float ddx = (xj.x - xi.x) + ox, ddy = (xj.y - xi.y) + oy, ddz = (xj.z - xi.z) + oz;
-            const float d2 = ddx * ddx + ddy * ddy + ddz * ddz;
-            if (!(d2 < s.rl_sq_hi)) continue;
-            bool inc;
-            if (!shifted) {
-              if (d2 <= s.rl_sq_lo) {
-                inc = true;
-              } else {
-                const double pj[3] = {s.x[j], s.y[j], s.z[j]};
-                inc = exact_within(pi, pj, sh, s.box, s.rl_sq);
-              }
-            } else {
-              const int gj = s.gcls[j];
-              const int msh[3] = {-sx, -sy, -sz};
-              const bool img_j = has_image(gj, sh);   // reference ghost of j at r_j + sL
-              const bool img_i = has_image(gi, msh);  // reference ghost of i at r_i - sL
-              if (!img_j && !img_i) {
-                inc = false;
-              } else if (d2 <= s.rl_sq_lo) {
-                inc = true;
-              } else {
-                const double pj[3] = {s.x[j], s.y[j], s.z[j]};
-                inc = (img_j && exact_within(pi, pj, sh, s.box, s.rl_sq)) ||
-                      (img_i && exact_within(pj, pi, msh, s.box, s.rl_sq));
-              }
+        const int rowbase = nc0 * (jy + nc1 * jz);
+        if (rows) {
+          // unwrapped x range [cx-R, cx+R] = part with sx=-1, sx=0, sx=+1
+          for (int sx = -1; sx <= 1; ++sx) {
+            int ua = cx - R, ub = cx + R;
+            if (sx < 0) ub = min(ub, -1);
+            if (sx == 0) {
+              ua = max(ua, 0);
+              ub = min(ub, nc0 - 1);
             }
-            if (inc) {
-              if (!count_only && cnt < s.cap)
-                row[(size_t)(cnt >> log2_tpa) * stride + (cnt & (tpa - 1))] = (uint32_t)j | (code << CODE_SHIFT);
-              ++cnt;
+            if (sx > 0) ua = max(ua, nc0);
+            if (ua > ub) continue;
+            if (sx != 0 && !s.box.bc[0]) continue;
+            const int jb = s.cell_start[rowbase + ua - sx * nc0];
+            const int je = s.cell_start[rowbase + ub - sx * nc0 + 1];
+            const int xoff = sx * nc0 - cx;  // dx = cell_x(j) + xoff
+            for (int j = jb; j < je; j += 4) {
+              float4 q[4];
+#pragma unroll
+              for (int u = 0; u < 4; ++u) q[u] = (j + u < je) ? s.xb[j + u] : xi;
+#pragma unroll
+              for (int u = 0; u < 4; ++u)
+                if (j + u < je)
+                  consider(s, i, xi, pi, gi, j + u, q[u], __float_as_int(q[u].w) + xoff, dy, dz, sx, sy, sz, cnt, row,
+                           stride, log2_tpa, count_only);
             }
+          }
+        } else {
+          for (int dx = -R; dx <= R; ++dx) {
+            const int sx = floor_div(cx + dx, nc0);
+            if (sx != 0 && !s.box.bc[0]) continue;
+            const int jx = cx + dx - sx * nc0;
+            const int cj = jx + rowbase;
+            const int jb = s.cell_start[cj], je = s.cell_start[cj + 1];
+            for (int j = jb; j < je; ++j)
+              consider(s, i, xi, pi, gi, j, s.xb[j], dx, dy, dz, sx, sy, sz, cnt, row, stride, log2_tpa, count_only);
           }
         }
       }

@@ -69,17 +69,58 @@ template <typename real> struct EwrArgs {
 // --------------------------------------------------------------- pair force
 // TPA lanes per atom stride through the atom's list row; lanes reduce with
 // shuffles.  use_mol enables the molecule tests (ignore_intra_molecule,
-// Ewald lambda).  EV adds energies + virial (FP64 per thread, FP64 block sums into
-// partials[block*3 + {e_lj, e_ewr, virial}]).
-template <typename real, int TPA, bool LJ, bool EWR, bool EV>
+// Ewald lambda).  ONE_TYPE keeps the single type pair's LJ constants in
+// registers (no table lookups).  The LJ cutoff is a select, not a branch.
+// EV adds energies + virial (FP64 per thread, FP64 block sums into
+// partials[block*3 + {e_lj, e_ewr, virial}]).  Entries are unrolled by two
+// so that two neighbour gathers are in flight per lane.
+template <typename real> struct PairAcc {
+  real fx, fy, fz;
+  double e_lj, e_ew, vir;
+};
+
+template <typename real, bool LJ, bool EWR, bool EV>
+__device__ __forceinline__ void pair_term(PairAcc<real> &A, real dx, real dy, real dz, const PairCoef<real> &pc,
+                                          bool same_mol, int ignore_intra, const EwrArgs<real> &ew) {
+  const real r2 = dx * dx + dy * dy + dz * dz;
+  real c = 0;
+  if (LJ) {
+    // lj.cpp:417-448: skip r^2 > rc^2 (rc2 < 0 when eps = 0)
+    const real r2i = fast_rcp(r2);
+    const real s2 = pc.sig2 * r2i;
+    const real s6 = s2 * s2 * s2;
+    const bool in = (r2 <= pc.rc2) && !(same_mol && ignore_intra);
+    const real cl = r2i * s6 * (pc.eps24 - pc.eps48 * s6) + pc.K;
+    c = in ? cl : (real)0;
+    if (EV && in) A.e_lj += (double)(pc.e4 * (s6 * s6 - s6) + pc.C1 * r2 + pc.C0);
+  }
+  if (EWR) {
+    // electrostatic_ewald_r.cpp:179-198: every list pair, coincident skipped
+    if (r2 > (real)0 && (ew.cut2 < (real)0 || r2 <= ew.cut2)) {
+      const real rinv = fast_rsqrt(r2);
+      const real r = r2 * rinv;
+      const real erfcv = erfc_r(ew.alpha * r);
+      const real sv = (ew.two_alpha_spi * fast_exp(-ew.alpha2 * r2) + erfcv * rinv) * (rinv * rinv);
+      const real lam = same_mol ? pc.lam : (real)1;
+      c -= lam * pc.qq * sv;
+      if (EV) A.e_ew += (double)(lam * pc.qq * erfcv * rinv);
+    }
+  }
+  A.fx += c * dx;
+  A.fy += c * dy;
+  A.fz += c * dz;
+  if (EV) A.vir -= (double)(c * r2);
+}
+
+template <typename real, int TPA, bool LJ, bool EWR, bool EV, bool ONE_TYPE>
 __global__ void __launch_bounds__(128) k_pair(DevState<real> s, const PairCoef<real> *__restrict__ coef_g,
                                               const typename V4<real>::t *__restrict__ offs_g, EwrArgs<real> ew,
                                               int ignore_intra, int use_mol, double *__restrict__ partials) {
   using real4 = typename V4<real>::t;
-  __shared__ PairCoef<real> coef[MAX_TYPES * MAX_TYPES];
+  __shared__ PairCoef<real> coef[ONE_TYPE ? 1 : MAX_TYPES * MAX_TYPES];
   __shared__ real4 offs[125];
   const int T = s.n_types;
-  for (int t = threadIdx.x; t < T * T; t += blockDim.x) coef[t] = coef_g[t];
+  for (int t = threadIdx.x; t < (ONE_TYPE ? 1 : T * T); t += blockDim.x) coef[t] = coef_g[t];
   for (int t = threadIdx.x; t < s.cells.S * s.cells.S * s.cells.S; t += blockDim.x) offs[t] = offs_g[t];
   __syncthreads();
   if (*s.err) return;
@@ -87,72 +128,59 @@ __global__ void __launch_bounds__(128) k_pair(DevState<real> s, const PairCoef<r
   const int gid = blockIdx.x * blockDim.x + threadIdx.x;
   const int i = gid / TPA, lane = gid % TPA;
   const bool valid = i < s.n;
-  real fx = 0, fy = 0, fz = 0;
-  double e_lj = 0, e_ew = 0, vir = 0;
+  PairAcc<real> A{0, 0, 0, 0.0, 0.0, 0.0};
   int ti = 0;
   if (valid) {
     const real4 xi = s.x4[i];
     ti = type_of(xi.w);
     const int moli = use_mol ? s.mol[i] : 0;
     const int cnt = s.ncount[i];
-    const uint32_t *row = s.nlist + (size_t)i * TPA + lane;
     const size_t stride = (size_t)s.n_pad * TPA;
-    const PairCoef<real> *ci = coef + ti * T;
-    for (int k = lane, it = 0; k < cnt; k += TPA, ++it) {
-      const uint32_t e = __ldg(row + (size_t)it * stride);
-      const int j = (int)(e & INDEX_MASK);
-      const real4 o = offs[e >> CODE_SHIFT];
-      const real4 xj = s.x4[j];
-      const real dx = (xj.x - xi.x) + o.x;
-      const real dy = (xj.y - xi.y) + o.y;
-      const real dz = (xj.z - xi.z) + o.z;
-      const real r2 = dx * dx + dy * dy + dz * dz;
-      const int tj = type_of(xj.w);
-      const PairCoef<real> &pc = ci[tj];
-      const bool same_mol = use_mol && (moli == s.mol[j]);
-      real c = 0;
-      if (LJ) {
-        // lj.cpp:417-448: skip r^2 > rc^2 (rc2 < 0 when eps = 0 or excluded)
-        if (r2 <= pc.rc2 && !(same_mol && ignore_intra)) {
-          const real r2i = fast_rcp(r2);
-          const real s2 = pc.sig2 * r2i;
-          const real s6 = s2 * s2 * s2;
-          c = r2i * s6 * (pc.eps24 - pc.eps48 * s6) + pc.K;
-          if (EV) e_lj += (double)(pc.e4 * (s6 * s6 - s6) + pc.C1 * r2 + pc.C0);
-        }
-      }
-      if (EWR) {
-        // electrostatic_ewald_r.cpp:179-198: every list pair, coincident skipped
-        if (r2 > (real)0 && (ew.cut2 < (real)0 || r2 <= ew.cut2)) {
-          const real rinv = fast_rsqrt(r2);
-          const real r = r2 * rinv;
-          const real erfcv = erfc_r(ew.alpha * r);
-          const real sv = (ew.two_alpha_spi * fast_exp(-ew.alpha2 * r2) + erfcv * rinv) * (rinv * rinv);
-          const real lam = same_mol ? pc.lam : (real)1;
-          c -= lam * pc.qq * sv;
-          if (EV) e_ew += (double)(lam * pc.qq * erfcv * rinv);
-        }
-      }
-      fx += c * dx;
-      fy += c * dy;
-      fz += c * dz;
-      if (EV) vir -= (double)(c * r2);
+    const uint32_t *row = s.nlist + (size_t)i * TPA + lane;
+    const PairCoef<real> *ci = coef + (ONE_TYPE ? 0 : ti * T);
+    PairCoef<real> c1;
+    if (ONE_TYPE) c1 = coef[0];
+    int k = lane;
+    for (; k + TPA < cnt; k += 2 * TPA) {
+      const uint32_t e0 = __ldcs(row);
+      const uint32_t e1 = __ldcs(row + stride);
+      row += 2 * stride;
+      const int j0 = (int)(e0 & INDEX_MASK), j1 = (int)(e1 & INDEX_MASK);
+      const real4 xj0 = s.x4[j0];
+      const real4 xj1 = s.x4[j1];
+      const real4 o0 = offs[e0 >> CODE_SHIFT];
+      const real4 o1 = offs[e1 >> CODE_SHIFT];
+      const bool sm0 = use_mol && (moli == s.mol[j0]);
+      const bool sm1 = use_mol && (moli == s.mol[j1]);
+      pair_term<real, LJ, EWR, EV>(A, (xj0.x - xi.x) + o0.x, (xj0.y - xi.y) + o0.y, (xj0.z - xi.z) + o0.z,
+                                   ONE_TYPE ? c1 : ci[type_of(xj0.w)], sm0, ignore_intra, ew);
+      pair_term<real, LJ, EWR, EV>(A, (xj1.x - xi.x) + o1.x, (xj1.y - xi.y) + o1.y, (xj1.z - xi.z) + o1.z,
+                                   ONE_TYPE ? c1 : ci[type_of(xj1.w)], sm1, ignore_intra, ew);
+    }
+    if (k < cnt) {
+      const uint32_t e0 = __ldcs(row);
+      const int j0 = (int)(e0 & INDEX_MASK);
+      const real4 xj0 = s.x4[j0];
+      const real4 o0 = offs[e0 >> CODE_SHIFT];
+      const bool sm0 = use_mol && (moli == s.mol[j0]);
+      pair_term<real, LJ, EWR, EV>(A, (xj0.x - xi.x) + o0.x, (xj0.y - xi.y) + o0.y, (xj0.z - xi.z) + o0.z,
+                                   ONE_TYPE ? c1 : ci[type_of(xj0.w)], sm0, ignore_intra, ew);
     }
   }
 #pragma unroll
   for (int o = TPA / 2; o > 0; o >>= 1) {
-    fx += __shfl_xor_sync(0xffffffffu, fx, o);
-    fy += __shfl_xor_sync(0xffffffffu, fy, o);
-    fz += __shfl_xor_sync(0xffffffffu, fz, o);
+    A.fx += __shfl_xor_sync(0xffffffffu, A.fx, o);
+    A.fy += __shfl_xor_sync(0xffffffffu, A.fy, o);
+    A.fz += __shfl_xor_sync(0xffffffffu, A.fz, o);
   }
   if (valid && lane == 0) {
     const real mi = (real)s.mass_inv[ti];
-    s.ax[i] = fx * mi;
-    s.ay[i] = fy * mi;
-    s.az[i] = fz * mi;
+    s.ax[i] = A.fx * mi;
+    s.ay[i] = A.fy * mi;
+    s.az[i] = A.fz * mi;
   }
   if (EV) {
-    double v[3] = {0.5 * e_lj, 0.5 * e_ew, 0.5 * vir};  // full list: each pair twice
+    double v[3] = {0.5 * A.e_lj, 0.5 * A.e_ew, 0.5 * A.vir};  // full list: each pair twice
     block_sum_store<3>(v, partials);
   }
 }
@@ -210,7 +238,8 @@ __device__ __forceinline__ T conj_if(T a, bool c) {
 }
 
 // S(k) partial sums: one thread per k-vector, one block row per chunk of
-// KCH atoms whose phase tables sit in shared memory.  FP64 accumulation.
+// KCH atoms whose phase tables sit in shared memory.  Products are summed in
+// `real` over groups of 16 atoms; groups and chunks accumulate in FP64.
 template <typename real, int KCH>
 __global__ void __launch_bounds__(256) k_sk_partial(DevState<real> s, KArgs<real> a) {
   using c2 = typename R2<real>::t;
@@ -244,14 +273,21 @@ __global__ void __launch_bounds__(256) k_sk_partial(DevState<real> s, KArgs<real
   const int mx = abs(kn.x), my = abs(kn.y), mz = abs(kn.z);
   double sr = 0, si = 0;
   const int na = min(KCH, s.n - a0);
-  for (int t = 0; t < na; ++t) {
-    const c2 *tb = tab + t * 3 * kp;
-    const c2 px = conj_if(tb[mx], kn.x < 0);
-    const c2 py = conj_if(tb[kp + my], kn.y < 0);
-    const c2 pz = conj_if(tb[2 * kp + mz], kn.z < 0);
-    const c2 p = cmul(cmul(px, py), pz);
-    sr += (double)(q[t] * p.x);
-    si += (double)(q[t] * p.y);
+  for (int t0 = 0; t0 < na; t0 += 16) {
+    // products in `real`, summed over 16 atoms, then accumulated in FP64
+    real pr = 0, pim = 0;
+    const int t1 = min(na, t0 + 16);
+    for (int t = t0; t < t1; ++t) {
+      const c2 *tb = tab + t * 3 * kp;
+      const c2 px = conj_if(tb[mx], kn.x < 0);
+      const c2 py = conj_if(tb[kp + my], kn.y < 0);
+      const c2 pz = conj_if(tb[2 * kp + mz], kn.z < 0);
+      const c2 p = cmul(cmul(px, py), pz);
+      pr += q[t] * p.x;
+      pim += q[t] * p.y;
+    }
+    sr += (double)pr;
+    si += (double)pim;
   }
   a.partial[(size_t)chunk * a.nk + k] = make_double2(sr, si);
 }
@@ -283,11 +319,16 @@ __global__ void __launch_bounds__(256) k_sk_reduce(DevState<real> s, KArgs<real>
   block_sum_store<1>(v, a.e_partials);
 }
 
-// k-space force: one thread per atom, its own phase table in shared memory,
-// runs of nz at fixed (nx, ny) so each k costs one complex multiply.
-// F_i = k_e q_i sum_k k Im(A_k e^{i k.r_i}) (electrostatic_ewald_k.cpp:215-218).
+// k-space force: one thread per atom, one block column per slice of the
+// k-runs (so a few thousand atoms still fill the GPU), the atom's phase
+// table in shared memory, runs of nz at fixed (nx, ny) so each k costs one
+// complex multiply.  F_i = k_e q_i sum_k k Im(A_k e^{i k.r_i})
+// (electrostatic_ewald_k.cpp:215-218).  With one slice the kernel adds into
+// the accelerations; with several it writes per-slice sums that
+// k_kforce_reduce adds in slice order (deterministic).
 template <typename real>
-__global__ void __launch_bounds__(128) k_kforce(DevState<real> s, KArgs<real> a) {
+__global__ void __launch_bounds__(128) k_kforce(DevState<real> s, KArgs<real> a, int runs_per_slice,
+                                                real *__restrict__ fpart) {
   using c2 = typename R2<real>::t;
   extern __shared__ unsigned char smem_raw[];
   const int kp = a.kp;
@@ -298,8 +339,10 @@ __global__ void __launch_bounds__(128) k_kforce(DevState<real> s, KArgs<real> a)
   const double pd[3] = {s.x[i], s.y[i], s.z[i]};
   for (int d = 0; d < 3; ++d)
     for (int m = 0; m <= a.kmax[d]; ++m) tab[d * kp + m] = phase<real>(pd[d] * a.inv_L[d], m);
+  const int r0 = blockIdx.y * runs_per_slice;
+  const int r1 = min(a.nruns, r0 + runs_per_slice);
   real fx = 0, fy = 0, fz = 0;
-  for (int r = 0; r < a.nruns; ++r) {
+  for (int r = r0; r < r1; ++r) {
     const KRun run = a.runs[r];
     const c2 pxy = cmul(conj_if(tab[abs(run.nx)], run.nx < 0), conj_if(tab[kp + abs(run.ny)], run.ny < 0));
     real tsum = 0;
@@ -313,6 +356,34 @@ __global__ void __launch_bounds__(128) k_kforce(DevState<real> s, KArgs<real> a)
     }
     fx += (real)run.nx * tsum;
     fy += (real)run.ny * tsum;
+  }
+  if (gridDim.y == 1) {
+    const int ti = s.type[i];
+    const real qm = (real)(a.k_e * a.charge[ti] * s.mass_inv[ti]);
+    s.ax[i] += qm * a.two_pi_over_L[0] * fx;
+    s.ay[i] += qm * a.two_pi_over_L[1] * fy;
+    s.az[i] += qm * a.two_pi_over_L[2] * fz;
+  } else {
+    const size_t n = (size_t)s.n, b = (size_t)blockIdx.y * 3 * n;
+    fpart[b + i] = fx;
+    fpart[b + n + i] = fy;
+    fpart[b + 2 * n + i] = fz;
+  }
+}
+
+template <typename real>
+__global__ void __launch_bounds__(256) k_kforce_reduce(DevState<real> s, KArgs<real> a, int nslices,
+                                                       const real *__restrict__ fpart) {
+  if (*s.err) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= s.n) return;
+  const size_t n = (size_t)s.n;
+  real fx = 0, fy = 0, fz = 0;
+  for (int sl = 0; sl < nslices; ++sl) {
+    const size_t b = (size_t)sl * 3 * n;
+    fx += fpart[b + i];
+    fy += fpart[b + n + i];
+    fz += fpart[b + 2 * n + i];
   }
   const int ti = s.type[i];
   const real qm = (real)(a.k_e * a.charge[ti] * s.mass_inv[ti]);
@@ -372,10 +443,15 @@ __global__ void __launch_bounds__(256) k_kick_drift(DevState<real> s, double dt)
 }
 
 // Second half kick; KE partials (sum m v^2, sum m v) when KE.  Also clears
-// the step's rebuild flag: every reader of it has run by now.
+// the step's rebuild flag (every reader of it has run by now) and counts the
+// step in counters[0].
 template <typename real, bool KE>
-__global__ void __launch_bounds__(256) k_kick(DevState<real> s, double dt, double *__restrict__ partials) {
-  if (blockIdx.x == 0 && threadIdx.x == 0) *s.flag = 0;
+__global__ void __launch_bounds__(256) k_kick(DevState<real> s, double dt, double *__restrict__ partials,
+                                              long long *__restrict__ counters) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    *s.flag = 0;
+    if (counters) counters[0]++;
+  }
   if (*s.err) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double v[4] = {0, 0, 0, 0};
@@ -396,6 +472,12 @@ __global__ void __launch_bounds__(256) k_kick(DevState<real> s, double dt, doubl
     }
   }
   if (KE) block_sum_store<4>(v, partials);
+}
+
+// Sets the step graph's IF condition from the device rebuild flag: the list
+// build nodes run only on steps that need them.
+__global__ void k_set_rebuild_condition(const int *__restrict__ flag, cudaGraphConditionalHandle h) {
+  cudaGraphSetConditional(h, (*flag != 0) ? 1u : 0u);
 }
 
 // KE partials without moving anything (thermo outside the step loop).
@@ -454,8 +536,8 @@ struct ThermoArgs {
   double total_mass, dof, volume, k_b, n_atoms, ek_coef, e_self;
   int com_removed;
   const int *n_builds;
-  double step;
-  double *out;  // CVR_N_THERMO doubles
+  long long *counters;  // [0] steps done, [1] next thermo record
+  double *out;          // base of the records, CVR_N_THERMO doubles each
 };
 
 __global__ void __launch_bounds__(256) k_thermo(ThermoArgs a) {
@@ -474,6 +556,8 @@ __global__ void __launch_bounds__(256) k_thermo(ThermoArgs a) {
     __syncthreads();
   }
   if (threadIdx.x == 0) {
+    const long long rec = a.counters[1]++;
+    double *out = a.out + rec * 10;
     const double mv2 = acc[0][0];
     double ke = 0.5 * mv2;
     if (a.com_removed && a.total_mass > 0) {
@@ -482,16 +566,16 @@ __global__ void __launch_bounds__(256) k_thermo(ThermoArgs a) {
     }
     const double temp = (a.dof > 0) ? 2.0 * ke / (a.k_b * a.dof) : 0.0;
     const double vir = acc[6][0];
-    a.out[0] = a.step;
-    a.out[1] = ke;
-    a.out[2] = temp;
-    a.out[3] = acc[4][0];
-    a.out[4] = acc[5][0];
-    a.out[5] = a.ek_coef * acc[7][0];
-    a.out[6] = a.e_self;
-    a.out[7] = vir;
-    a.out[8] = a.n_atoms * a.k_b * temp / a.volume + vir / (3.0 * a.volume);
-    a.out[9] = (double)(*a.n_builds);
+    out[0] = (double)a.counters[0];
+    out[1] = ke;
+    out[2] = temp;
+    out[3] = acc[4][0];
+    out[4] = acc[5][0];
+    out[5] = a.ek_coef * acc[7][0];
+    out[6] = a.e_self;
+    out[7] = vir;
+    out[8] = a.n_atoms * a.k_b * temp / a.volume + vir / (3.0 * a.volume);
+    out[9] = (double)(*a.n_builds);
   }
 }
 

@@ -185,3 +185,25 @@ def test_list_overflow_regrows(cuda_lib, oracle_lib):
     o = oracle_lib.Oracle(s2)
     o.build_list()
     assert np.array_equal(sim.pairs(), o.pairs())
+
+
+def test_graph_and_stream_paths_agree(cuda_lib):
+    """cvr_run replays one CUDA graph per step (list build in a conditional
+    node); with kernel timing on it launches the same kernels on the stream.
+    Both must give the same trajectory and thermo records, bit for bit."""
+    from caviar_b200 import workloads as W
+    s = W.fcc_lattice(8, 0.8442, 0.72, seed=5, jitter=0.05)
+    a = sim_for(cuda_lib, s, "mixed")
+    th_a = a.run(60, 10)
+    b = sim_for(cuda_lib, s, "mixed")
+    b.set_kernel_timing(True)
+    th_b = b.run(60, 10)
+    for x, y in zip(a.state(), b.state()):
+        assert np.array_equal(x, y)
+    assert np.array_equal(th_a, th_b)
+    assert a.info()["builds"] == b.info()["builds"] > 1
+    # thermo records: step numbers, and the last KE equals the state's
+    assert th_a[:, 0].tolist() == [10, 20, 30, 40, 50, 60]
+    _, vel, _ = a.state()
+    v = vel - vel.mean(axis=0)
+    assert abs(th_a[-1, 1] - 0.5 * np.sum(v * v)) < 1e-10 * th_a[-1, 1]
