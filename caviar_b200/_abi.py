@@ -12,7 +12,7 @@ from typing import Optional
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libcaviar_b200.so")
+LIB_PATH = os.environ.get("CAVIAR_B200_LIB", os.path.join(HERE, "libcaviar_b200.so"))
 
 OK = 0
 ERR = {1: "INVALID", 2: "CUDA", 3: "NAN", 4: "STATE", 5: "GEOMETRY", 6: "CAPACITY", 7: "NOMEM"}

@@ -186,6 +186,8 @@ DevState<real> dev_state(cvr_ctx *c) {
     s.box.gclo[d] = c->lo[d] + c->gc;  // x_llow = lower_global.x + ghost_cutoff
     s.box.gchi[d] = c->hi[d] - c->gc;  // x_lupp = upper_global.x - ghost_cutoff
     s.box.bc[d] = c->bc[d];
+    s.box.ctr[d] = c->lo[d] + 0.5 * c->L[d];
+    s.box.Lf[d] = (float)c->L[d];
     s.cells.nc[d] = c->nc[d];
     s.cells.w[d] = c->w[d];
     s.cells.inv_w[d] = 1.0 / c->w[d];
@@ -195,8 +197,16 @@ DevState<real> dev_state(cvr_ctx *c) {
   s.cells.S = 2 * c->R + 1;
   const double rl = c->cutoff * c->coef;  // cutoff_extra = cutoff * cutoff_extra_coef
   s.rl_sq = rl * rl;
-  s.rl_sq_lo = (float)(s.rl_sq * (1.0 - 1e-5));
-  s.rl_sq_hi = (float)(s.rl_sq * (1.0 + 1e-5));
+  // Guard band of the FP32 prefilter: each box-centred FP32 coordinate is off
+  // by at most 2^-24 (|L|/2 + rl) after rounding, a difference by twice that,
+  // so |d|^2 is off by at most 2 rl sqrt(3) (2 eps); the band is 16x that
+  // bound (and never below 1e-5 relative).
+  double half = 0;
+  for (int d = 0; d < 3; ++d) half = std::max(half, 0.5 * c->L[d] + rl);
+  const double eps_coord = 2.0 * std::ldexp(half, -24);
+  const double band = std::max(1e-5, 16.0 * 2.0 * rl * std::sqrt(3.0) * eps_coord / (rl * rl));
+  s.rl_sq_lo = (float)(s.rl_sq * (1.0 - band));
+  s.rl_sq_hi = (float)(s.rl_sq * (1.0 + band));
   const double half_skin = 0.5 * (rl - c->cutoff);  // threshold_distance_sq = 0.25 (rl - rc)^2
   s.thr_sq = (float)(half_skin * half_skin);
   s.x = c->x;

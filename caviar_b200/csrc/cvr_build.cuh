@@ -23,6 +23,15 @@
 #pragma once
 #include "cvr_device.cuh"
 
+// Candidates read per round trip by the one-thread-per-atom search, and the
+// minimum resident blocks it is compiled for (register budget).
+#ifndef CVR_BUILD_UNROLL
+#define CVR_BUILD_UNROLL 2
+#endif
+#ifndef CVR_BUILD_MINB
+#define CVR_BUILD_MINB 8
+#endif
+
 namespace cvr {
 
 __device__ __forceinline__ int ghost_val(double x, double gclo, double gchi, int bc) {
@@ -219,7 +228,8 @@ __global__ void k_permute(DevState<real> s) {
   else
     q.w = (double)ty;
   s.x4[k] = q;
-  s.xb[k] = make_float4((float)loc[0], (float)loc[1], (float)loc[2], __int_as_float(cc[0]));
+  s.xb[k] = make_float4((float)(p[0] - s.box.ctr[0]), (float)(p[1] - s.box.ctr[1]), (float)(p[2] - s.box.ctr[2]),
+                        __int_as_float(cc[0]));
   s.gcls[k] = (int8_t)code;
 }
 
@@ -250,22 +260,19 @@ __device__ __forceinline__ bool has_image(int gcode, const int sh[3]) {
   return true;
 }
 
-// One candidate of the pair search: FP32 prefilter on cell-local
-// coordinates, exact FP64 reference test near the threshold.
+// The pair search's per-candidate test.  The FP32 prefilter works on
+// box-centred coordinates: d = (xb_j + s L) - xb_i, with the image shift s
+// folded into per-row constants b = s L - xb_i, so a candidate costs three
+// adds and a dot product.  Candidates inside rl^2 (1 - band) are accepted at
+// once (no image shift) and candidates outside rl^2 (1 + band) rejected; the
+// band is sized on the host from the FP32 rounding of the box coordinates.
+// Everything else takes the reference's exact FP64 test (and the ghost-image
+// rules for shifted images).
 template <typename real>
-__device__ __forceinline__ bool in_list(const DevState<real> &s, int i, const float4 &xi, const double (&pi)[3],
-                                        int gi, int j, const float4 &xj, int dx, int dy, int dz, int sx, int sy,
-                                        int sz) {
-  const bool shifted = (sx | sy | sz) != 0;
-  if (j == i && !shifted) return false;
-  const float ddx = (xj.x - xi.x) + dx * (float)s.cells.w[0];
-  const float ddy = (xj.y - xi.y) + dy * (float)s.cells.w[1];
-  const float ddz = (xj.z - xi.z) + dz * (float)s.cells.w[2];
-  const float d2 = ddx * ddx + ddy * ddy + ddz * ddz;
-  if (!(d2 < s.rl_sq_hi)) return false;
+__device__ __forceinline__ bool in_list_slow(const DevState<real> &s, const double (&pi)[3], int gi, int j, float d2,
+                                          int sx, int sy, int sz) {
   const int sh[3] = {sx, sy, sz};
-  if (!shifted) {
-    if (d2 <= s.rl_sq_lo) return true;
+  if ((sx | sy | sz) == 0) {
     const double pj[3] = {s.x[j], s.y[j], s.z[j]};
     return exact_within(pi, pj, sh, s.box, s.rl_sq);
   }
@@ -284,21 +291,13 @@ __device__ __forceinline__ uint32_t list_entry(int j, int dx, int dy, int dz, in
   return (uint32_t)j | (code << CODE_SHIFT);
 }
 
-template <typename real>
-__device__ __forceinline__ void consider(const DevState<real> &s, int i, const float4 &xi, const double (&pi)[3],
-                                         int gi, int j, const float4 &xj, int dx, int dy, int dz, int sx, int sy,
-                                         int sz, int &cnt, uint32_t *row, size_t stride, int log2_tpa, int count_only) {
-  if (in_list(s, i, xi, pi, gi, j, xj, dx, dy, dz, sx, sy, sz)) {
-    if (!count_only && cnt < s.cap)
-      row[(size_t)(cnt >> log2_tpa) * stride + (cnt & ((1 << log2_tpa) - 1))] =
-          list_entry(j, dx, dy, dz, s.cells.R, s.cells.S);
-    ++cnt;
-  }
+__device__ __forceinline__ size_t list_slot(int cnt, int log2_tpa, size_t stride) {
+  return (size_t)(cnt >> log2_tpa) * stride + (size_t)(cnt & ((1 << log2_tpa) - 1));
 }
 
 // The same search with one WARP per atom, for systems too small to fill the
 // GPU with one thread per atom: the 32 lanes take consecutive candidates of a
-// stencil row, and a ballot keeps the accepted ones in candidate order, so
+// stencil cell, and a ballot keeps the accepted ones in candidate order, so
 // the list is identical to the one-thread-per-atom build.
 template <typename real>
 __global__ void __launch_bounds__(128) k_build_list_warp(DevState<real> s, int count_only, int log2_tpa) {
@@ -322,23 +321,34 @@ __global__ void __launch_bounds__(128) k_build_list_warp(DevState<real> s, int c
     const int sz = floor_div(cz + dz, nc2);
     if (sz != 0 && !s.box.bc[2]) continue;
     const int jz = cz + dz - sz * nc2;
+    const float bz = sz * s.box.Lf[2] - xi.z;
     for (int dy = -R; dy <= R; ++dy) {
       const int sy = floor_div(cy + dy, nc1);
       if (sy != 0 && !s.box.bc[1]) continue;
       const int jy = cy + dy - sy * nc1;
+      const float by = sy * s.box.Lf[1] - xi.y;
       const int rowbase = nc0 * (jy + nc1 * jz);
       for (int dx = -R; dx <= R; ++dx) {
         const int sx = floor_div(cx + dx, nc0);
         if (sx != 0 && !s.box.bc[0]) continue;
+        const float bx = sx * s.box.Lf[0] - xi.x;
+        const bool shifted = (sx | sy | sz) != 0;
+        const int self = shifted ? -1 : i;
         const int cj = cx + dx - sx * nc0 + rowbase;
         const int jb = s.cell_start[cj], je = s.cell_start[cj + 1];
         for (int base = jb; base < je; base += 32) {
           const int j = base + lane;
-          const bool ok = (j < je) && in_list(s, i, xi, pi, gi, j, s.xb[min(j, je - 1)], dx, dy, dz, sx, sy, sz);
+          bool ok = false;
+          if (j < je && j != self) {
+            const float4 q = s.xb[j];
+            const float ex = q.x + bx, ey = q.y + by, ez = q.z + bz;
+            const float d2 = ex * ex + ey * ey + ez * ez;
+            if (d2 < s.rl_sq_hi) ok = (d2 <= s.rl_sq_lo && !shifted) || in_list_slow(s, pi, gi, j, d2, sx, sy, sz);
+          }
           const unsigned m = __ballot_sync(0xffffffffu, ok);
           if (ok && !count_only) {
             const int k = cnt + __popc(m & lt);
-            if (k < s.cap) row[(size_t)(k >> log2_tpa) * stride + (k & ((1 << log2_tpa) - 1))] = list_entry(j, dx, dy, dz, R, S);
+            if (k < s.cap) row[list_slot(k, log2_tpa, stride)] = list_entry(j, dx, dy, dz, R, S);
           }
           cnt += __popc(m);
         }
@@ -354,12 +364,12 @@ __global__ void __launch_bounds__(128) k_build_list_warp(DevState<real> s, int c
 
 // Pass 5: the pair search, one thread per atom over the (2R+1)^3 stencil.
 // Each stencil row (fixed dy, dz) is at most two contiguous atom ranges (a
-// periodic wrap in x splits it); candidates are read four at a time, and a
-// candidate's cell x index comes from xb.w.  Rows of boxes narrower than the
-// stencil (nc_x < 2R+1) take the cell-by-cell path.  count_only = 1 only
-// counts (used to size the list before the first build).
+// periodic wrap in x splits it); candidates are read CVR_BUILD_UNROLL at a
+// time, and a candidate's cell x index comes from xb.w.  Rows of boxes
+// narrower than the stencil (nc_x < 2R+1) take the cell-by-cell path.
+// count_only = 1 only counts (used to size the list before the first build).
 template <typename real>
-__global__ void __launch_bounds__(128) k_build_list(DevState<real> s, int count_only, int log2_tpa) {
+__global__ void __launch_bounds__(128, CVR_BUILD_MINB) k_build_list(DevState<real> s, int count_only, int log2_tpa) {
   if (*s.flag == 0) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (blockIdx.x == 0 && threadIdx.x == 0 && !count_only) atomicAdd(s.n_builds, 1);
@@ -374,19 +384,25 @@ __global__ void __launch_bounds__(128) k_build_list(DevState<real> s, int count_
     const size_t stride = (size_t)s.n_pad << log2_tpa;
     uint32_t *row = s.nlist + ((size_t)i << log2_tpa);
     const int nc0 = s.cells.nc[0], nc1 = s.cells.nc[1], nc2 = s.cells.nc[2];
-    const bool rows = nc0 >= S;
+    const float lo2 = s.rl_sq_lo, hi2 = s.rl_sq_hi;
     for (int dz = -R; dz <= R; ++dz) {
       const int sz = floor_div(cz + dz, nc2);
       if (sz != 0 && !s.box.bc[2]) continue;
       const int jz = cz + dz - sz * nc2;
+      const float bz = sz * s.box.Lf[2] - xi.z;
       for (int dy = -R; dy <= R; ++dy) {
         const int sy = floor_div(cy + dy, nc1);
         if (sy != 0 && !s.box.bc[1]) continue;
         const int jy = cy + dy - sy * nc1;
+        const float by = sy * s.box.Lf[1] - xi.y;
         const int rowbase = nc0 * (jy + nc1 * jz);
-        if (rows) {
-          // unwrapped x range [cx-R, cx+R] = part with sx=-1, sx=0, sx=+1
-          for (int sx = -1; sx <= 1; ++sx) {
+        const int parts = (nc0 >= S) ? 3 : S;
+        for (int part = 0; part < parts; ++part) {
+          // row mode: parts are the sx = -1, 0, +1 pieces of the unwrapped x
+          // range [cx-R, cx+R]; cell mode: one stencil cell per part
+          int sx, ca, cb, dxc;
+          if (nc0 >= S) {
+            sx = part - 1;
             int ua = cx - R, ub = cx + R;
             if (sx < 0) ub = min(ub, -1);
             if (sx == 0) {
@@ -395,30 +411,40 @@ __global__ void __launch_bounds__(128) k_build_list(DevState<real> s, int count_
             }
             if (sx > 0) ua = max(ua, nc0);
             if (ua > ub) continue;
-            if (sx != 0 && !s.box.bc[0]) continue;
-            const int jb = s.cell_start[rowbase + ua - sx * nc0];
-            const int je = s.cell_start[rowbase + ub - sx * nc0 + 1];
-            const int xoff = sx * nc0 - cx;  // dx = cell_x(j) + xoff
-            for (int j = jb; j < je; j += 4) {
-              float4 q[4];
-#pragma unroll
-              for (int u = 0; u < 4; ++u) q[u] = (j + u < je) ? s.xb[j + u] : xi;
-#pragma unroll
-              for (int u = 0; u < 4; ++u)
-                if (j + u < je)
-                  consider(s, i, xi, pi, gi, j + u, q[u], __float_as_int(q[u].w) + xoff, dy, dz, sx, sy, sz, cnt, row,
-                           stride, log2_tpa, count_only);
-            }
+            ca = ua - sx * nc0;
+            cb = ub - sx * nc0;
+            dxc = sx * nc0 - cx;  // dx = cell_x(j) + dxc
+          } else {
+            const int dx = part - R;
+            sx = floor_div(cx + dx, nc0);
+            ca = cb = cx + dx - sx * nc0;
+            dxc = dx - ca;
           }
-        } else {
-          for (int dx = -R; dx <= R; ++dx) {
-            const int sx = floor_div(cx + dx, nc0);
-            if (sx != 0 && !s.box.bc[0]) continue;
-            const int jx = cx + dx - sx * nc0;
-            const int cj = jx + rowbase;
-            const int jb = s.cell_start[cj], je = s.cell_start[cj + 1];
-            for (int j = jb; j < je; ++j)
-              consider(s, i, xi, pi, gi, j, s.xb[j], dx, dy, dz, sx, sy, sz, cnt, row, stride, log2_tpa, count_only);
+          if (sx != 0 && !s.box.bc[0]) continue;
+          const float bx = sx * s.box.Lf[0] - xi.x;
+          const bool shifted = (sx | sy | sz) != 0;
+          const int self = shifted ? -1 : i;
+          const int jb = s.cell_start[rowbase + ca];
+          const int je = s.cell_start[rowbase + cb + 1];
+          for (int j = jb; j < je; j += CVR_BUILD_UNROLL) {
+            float4 q[CVR_BUILD_UNROLL];
+#pragma unroll
+            for (int u = 0; u < CVR_BUILD_UNROLL; ++u) q[u] = (j + u < je) ? s.xb[j + u] : xi;
+#pragma unroll
+            for (int u = 0; u < CVR_BUILD_UNROLL; ++u) {
+              const int jj = j + u;
+              const float ex = q[u].x + bx, ey = q[u].y + by, ez = q[u].z + bz;
+              const float d2 = ex * ex + ey * ey + ez * ez;
+              if (jj < je && jj != self && d2 < hi2) {
+                const bool inc = (d2 <= lo2 && !shifted) || in_list_slow(s, pi, gi, jj, d2, sx, sy, sz);
+                if (inc) {
+                  if (!count_only && cnt < s.cap)
+                    row[list_slot(cnt, log2_tpa, stride)] =
+                        list_entry(jj, __float_as_int(q[u].w) + dxc, dy, dz, R, S);
+                  ++cnt;
+                }
+              }
+            }
           }
         }
       }

@@ -30,6 +30,8 @@ template <> struct V4<double> { using t = double4; };
 struct DBox {
   double lo[3], hi[3], L[3];
   double gclo[3], gchi[3];  // lower + ghost_cutoff, upper - ghost_cutoff (ghost zones)
+  double ctr[3];            // box centre: origin of the FP32 coordinates the list search uses
+  float Lf[3];
   int bc[3];
 };
 
@@ -60,7 +62,7 @@ template <typename real> struct DevState {
   double *x, *y, *z, *vx, *vy, *vz;
   real *ax, *ay, *az;
   typename V4<real>::t *x4;
-  float4 *xb;
+  float4 *xb;  // box-centred FP32 position at the last build, cell x index in .w (list search, rebuild trigger)
   int *cell, *id, *type, *mol;
   int8_t *gcls;                 // ghost-zone classification at build (x_val+1)+3(y_val+1)+9(z_val+1)
   // rebuild temporaries

@@ -18,6 +18,15 @@
 #pragma once
 #include "cvr_device.cuh"
 
+// List entries each pair-kernel lane has in flight, and the minimum resident
+// blocks the pair kernel is compiled for.
+#ifndef CVR_PAIR_UNROLL
+#define CVR_PAIR_UNROLL 4
+#endif
+#ifndef CVR_PAIR_MINB
+#define CVR_PAIR_MINB 1
+#endif
+
 namespace cvr {
 
 template <typename real> struct R2;
@@ -72,8 +81,8 @@ template <typename real> struct EwrArgs {
 // Ewald lambda).  ONE_TYPE keeps the single type pair's LJ constants in
 // registers (no table lookups).  The LJ cutoff is a select, not a branch.
 // EV adds energies + virial (FP64 per thread, FP64 block sums into
-// partials[block*3 + {e_lj, e_ewr, virial}]).  Entries are unrolled by two
-// so that two neighbour gathers are in flight per lane.
+// partials[block*3 + {e_lj, e_ewr, virial}]).  Entries are unrolled by
+// CVR_PAIR_UNROLL so that several neighbour gathers are in flight per lane.
 template <typename real> struct PairAcc {
   real fx, fy, fz;
   double e_lj, e_ew, vir;
@@ -113,7 +122,7 @@ __device__ __forceinline__ void pair_term(PairAcc<real> &A, real dx, real dy, re
 }
 
 template <typename real, int TPA, bool LJ, bool EWR, bool EV, bool ONE_TYPE>
-__global__ void __launch_bounds__(128) k_pair(DevState<real> s, const PairCoef<real> *__restrict__ coef_g,
+__global__ void __launch_bounds__(128, CVR_PAIR_MINB) k_pair(DevState<real> s, const PairCoef<real> *__restrict__ coef_g,
                                               const typename V4<real>::t *__restrict__ offs_g, EwrArgs<real> ew,
                                               int ignore_intra, int use_mol, double *__restrict__ partials) {
   using real4 = typename V4<real>::t;
@@ -140,25 +149,31 @@ __global__ void __launch_bounds__(128) k_pair(DevState<real> s, const PairCoef<r
     const PairCoef<real> *ci = coef + (ONE_TYPE ? 0 : ti * T);
     PairCoef<real> c1;
     if (ONE_TYPE) c1 = coef[0];
+    constexpr int U = CVR_PAIR_UNROLL;
     int k = lane;
-    for (; k + TPA < cnt; k += 2 * TPA) {
-      const uint32_t e0 = __ldcs(row);
-      const uint32_t e1 = __ldcs(row + stride);
-      row += 2 * stride;
-      const int j0 = (int)(e0 & INDEX_MASK), j1 = (int)(e1 & INDEX_MASK);
-      const real4 xj0 = s.x4[j0];
-      const real4 xj1 = s.x4[j1];
-      const real4 o0 = offs[e0 >> CODE_SHIFT];
-      const real4 o1 = offs[e1 >> CODE_SHIFT];
-      const bool sm0 = use_mol && (moli == s.mol[j0]);
-      const bool sm1 = use_mol && (moli == s.mol[j1]);
-      pair_term<real, LJ, EWR, EV>(A, (xj0.x - xi.x) + o0.x, (xj0.y - xi.y) + o0.y, (xj0.z - xi.z) + o0.z,
-                                   ONE_TYPE ? c1 : ci[type_of(xj0.w)], sm0, ignore_intra, ew);
-      pair_term<real, LJ, EWR, EV>(A, (xj1.x - xi.x) + o1.x, (xj1.y - xi.y) + o1.y, (xj1.z - xi.z) + o1.z,
-                                   ONE_TYPE ? c1 : ci[type_of(xj1.w)], sm1, ignore_intra, ew);
+    for (; k + (U - 1) * TPA < cnt; k += U * TPA) {
+      uint32_t e[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) e[u] = __ldcs(row + u * stride);
+      row += U * stride;
+      real4 xj[U], o[U];
+      bool sm[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int j = (int)(e[u] & INDEX_MASK);
+        xj[u] = s.x4[j];
+        o[u] = offs[e[u] >> CODE_SHIFT];
+        sm[u] = use_mol && (moli == s.mol[j]);
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+        pair_term<real, LJ, EWR, EV>(A, (xj[u].x - xi.x) + o[u].x, (xj[u].y - xi.y) + o[u].y,
+                                     (xj[u].z - xi.z) + o[u].z, ONE_TYPE ? c1 : ci[type_of(xj[u].w)], sm[u],
+                                     ignore_intra, ew);
     }
-    if (k < cnt) {
+    for (; k < cnt; k += TPA) {
       const uint32_t e0 = __ldcs(row);
+      row += stride;
       const int j0 = (int)(e0 & INDEX_MASK);
       const real4 xj0 = s.x4[j0];
       const real4 o0 = offs[e0 >> CODE_SHIFT];
@@ -434,7 +449,8 @@ __global__ void __launch_bounds__(256) k_kick_drift(DevState<real> s, double dt)
     q.z = (real)loc[2];
     s.x4[i] = q;
     const float4 b = s.xb[i];
-    const float ex = (float)loc[0] - b.x, ey = (float)loc[1] - b.y, ez = (float)loc[2] - b.z;
+    const float ex = (float)(p[0] - s.box.ctr[0]) - b.x, ey = (float)(p[1] - s.box.ctr[1]) - b.y,
+                ez = (float)(p[2] - s.box.ctr[2]) - b.z;
     if (ex * ex + ey * ey + ez * ez > s.thr_sq) need = true;
     if (s.policy == 1 && code != s.gcls[i]) need = true;  // ghost set changed
     if (s.policy == 2) need = true;
@@ -510,8 +526,7 @@ __global__ void __launch_bounds__(256) k_check(DevState<real> s) {
     const float4 b = s.xb[i];
     const float bb[3] = {b.x, b.y, b.z};
     for (int d = 0; d < 3; ++d) {
-      const double loc = p[d] - (s.box.lo[d] + (cc[d] + 0.5) * s.cells.w[d]);
-      e[d] = (float)loc - bb[d];
+      e[d] = (float)(p[d] - s.box.ctr[d]) - bb[d];
       if (s.policy == 1) {
         if (s.box.bc[d] == 1 && (p[d] < s.box.lo[d] || p[d] > s.box.hi[d])) need = true;
         code += (ghost_val(p[d], s.box.gclo[d], s.box.gchi[d], s.box.bc[d]) + 1) * mul;
