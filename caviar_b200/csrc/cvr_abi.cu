@@ -207,6 +207,9 @@ DevState<real> dev_state(cvr_ctx *c) {
   const double band = std::max(1e-5, 16.0 * 2.0 * rl * std::sqrt(3.0) * eps_coord / (rl * rl));
   s.rl_sq_lo = (float)(s.rl_sq * (1.0 - band));
   s.rl_sq_hi = (float)(s.rl_sq * (1.0 + band));
+  s.regular_images = 1;
+  for (int d = 0; d < 3; ++d)
+    if (c->bc[d] == 1 && !(c->gc >= rl && c->gc <= 0.5 * c->L[d])) s.regular_images = 0;
   const double half_skin = 0.5 * (rl - c->cutoff);  // threshold_distance_sq = 0.25 (rl - rc)^2
   s.thr_sq = (float)(half_skin * half_skin);
   s.x = c->x;
@@ -484,8 +487,9 @@ int alloc_cells(cvr_ctx *c) {
 }
 
 int alloc_list(cvr_ctx *c, int cap) {
-  c->cap = (cap + c->tpa - 1) / c->tpa * c->tpa;
-  const size_t entries = (size_t)c->cap * c->n_pad;
+  const int ilv = 1 << c->log2_tpa;
+  c->cap = (cap + ilv - 1) / ilv * ilv;
+  const size_t entries = (size_t)c->cap * c->n_pad;  // cap is a multiple of the interleave
   int r;
   if ((r = dalloc(c, &c->nlist, entries))) return r;
   c->nlist_bytes = entries * 4;
@@ -975,7 +979,7 @@ int pairs_impl(cvr_ctx *c, std::vector<std::array<int32_t, 5>> &out) {
   CVR_CUDA(c, cudaMemcpyAsync(cells.data(), c->cell, n * 4, cudaMemcpyDeviceToHost, c->stream));
   CVR_CUDA(c, cudaMemcpyAsync(lst.data(), c->nlist, lst.size() * 4, cudaMemcpyDeviceToHost, c->stream));
   CVR_CUDA(c, cudaStreamSynchronize(c->stream));
-  const int S = 2 * c->R + 1, tpa = c->tpa;
+  const int tpa = 1 << c->log2_tpa;  // list interleave (quads when one lane per atom)
   const size_t stride = (size_t)c->n_pad * tpa;
   auto fdiv = [](int a, int b) { return (a >= 0) ? a / b : -((-a + b - 1) / b); };
   out.clear();
@@ -985,8 +989,9 @@ int pairs_impl(cvr_ctx *c, std::vector<std::array<int32_t, 5>> &out) {
     const int cxyz[3] = {ck % c->nc[0], (ck / c->nc[0]) % c->nc[1], ck / (c->nc[0] * c->nc[1])};
     for (int e = 0; e < cnt[k]; ++e) {
       const uint32_t v = lst[(size_t)(e / tpa) * stride + (size_t)k * tpa + (e % tpa)];
-      const int j = (int)(v & INDEX_MASK), code = (int)(v >> CODE_SHIFT);
-      const int dd[3] = {code % S - c->R, (code / S) % S - c->R, code / (S * S) - c->R};
+      const int j = (int)(v & INDEX_MASK);
+      const int dd[3] = {(int)((v >> CODE_SHIFT) & 7u) - c->R, (int)((v >> (CODE_SHIFT + 3)) & 7u) - c->R,
+                         (int)((v >> (CODE_SHIFT + 6)) & 7u) - c->R};
       int sh[3];
       for (int d = 0; d < 3; ++d) sh[d] = fdiv(cxyz[d] + dd[d], c->nc[d]);
       int a = ids[k], b = ids[j];
@@ -1152,7 +1157,8 @@ int cvr_set_state(cvr_ctx *c, int64_t n, const double *pos, const double *vel, c
     if (int r = dalloc(c, &c->stage, 9 * (size_t)n)) return r;
     c->cap = 0;
     c->tpa = choose_tpa(n);
-    c->log2_tpa = (c->tpa == 32) ? 5 : (c->tpa == 8 ? 3 : 0);
+    // list interleave: TPA lanes per atom, or quads of four entries when one lane per atom
+    c->log2_tpa = (c->tpa == 32) ? 5 : (c->tpa == 8 ? 3 : 2);
   }
   CVR_CUDA(c, cudaMemcpyAsync(c->stage, pos, (size_t)n * 3 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   if (vel)

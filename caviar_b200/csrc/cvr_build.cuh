@@ -40,7 +40,12 @@ __device__ __forceinline__ int ghost_val(double x, double gclo, double gchi, int
   return v * bc;
 }
 
+// floor(a / b) for b > 0; the stencil only ever asks for -1, 0 or 1 when the
+// grid has at least 2R+1 cells, so those are answered without a division.
 __device__ __forceinline__ int floor_div(int a, int b) {
+  if (a >= 0 && a < b) return 0;
+  if (a < 0 && a >= -b) return -1;
+  if (a >= b && a < 2 * b) return 1;
   const int q = a / b;
   return (a % b != 0 && ((a < 0) != (b < 0))) ? q - 1 : q;
 }
@@ -263,11 +268,13 @@ __device__ __forceinline__ bool has_image(int gcode, const int sh[3]) {
 // The pair search's per-candidate test.  The FP32 prefilter works on
 // box-centred coordinates: d = (xb_j + s L) - xb_i, with the image shift s
 // folded into per-row constants b = s L - xb_i, so a candidate costs three
-// adds and a dot product.  Candidates inside rl^2 (1 - band) are accepted at
-// once (no image shift) and candidates outside rl^2 (1 + band) rejected; the
+// adds and a dot product.  Candidates outside rl^2 (1 + band) are rejected;
+// candidates inside rl^2 (1 - band) are accepted at once when there is no
+// image shift, or when the geometry is regular (rl <= ghost_cutoff <= L/2 on
+// every periodic axis: then both atoms of a pair clearly inside rl across a
+// face lie in the ghost zones, so the reference has the ghost image).  The
 // band is sized on the host from the FP32 rounding of the box coordinates.
-// Everything else takes the reference's exact FP64 test (and the ghost-image
-// rules for shifted images).
+// Everything else takes the reference's exact FP64 test and ghost-image rules.
 template <typename real>
 __device__ __forceinline__ bool in_list_slow(const DevState<real> &s, const double (&pi)[3], int gi, int j, float d2,
                                           int sx, int sy, int sz) {
@@ -287,13 +294,15 @@ __device__ __forceinline__ bool in_list_slow(const DevState<real> &s, const doub
 }
 
 __device__ __forceinline__ uint32_t list_entry(int j, int dx, int dy, int dz, int R, int S) {
-  const uint32_t code = (uint32_t)((dx + R) + S * ((dy + R) + S * (dz + R)));
-  return (uint32_t)j | (code << CODE_SHIFT);
+  (void)S;
+  return (uint32_t)j | ((uint32_t)(dx + R) << CODE_SHIFT) | ((uint32_t)(dy + R) << (CODE_SHIFT + 3)) |
+         ((uint32_t)(dz + R) << (CODE_SHIFT + 6));
 }
 
 __device__ __forceinline__ size_t list_slot(int cnt, int log2_tpa, size_t stride) {
   return (size_t)(cnt >> log2_tpa) * stride + (size_t)(cnt & ((1 << log2_tpa) - 1));
 }
+
 
 // The same search with one WARP per atom, for systems too small to fill the
 // GPU with one thread per atom: the 32 lanes take consecutive candidates of a
@@ -333,6 +342,7 @@ __global__ void __launch_bounds__(128) k_build_list_warp(DevState<real> s, int c
         if (sx != 0 && !s.box.bc[0]) continue;
         const float bx = sx * s.box.Lf[0] - xi.x;
         const bool shifted = (sx | sy | sz) != 0;
+        const bool fast_ok = !shifted || s.regular_images;
         const int self = shifted ? -1 : i;
         const int cj = cx + dx - sx * nc0 + rowbase;
         const int jb = s.cell_start[cj], je = s.cell_start[cj + 1];
@@ -343,7 +353,7 @@ __global__ void __launch_bounds__(128) k_build_list_warp(DevState<real> s, int c
             const float4 q = s.xb[j];
             const float ex = q.x + bx, ey = q.y + by, ez = q.z + bz;
             const float d2 = ex * ex + ey * ey + ez * ez;
-            if (d2 < s.rl_sq_hi) ok = (d2 <= s.rl_sq_lo && !shifted) || in_list_slow(s, pi, gi, j, d2, sx, sy, sz);
+            if (d2 < s.rl_sq_hi) ok = (d2 <= s.rl_sq_lo && fast_ok) || in_list_slow(s, pi, gi, j, d2, sx, sy, sz);
           }
           const unsigned m = __ballot_sync(0xffffffffu, ok);
           if (ok && !count_only) {
@@ -367,7 +377,9 @@ __global__ void __launch_bounds__(128) k_build_list_warp(DevState<real> s, int c
 // periodic wrap in x splits it); candidates are read CVR_BUILD_UNROLL at a
 // time, and a candidate's cell x index comes from xb.w.  Rows of boxes
 // narrower than the stencil (nc_x < 2R+1) take the cell-by-cell path.
-// count_only = 1 only counts (used to size the list before the first build).
+// With one lane per atom the list interleave is 4 (log2_tpa = 2): the pair
+// kernel reads an atom's entries four at a time.  count_only = 1 only counts (used to size the list before
+// the first build).
 template <typename real>
 __global__ void __launch_bounds__(128, CVR_BUILD_MINB) k_build_list(DevState<real> s, int count_only, int log2_tpa) {
   if (*s.flag == 0) return;
@@ -423,6 +435,7 @@ __global__ void __launch_bounds__(128, CVR_BUILD_MINB) k_build_list(DevState<rea
           if (sx != 0 && !s.box.bc[0]) continue;
           const float bx = sx * s.box.Lf[0] - xi.x;
           const bool shifted = (sx | sy | sz) != 0;
+          const bool fast_ok = !shifted || s.regular_images;
           const int self = shifted ? -1 : i;
           const int jb = s.cell_start[rowbase + ca];
           const int je = s.cell_start[rowbase + cb + 1];
@@ -436,11 +449,10 @@ __global__ void __launch_bounds__(128, CVR_BUILD_MINB) k_build_list(DevState<rea
               const float ex = q[u].x + bx, ey = q[u].y + by, ez = q[u].z + bz;
               const float d2 = ex * ex + ey * ey + ez * ez;
               if (jj < je && jj != self && d2 < hi2) {
-                const bool inc = (d2 <= lo2 && !shifted) || in_list_slow(s, pi, gi, jj, d2, sx, sy, sz);
+                const bool inc = (d2 <= lo2 && fast_ok) || in_list_slow(s, pi, gi, jj, d2, sx, sy, sz);
                 if (inc) {
                   if (!count_only && cnt < s.cap)
-                    row[list_slot(cnt, log2_tpa, stride)] =
-                        list_entry(jj, __float_as_int(q[u].w) + dxc, dy, dz, R, S);
+                    row[list_slot(cnt, log2_tpa, stride)] = list_entry(jj, __float_as_int(q[u].w) + dxc, dy, dz, R, S);
                   ++cnt;
                 }
               }
@@ -449,8 +461,10 @@ __global__ void __launch_bounds__(128, CVR_BUILD_MINB) k_build_list(DevState<rea
         }
       }
     }
-    if (!count_only) s.ncount[i] = min(cnt, s.cap);
-    if (!count_only && cnt > s.cap) atomicOr(s.err, ERR_OVERFLOW);
+    if (!count_only) {
+      s.ncount[i] = min(cnt, s.cap);
+      if (cnt > s.cap) atomicOr(s.err, ERR_OVERFLOW);
+    }
   }
   // largest count, one atomic per warp
   int m = cnt;

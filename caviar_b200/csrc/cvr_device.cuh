@@ -8,7 +8,8 @@
 //                      type in .w: the only per-neighbour gather of the pair kernel (16 B mixed)
 //   xb                 float4 cell-local position at the last build (rebuild trigger)
 //   cell,id,type,mol   int per atom; id = the caller's atom index
-//   nlist              uint32 entries j | (stencil offset code << 25), TPA-interleaved rows:
+//   nlist              uint32 entries: atom j in bits 0-22, stencil offset dx+R, dy+R, dz+R
+//                      in 3-bit fields at bits 23, 26, 29; TPA-interleaved rows:
 //                      entry k of atom i at (k/TPA)*(n_pad*TPA) + i*TPA + k%TPA
 //   ncount             neighbours per atom
 #pragma once
@@ -18,8 +19,9 @@
 namespace cvr {
 
 enum : int { ERR_NAN = 1, ERR_OVERFLOW = 2, ERR_GEOMETRY = 4 };
-constexpr int CODE_SHIFT = 25;
+constexpr int CODE_SHIFT = 23;  // first of the three 3-bit stencil-offset fields
 constexpr unsigned INDEX_MASK = (1u << CODE_SHIFT) - 1u;
+constexpr int MAX_STENCIL_R = 3;  // dx + R must fit in 3 bits
 constexpr int MAX_TYPES = 16;
 constexpr int MAX_KMAX = 31;
 
@@ -59,6 +61,8 @@ template <typename real> struct DevState {
   double rl_sq;                 // (cutoff*coef)^2, FP64 list threshold
   float rl_sq_lo, rl_sq_hi;     // FP32 guard band around rl_sq for the prefilter
   float thr_sq;                 // (skin/2)^2 rebuild threshold
+  int regular_images;           // rl <= ghost_cutoff <= L/2 on every periodic axis: every image pair
+                                // clearly inside rl has its reference ghost (no per-pair image test)
   double *x, *y, *z, *vx, *vy, *vz;
   real *ax, *ay, *az;
   typename V4<real>::t *x4;

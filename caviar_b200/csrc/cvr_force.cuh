@@ -46,6 +46,35 @@ __device__ __forceinline__ int type_of(double w) { return (int)w; }
 __device__ __forceinline__ void sincospi_r(float a, float *s, float *c) { sincospif(a, s, c); }
 __device__ __forceinline__ void sincospi_r(double a, double *s, double *c) { sincospi(a, s, c); }
 
+// Stencil offset of a list entry, (dx, dy, dz) * cell width, from its three
+// 3-bit fields.  The small integer field is turned into a float exactly by
+// placing it in the mantissa of 2^23 and subtracting 2^23 (+ R): no
+// int-to-float conversion instruction and no table lookup (the offset table
+// in shared memory was the busiest user of the L1 data pipe).
+__device__ __forceinline__ float stencil_f(uint32_t e, int shift, float bias) {
+  return __uint_as_float(0x4B000000u | ((e >> shift) & 7u)) - bias;
+}
+__device__ __forceinline__ double stencil_f64(uint32_t e, int shift, double bias) {
+  return __longlong_as_double(0x4330000000000000ll | (long long)((e >> shift) & 7u)) - bias;
+}
+template <typename real> struct Stencil;
+template <> struct Stencil<float> {
+  float bias, wx, wy, wz;
+  __device__ __forceinline__ void get(uint32_t e, float &ox, float &oy, float &oz) const {
+    ox = stencil_f(e, CODE_SHIFT, bias) * wx;
+    oy = stencil_f(e, CODE_SHIFT + 3, bias) * wy;
+    oz = stencil_f(e, CODE_SHIFT + 6, bias) * wz;
+  }
+};
+template <> struct Stencil<double> {
+  double bias, wx, wy, wz;
+  __device__ __forceinline__ void get(uint32_t e, double &ox, double &oy, double &oz) const {
+    ox = stencil_f64(e, CODE_SHIFT, bias) * wx;
+    oy = stencil_f64(e, CODE_SHIFT + 3, bias) * wy;
+    oz = stencil_f64(e, CODE_SHIFT + 6, bias) * wz;
+  }
+};
+
 // Block-wide sum of NV doubles into out[blockIdx.x * NV + q] (fixed order).
 template <int NV>
 __device__ __forceinline__ void block_sum_store(double (&v)[NV], double *out) {
@@ -127,10 +156,14 @@ __global__ void __launch_bounds__(128, CVR_PAIR_MINB) k_pair(DevState<real> s, c
                                               int ignore_intra, int use_mol, double *__restrict__ partials) {
   using real4 = typename V4<real>::t;
   __shared__ PairCoef<real> coef[ONE_TYPE ? 1 : MAX_TYPES * MAX_TYPES];
-  __shared__ real4 offs[125];
   const int T = s.n_types;
   for (int t = threadIdx.x; t < (ONE_TYPE ? 1 : T * T); t += blockDim.x) coef[t] = coef_g[t];
-  for (int t = threadIdx.x; t < s.cells.S * s.cells.S * s.cells.S; t += blockDim.x) offs[t] = offs_g[t];
+  (void)offs_g;
+  Stencil<real> st;
+  st.bias = (real)(sizeof(real) == 4 ? 8388608.0 : 4503599627370496.0) + (real)s.cells.R;
+  st.wx = (real)s.cells.w[0];
+  st.wy = (real)s.cells.w[1];
+  st.wz = (real)s.cells.w[2];
   __syncthreads();
   if (*s.err) return;
 
@@ -144,42 +177,71 @@ __global__ void __launch_bounds__(128, CVR_PAIR_MINB) k_pair(DevState<real> s, c
     ti = type_of(xi.w);
     const int moli = use_mol ? s.mol[i] : 0;
     const int cnt = s.ncount[i];
-    const size_t stride = (size_t)s.n_pad * TPA;
-    const uint32_t *row = s.nlist + (size_t)i * TPA + lane;
     const PairCoef<real> *ci = coef + (ONE_TYPE ? 0 : ti * T);
     PairCoef<real> c1;
     if (ONE_TYPE) c1 = coef[0];
-    constexpr int U = CVR_PAIR_UNROLL;
-    int k = lane;
-    for (; k + (U - 1) * TPA < cnt; k += U * TPA) {
-      uint32_t e[U];
+    if (TPA == 1) {
+      // one lane per atom: entries in quads, one 16-byte load per four
+      const uint4 *q4 = reinterpret_cast<const uint4 *>(s.nlist) + i;
+      for (int k = 0; k < cnt; k += 4) {
+        const uint4 e4 = __ldcs(q4);
+        q4 += s.n_pad;
+        const uint32_t e[4] = {e4.x, e4.y, e4.z, e4.w};
+        real4 xj[4];
+        bool sm[4];
 #pragma unroll
-      for (int u = 0; u < U; ++u) e[u] = __ldcs(row + u * stride);
-      row += U * stride;
-      real4 xj[U], o[U];
-      bool sm[U];
+        for (int u = 0; u < 4; ++u) {
+          const int j = (k + u < cnt) ? (int)(e[u] & INDEX_MASK) : i;
+          xj[u] = s.x4[j];
+          sm[u] = use_mol && (moli == s.mol[j]);
+        }
 #pragma unroll
-      for (int u = 0; u < U; ++u) {
-        const int j = (int)(e[u] & INDEX_MASK);
-        xj[u] = s.x4[j];
-        o[u] = offs[e[u] >> CODE_SHIFT];
-        sm[u] = use_mol && (moli == s.mol[j]);
+        for (int u = 0; u < 4; ++u) {
+          if (k + u < cnt) {
+            real ox, oy, oz;
+            st.get(e[u], ox, oy, oz);
+            pair_term<real, LJ, EWR, EV>(A, (xj[u].x - xi.x) + ox, (xj[u].y - xi.y) + oy, (xj[u].z - xi.z) + oz,
+                                         ONE_TYPE ? c1 : ci[type_of(xj[u].w)], sm[u], ignore_intra, ew);
+          }
+        }
       }
+    } else {
+      const size_t stride = (size_t)s.n_pad * TPA;
+      const uint32_t *row = s.nlist + (size_t)i * TPA + lane;
+      constexpr int U = CVR_PAIR_UNROLL;
+      int k = lane;
+      for (; k + (U - 1) * TPA < cnt; k += U * TPA) {
+        uint32_t e[U];
 #pragma unroll
-      for (int u = 0; u < U; ++u)
-        pair_term<real, LJ, EWR, EV>(A, (xj[u].x - xi.x) + o[u].x, (xj[u].y - xi.y) + o[u].y,
-                                     (xj[u].z - xi.z) + o[u].z, ONE_TYPE ? c1 : ci[type_of(xj[u].w)], sm[u],
-                                     ignore_intra, ew);
-    }
-    for (; k < cnt; k += TPA) {
-      const uint32_t e0 = __ldcs(row);
-      row += stride;
-      const int j0 = (int)(e0 & INDEX_MASK);
-      const real4 xj0 = s.x4[j0];
-      const real4 o0 = offs[e0 >> CODE_SHIFT];
-      const bool sm0 = use_mol && (moli == s.mol[j0]);
-      pair_term<real, LJ, EWR, EV>(A, (xj0.x - xi.x) + o0.x, (xj0.y - xi.y) + o0.y, (xj0.z - xi.z) + o0.z,
-                                   ONE_TYPE ? c1 : ci[type_of(xj0.w)], sm0, ignore_intra, ew);
+        for (int u = 0; u < U; ++u) e[u] = __ldcs(row + u * stride);
+        row += U * stride;
+        real4 xj[U];
+        bool sm[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const int j = (int)(e[u] & INDEX_MASK);
+          xj[u] = s.x4[j];
+          sm[u] = use_mol && (moli == s.mol[j]);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          real ox, oy, oz;
+          st.get(e[u], ox, oy, oz);
+          pair_term<real, LJ, EWR, EV>(A, (xj[u].x - xi.x) + ox, (xj[u].y - xi.y) + oy, (xj[u].z - xi.z) + oz,
+                                       ONE_TYPE ? c1 : ci[type_of(xj[u].w)], sm[u], ignore_intra, ew);
+        }
+      }
+      for (; k < cnt; k += TPA) {
+        const uint32_t e0 = __ldcs(row);
+        row += stride;
+        const int j0 = (int)(e0 & INDEX_MASK);
+        const real4 xj0 = s.x4[j0];
+        const bool sm0 = use_mol && (moli == s.mol[j0]);
+        real ox, oy, oz;
+        st.get(e0, ox, oy, oz);
+        pair_term<real, LJ, EWR, EV>(A, (xj0.x - xi.x) + ox, (xj0.y - xi.y) + oy, (xj0.z - xi.z) + oz,
+                                     ONE_TYPE ? c1 : ci[type_of(xj0.w)], sm0, ignore_intra, ew);
+      }
     }
   }
 #pragma unroll
