@@ -149,12 +149,21 @@ def time_run(sim, torch, steps: int, warmup: int, dist=None, thermo_every: int =
     return e0.elapsed_time(e1)
 
 
-def max_over_ranks(x: float, dist, torch):
+def max_over_ranks(x: float, dist, torch, device: str = "cuda"):
+    """The slowest rank's time (replicas: the job ends when the last one does)."""
     if dist is None:
         return x
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def whole_job_rate(ms_local: float, atoms_per_rank: int, steps: int, dist, torch, device: str = "cuda"):
+    """(max-over-ranks ms, whole-job atom-steps/s): every rank advances its own
+    replica of atoms_per_rank atoms for `steps` steps."""
+    world = dist.get_world_size() if dist is not None else 1
+    ms_max = max_over_ranks(ms_local, dist, torch, device)
+    return ms_max, world * atoms_per_rank * steps / (ms_max / 1e3)
 
 
 def force_error(abi, s):
@@ -206,8 +215,7 @@ def gpu_arm(args):
     sim.set_kernel_timing(False)
     info = sim.info()
     builds = info["builds"] - b0
-    ms_max = max_over_ranks(ms, dist, torch)
-    value = world * n * steps / (ms_max / 1e3)
+    ms_max, value = whole_job_rate(ms, n, steps, dist, torch)
 
     # --- e2e through the public API: host (pinned) buffers in, results out
     pos_h = torch.from_numpy(np.ascontiguousarray(s_lj.pos)).pin_memory()

@@ -27,7 +27,7 @@ EXPORTED = ["cvr_create", "cvr_destroy", "cvr_set_neighborlist", "cvr_set_lj", "
             "cvr_set_integrator", "cvr_set_precision", "cvr_set_state", "cvr_build_neighbors", "cvr_compute_forces",
             "cvr_run", "cvr_get_state", "cvr_get_pairs", "cvr_get_sk", "cvr_get_scalars", "cvr_last_error",
             "cvr_launch_count", "cvr_get_stream", "cvr_get_info", "cvr_set_kernel_timing", "cvr_kernel_time",
-            "cvr_structure_factor_noalloc"]
+            "cvr_structure_factor_noalloc", "cvr_casl_run_file"]
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int32)
@@ -79,6 +79,18 @@ def load(path: str = LIB_PATH):
     L.cvr_kernel_time.argtypes = [vp, ctypes.c_int, _dp, ctypes.POINTER(ctypes.c_int64)]
     _lib = L
     return L
+
+
+def run_casl(path: str) -> None:
+    """Run a CASL script on the GPU (cvr_casl_run_file); raises on error."""
+    L = load()
+    f = L.cvr_casl_run_file
+    f.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_size_t]
+    f.restype = ctypes.c_int
+    buf = ctypes.create_string_buffer(1024)
+    rc = f(path.encode(), buf, 1024)
+    if rc != OK:
+        raise CvrError(rc, buf.value.decode(errors="replace"))
 
 
 def _d(a):

@@ -9,8 +9,10 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libcaviar_b200.so")
-SOURCES = [os.path.join(HERE, "csrc", "cvr_abi.cu"), os.path.join(HERE, "csrc", "cvr_noalloc.cu")]
-DEPS = SOURCES + [os.path.join(HERE, "csrc", f) for f in ("cvr_device.cuh", "cvr_build.cuh", "cvr_force.cuh")] + [
+SOURCES = [os.path.join(HERE, "csrc", "cvr_abi.cu"), os.path.join(HERE, "csrc", "cvr_noalloc.cu"),
+           os.path.join(HERE, "csrc", "cvr_casl.cpp")]
+CLI = os.path.join(HERE, "caviar_b200_casl")
+DEPS = SOURCES + [os.path.join(HERE, "csrc", f) for f in ("cvr_device.cuh", "cvr_build.cuh", "cvr_force.cuh", "cvr_main.cpp")] + [
     os.path.join(ROOT, "include", "caviar_b200.h")]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -38,6 +40,9 @@ def build(force: bool = False, verbose: bool = False) -> str:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)
     os.replace(LIB + ".tmp", LIB)
+    # command-line front end: caviar_b200_casl script.casl (like `CAVIAR -i script`)
+    subprocess.run([nvcc(), *ARCH, "-O2", "-std=c++17", "-o", CLI, os.path.join(HERE, "csrc", "cvr_main.cpp"),
+                    "-L" + HERE, "-lcaviar_b200", "-Xlinker", "-rpath,$ORIGIN"], check=True)
     return LIB
 
 

@@ -1,0 +1,664 @@
+// cvr_casl.cpp -- the hot-path subset of CAVIAR's CASL scripting language and
+// object model, in front of the C ABI (include/caviar_b200.h).
+//
+// A script written for the reference's objects runs here unchanged as long as
+// it only uses the hot-path objects and keywords:
+//   domain box <name>          xmin xmax ymin ymax zmin zmax (or lower_global.x ...),
+//                              boundary_condition|bc i j k, generate
+//                              (reference: src/caviar/objects/domain.cpp:206-266)
+//   atom_data basic <name>     ghost_cutoff, k_b, set_domain|domain, add_type_mass t m,
+//                              add_type_charge t q, add_xyz_data_file file_name "<f>"
+//                              [read_velocity] [last_frame] [replace_data],
+//                              set_owned_position|set_owned_velocity i x y z
+//                              (atom_data.cpp:78-306, atom_data/add_xyz_data_file.cpp:22-168)
+//   neighborlist basic <name>  set_atom_data|atom_data, set_domain|domain, cutoff,
+//                              cutoff_extra_coef, build_cell_list,
+//                              make_verlet_list_from_cell_list, rebuild_test, dt
+//                              (neighborlist.cpp:193-251)
+//   force_field lj <name>      cutoff, cutoff_list i j v, epsilon i j v, sigma i j v,
+//                              epsilon_atom i v, sigma_atom i v, lambda_s i j v,
+//                              lambda_e i j v, wca, ignore_intra_molecule,
+//                              make_off_diagonal_vectors, set_neighborlist|neighborlist,
+//                              set_atom_data|atom_data, set_domain|domain (lj.cpp:42-353)
+//   force_field electrostatic_ewald_r <name>  cutoff, alpha, k_electrostatic, lambda i j v,
+//                              set_neighborlist, set_atom_data (electrostatic_ewald_r.cpp:38-107)
+//   force_field electrostatic_ewald_k <name>  alpha, k_max, kx_max, ky_max, kz_max,
+//                              k_electrostatic, set_atom_data, set_domain (electrostatic_ewald_k.cpp:48-143)
+//   md_simulator basic <name>  set_atom_data, add_force_field|force_field,
+//                              add_neighborlist|neighborlist, integrator_type velocity_verlet,
+//                              dt, initial_step, final_step, final_step_add, run
+//                              (md_simulator.cpp:58-233)
+// plus the variables `real name value` / `int name value`, comments (#) and
+// `exit`.  Keywords of these objects that sit off the hot path (writers,
+// constraints, Langevin, slab/dipole Ewald, jump_tol) are rejected with a
+// message instead of being ignored.
+//
+// Extensions for the B200 path (md_simulator): precision mixed|fp64,
+// rebuild_policy displacement|reference, thermo_step N, thermo_file "<f>",
+// state_file "<f>" (FP64 binary dump of the final state, id order).
+//
+// Errors come back as CVR_ERR_INVALID with "file:line: message"; nothing here
+// exits the process (the reference prints and exits, interpreter/error.cpp:27-31).
+#include <algorithm>
+#include <cctype>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <map>
+#include <memory>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/caviar_b200.h"
+
+namespace {
+
+struct CaslError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
+// ------------------------------------------------------------------ lexer
+struct Line {
+  std::vector<std::string> tok;
+  std::vector<bool> quoted;
+  int lineno = 0;
+  size_t pos = 0;
+  bool done() const { return pos >= tok.size(); }
+};
+
+std::vector<Line> lex(const std::string &path) {
+  std::ifstream f(path);
+  if (!f) throw CaslError("cannot open script " + path);
+  std::vector<Line> out;
+  std::string raw;
+  int no = 0;
+  while (std::getline(f, raw)) {
+    ++no;
+    Line L;
+    L.lineno = no;
+    size_t k = 0;
+    while (k < raw.size()) {
+      const char c = raw[k];
+      if (c == '#') break;
+      if (std::isspace((unsigned char)c)) {
+        ++k;
+        continue;
+      }
+      if (c == '"' || c == '\'') {
+        const size_t e = raw.find(c, k + 1);
+        if (e == std::string::npos) throw CaslError(path + ":" + std::to_string(no) + ": unterminated string");
+        L.tok.push_back(raw.substr(k + 1, e - k - 1));
+        L.quoted.push_back(true);
+        k = e + 1;
+        continue;
+      }
+      size_t e = k;
+      while (e < raw.size() && !std::isspace((unsigned char)raw[e]) && raw[e] != '#') ++e;
+      L.tok.push_back(raw.substr(k, e - k));
+      L.quoted.push_back(false);
+      k = e;
+    }
+    if (!L.tok.empty()) out.push_back(L);
+  }
+  return out;
+}
+
+std::string dir_of(const std::string &p) {
+  const size_t s = p.find_last_of('/');
+  return (s == std::string::npos) ? std::string(".") : p.substr(0, s);
+}
+
+// ------------------------------------------------------------- objects
+struct Script;
+
+struct Object {
+  std::string name;
+  virtual ~Object() = default;
+};
+
+struct Domain : Object {
+  double lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+  int bc[3] = {0, 0, 0};
+  bool generated = false;
+};
+
+struct Atom_data : Object {
+  Domain *domain = nullptr;
+  double ghost_cutoff = -1.0, k_b = -1.0;
+  std::vector<double> mass, charge;
+  std::vector<int32_t> type, mol;
+  std::vector<double> pos, vel;
+  int64_t n() const { return (int64_t)type.size(); }
+};
+
+struct Neighborlist : Object {
+  Atom_data *atom_data = nullptr;
+  Domain *domain = nullptr;
+  double cutoff = 0.0, coef = 1.12347;  // neighborlist.h:134
+  bool rebuild_test = false, from_cell_list = false;
+};
+
+struct Force_field : Object {
+  Atom_data *atom_data = nullptr;
+  Neighborlist *neighborlist = nullptr;
+  Domain *domain = nullptr;
+};
+
+using Mat = std::vector<std::vector<double>>;
+
+void set_elem(Mat &m, int i, int j, double v, double fill) {
+  if (i < 0 || j < 0) throw CaslError("negative type index");
+  if ((int)m.size() <= i) m.resize(i + 1);
+  if ((int)m[i].size() <= j) m[i].resize(j + 1, fill);
+  m[i][j] = v;
+}
+
+double elem(const Mat &m, int i, int j, double fill) {
+  if (i < (int)m.size() && j < (int)m[i].size()) return m[i][j];
+  return fill;
+}
+
+struct Lj : Force_field {
+  double cutoff = 0.0;
+  Mat epsilon, sigma, cutoff_list, lambda_s, lambda_e;
+  std::vector<double> epsilon_atom, sigma_atom;
+  bool by_array = false, by_atom = false, wca = false, cutoff_list_on = false, ignore_intra = false;
+};
+
+struct Ewald_r : Force_field {
+  double cutoff = 0.0, alpha = 1.0, k_e = 1.0;
+  Mat lambda;
+  bool lambda_on = false;
+};
+
+struct Ewald_k : Force_field {
+  double alpha = 1.0, k_e = 1.0;
+  int kmax[3] = {1, 1, 1};
+};
+
+struct Md_simulator : Object {
+  Atom_data *atom_data = nullptr;
+  std::vector<Force_field *> force_field;
+  std::vector<Neighborlist *> neighborlist;
+  double dt = -1.0;
+  int64_t initial_step = 0, final_step = 0;
+  bool vv = false, use_step = false;
+  int precision = CVR_PREC_MIXED, policy = CVR_REBUILD_DISPLACEMENT;
+  int64_t thermo_step = 0;
+  std::string thermo_file, state_file;
+};
+
+// ------------------------------------------------------------- interpreter
+struct Script {
+  std::string path, dir;
+  std::map<std::string, std::unique_ptr<Object>> objects;
+  std::map<std::string, double> vars;
+  Line *cur = nullptr;
+
+  [[noreturn]] void err(const std::string &m) const {
+    throw CaslError(path + ":" + std::to_string(cur ? cur->lineno : 0) + ": " + m);
+  }
+  std::string word() {
+    if (cur->done()) err("expected a value");
+    return cur->tok[cur->pos++];
+  }
+  double real() {
+    const std::string w = word();
+    auto it = vars.find(w);
+    if (it != vars.end()) return it->second;
+    char *end = nullptr;
+    const double v = std::strtod(w.c_str(), &end);
+    if (end == w.c_str() || *end) err("expected a real number or variable, got '" + w + "'");
+    return v;
+  }
+  int integer() {
+    const double v = real();
+    if (v != std::floor(v)) err("expected an integer");
+    return (int)v;
+  }
+  template <typename T>
+  T *find(const std::string &nm) {
+    auto it = objects.find(nm);
+    if (it == objects.end()) err("undefined object '" + nm + "'");
+    T *p = dynamic_cast<T *>(it->second.get());
+    if (!p) err("object '" + nm + "' has the wrong class");
+    return p;
+  }
+
+  void create(const std::string &cls, const std::string &type, const std::string &nm) {
+    if (objects.count(nm)) err("object name '" + nm + "' already used");
+    std::unique_ptr<Object> o;
+    if (cls == "domain" && type == "box") o.reset(new Domain);
+    else if (cls == "atom_data" && type == "basic") o.reset(new Atom_data);
+    else if (cls == "neighborlist" && type == "basic") o.reset(new Neighborlist);
+    else if (cls == "force_field" && type == "lj") o.reset(new Lj);
+    else if (cls == "force_field" && type == "electrostatic_ewald_r") o.reset(new Ewald_r);
+    else if (cls == "force_field" && type == "electrostatic_ewald_k") o.reset(new Ewald_k);
+    else if (cls == "md_simulator" && type == "basic") o.reset(new Md_simulator);
+    else err("'" + cls + " " + type + "' is not on the B200 hot path");
+    o->name = nm;
+    objects[nm] = std::move(o);
+  }
+
+  void read_domain(Domain &d) {
+    while (!cur->done()) {
+      const std::string t = word();
+      const char *ax[3][2] = {{"xmin", "xmax"}, {"ymin", "ymax"}, {"zmin", "zmax"}};
+      const char *ax2[3][2] = {{"lower_global.x", "upper_global.x"},
+                               {"lower_global.y", "upper_global.y"},
+                               {"lower_global.z", "upper_global.z"}};
+      bool done = false;
+      for (int a = 0; a < 3 && !done; ++a) {
+        if (t == ax[a][0] || t == ax2[a][0]) d.lo[a] = real(), done = true;
+        else if (t == ax[a][1] || t == ax2[a][1]) d.hi[a] = real(), done = true;
+      }
+      if (done) continue;
+      if (t == "boundary_condition" || t == "bc") {
+        for (int a = 0; a < 3; ++a) d.bc[a] = integer();
+      } else if (t == "generate") {
+        d.generated = true;
+      } else err("domain: unknown keyword '" + t + "'");
+    }
+  }
+
+  void add_xyz(Atom_data &a) {
+    std::string file;
+    bool read_velocity = false, last_frame = false, replace = false;
+    while (!cur->done()) {
+      const std::string t = word();
+      if (t == "file_name") file = word();
+      else if (t == "read_velocity") read_velocity = true;
+      else if (t == "last_frame") last_frame = true;
+      else if (t == "replace_data") replace = true;
+      else err("add_xyz_data_file: unknown keyword '" + t + "'");
+    }
+    if (file.empty()) err("add_xyz_data_file needs file_name");
+    const std::string full = (file[0] == '/') ? file : dir + "/" + file;
+    std::ifstream f(full);
+    if (!f) err("file does not exist : " + full);
+    std::vector<std::string> lines;
+    std::string l;
+    while (std::getline(f, l)) lines.push_back(l);
+    // frames: <count> / comment / count lines; last_frame picks the last one
+    size_t start = 0;
+    if (last_frame) {
+      size_t k = 0;
+      while (k < lines.size()) {
+        std::istringstream is(lines[k]);
+        long long m;
+        if (!(is >> m) || m <= 0) break;
+        start = k;
+        k += 2 + (size_t)m;
+      }
+    }
+    std::istringstream hs(lines.size() > start ? lines[start] : "");
+    long long m = 0;
+    if (!(hs >> m) || m <= 0) err("no atom found in the xyz file. Something is wrong.");
+    if (replace && m != a.n()) err("XYZ file is not compatible: Different number of existing atoms");
+    for (long long k = 0; k < m; ++k) {
+      if (start + 2 + k >= lines.size()) err("xyz file ends early");
+      std::istringstream is(lines[start + 2 + (size_t)k]);
+      int ty;
+      double p[3], v[3] = {0, 0, 0};
+      if (!(is >> ty >> p[0] >> p[1] >> p[2])) err("bad xyz line");
+      if (read_velocity && !(is >> v[0] >> v[1] >> v[2])) err("bad xyz velocity");
+      if (replace) {
+        if (ty != a.type[(size_t)k]) err("XYZ file is not compatible: Different atom type order exists.");
+        for (int d = 0; d < 3; ++d) {
+          a.pos[3 * (size_t)k + d] = p[d];
+          a.vel[3 * (size_t)k + d] = v[d];
+        }
+      } else {
+        a.type.push_back(ty);
+        a.mol.push_back(-1);
+        for (int d = 0; d < 3; ++d) {
+          a.pos.push_back(p[d]);
+          a.vel.push_back(v[d]);
+        }
+      }
+    }
+  }
+
+  void read_atom_data(Atom_data &a) {
+    while (!cur->done()) {
+      const std::string t = word();
+      if (t == "ghost_cutoff") a.ghost_cutoff = real();
+      else if (t == "k_b") a.k_b = real();
+      else if (t == "set_domain" || t == "domain") a.domain = find<Domain>(word());
+      else if (t == "add_type_mass") {
+        const int i = integer();
+        const double v = real();
+        if ((int)a.mass.size() <= i) a.mass.resize(i + 1, 0.0);
+        a.mass[i] = v;
+      } else if (t == "add_type_charge") {
+        const int i = integer();
+        const double v = real();
+        if ((int)a.charge.size() <= i) a.charge.resize(i + 1, 0.0);
+        a.charge[i] = v;
+      } else if (t == "add_xyz_data_file") {
+        add_xyz(a);
+      } else if (t == "set_owned_position" || t == "set_owned_velocity") {
+        const int i = integer();
+        if (i < 0 || i >= a.n()) err(t + ": atom index out of range");
+        auto &dst = (t == "set_owned_position") ? a.pos : a.vel;
+        for (int d = 0; d < 3; ++d) dst[3 * (size_t)i + d] = real();
+      } else if (t == "temperature_process" || t == "pressure_process") {
+        // thermo is always computed on the GPU path
+      } else err("atom_data: '" + t + "' is not on the B200 hot path");
+    }
+  }
+
+  void read_neighborlist(Neighborlist &nl) {
+    while (!cur->done()) {
+      const std::string t = word();
+      if (t == "set_atom_data" || t == "atom_data") nl.atom_data = find<Atom_data>(word());
+      else if (t == "set_domain" || t == "domain") nl.domain = find<Domain>(word());
+      else if (t == "cutoff") {
+        nl.cutoff = real();
+        if (nl.cutoff <= 0.0) err("cutoff have to non-negative.");
+      } else if (t == "cutoff_extra_coef") {
+        nl.coef = real();
+        if (nl.coef < 1.0) err("cutoff_extra_coef must be larger than 1.0");
+      } else if (t == "make_verlet_list_from_cell_list" || t == "build_cell_list") {
+        nl.from_cell_list = true;
+      } else if (t == "rebuild_test") {
+        nl.rebuild_test = true;
+      } else if (t == "dt") {
+        real();
+      } else err("neighborlist: '" + t + "' is not supported on the B200 path");
+    }
+  }
+
+  void common_ff(Force_field &f, const std::string &t, bool &handled) {
+    handled = true;
+    if (t == "set_neighborlist" || t == "neighborlist") f.neighborlist = find<Neighborlist>(word());
+    else if (t == "set_atom_data" || t == "atom_data") f.atom_data = find<Atom_data>(word());
+    else if (t == "set_domain" || t == "domain") f.domain = find<Domain>(word());
+    else handled = false;
+  }
+
+  void read_lj(Lj &f) {
+    while (!cur->done()) {
+      const std::string t = word();
+      bool h;
+      common_ff(f, t, h);
+      if (h) continue;
+      if (t == "cutoff") {
+        f.cutoff = real();
+        if (f.cutoff < 0) err("Force field cutoff have to non-negative.");
+      } else if (t == "cutoff_list") {
+        const int i = integer(), j = integer();
+        set_elem(f.cutoff_list, i, j, real(), 0.0);
+        f.cutoff_list_on = true;
+      } else if (t == "epsilon" || t == "sigma") {
+        const int i = integer(), j = integer();
+        const double v = real();
+        if (v < 0) err("Epsilon have to be non-negative.");
+        set_elem(t == "epsilon" ? f.epsilon : f.sigma, i, j, v, 0.0);
+        f.by_array = true;
+      } else if (t == "lambda_s" || t == "lambda_e") {
+        const int i = integer(), j = integer();
+        set_elem(t == "lambda_s" ? f.lambda_s : f.lambda_e, i, j, real(), 1.0);
+      } else if (t == "epsilon_atom" || t == "sigma_atom") {
+        const int i = integer();
+        auto &v = (t == "epsilon_atom") ? f.epsilon_atom : f.sigma_atom;
+        if ((int)v.size() <= i) v.resize(i + 1, 0.0);
+        v[i] = real();
+        f.by_atom = true;
+      } else if (t == "wca") {
+        f.wca = true;
+        f.cutoff_list_on = true;
+      } else if (t == "ignore_intra_molecule") {
+        f.ignore_intra = true;
+      } else if (t == "make_off_diagonal_vectors") {
+        // no effect on the forces
+      } else err("force_field lj: '" + t + "' is not supported on the B200 path");
+    }
+  }
+
+  void read_ewald_r(Ewald_r &f) {
+    while (!cur->done()) {
+      const std::string t = word();
+      bool h;
+      common_ff(f, t, h);
+      if (h) continue;
+      if (t == "cutoff") f.cutoff = real();  // parsed, unused by the force (electrostatic_ewald_r.cpp:142-226)
+      else if (t == "alpha") f.alpha = real();
+      else if (t == "k_electrostatic") f.k_e = real();
+      else if (t == "lambda") {
+        const int i = integer(), j = integer();
+        set_elem(f.lambda, i, j, real(), 1.0);
+        f.lambda_on = true;
+      } else err("force_field electrostatic_ewald_r: '" + t + "' is not supported on the B200 path");
+    }
+  }
+
+  void read_ewald_k(Ewald_k &f) {
+    while (!cur->done()) {
+      const std::string t = word();
+      bool h;
+      common_ff(f, t, h);
+      if (h) continue;
+      if (t == "alpha") f.alpha = real();
+      else if (t == "k_electrostatic") f.k_e = real();
+      else if (t == "k_max") f.kmax[0] = f.kmax[1] = f.kmax[2] = integer();
+      else if (t == "kx_max") f.kmax[0] = integer();
+      else if (t == "ky_max") f.kmax[1] = integer();
+      else if (t == "kz_max") f.kmax[2] = integer();
+      else err("force_field electrostatic_ewald_k: '" + t + "' is not supported on the B200 path");
+    }
+  }
+
+  void read_md(Md_simulator &m) {
+    while (!cur->done()) {
+      const std::string t = word();
+      if (t == "set_atom_data" || t == "atom_data") m.atom_data = find<Atom_data>(word());
+      else if (t == "add_force_field" || t == "force_field") m.force_field.push_back(find<Force_field>(word()));
+      else if (t == "add_neighborlist" || t == "neighborlist") m.neighborlist.push_back(find<Neighborlist>(word()));
+      else if (t == "integrator_type") {
+        const std::string v = word();
+        if (v != "velocity_verlet") err("integrator_type '" + v + "' is not on the B200 hot path");
+        m.vv = true;
+      } else if (t == "dt") m.dt = real();
+      else if (t == "initial_step") m.initial_step = integer(), m.use_step = true;
+      else if (t == "final_step") m.final_step = integer(), m.use_step = true;
+      else if (t == "final_step_add") m.final_step += integer(), m.use_step = true;
+      else if (t == "precision") {
+        const std::string v = word();
+        if (v == "mixed") m.precision = CVR_PREC_MIXED;
+        else if (v == "fp64") m.precision = CVR_PREC_FP64;
+        else err("precision mixed|fp64");
+      } else if (t == "rebuild_policy") {
+        const std::string v = word();
+        if (v == "displacement") m.policy = CVR_REBUILD_DISPLACEMENT;
+        else if (v == "reference") m.policy = CVR_REBUILD_REFERENCE;
+        else err("rebuild_policy displacement|reference");
+      } else if (t == "thermo_step") m.thermo_step = integer();
+      else if (t == "thermo_file") m.thermo_file = word();
+      else if (t == "state_file") m.state_file = word();
+      else if (t == "run") run(m);
+      else err("md_simulator: '" + t + "' is not supported on the B200 path");
+    }
+  }
+
+  // Lj::verify_settings (lj.cpp:149-353): the per-type-pair tables.
+  void lj_tables(const Lj &f, int T, std::vector<double> &eps, std::vector<double> &sig, std::vector<double> &cut,
+                 bool &use_cut) {
+    if (f.by_atom && f.by_array) err("lj: (input_by_atom && input_by_array)");
+    eps.assign(T * T, 0.0);
+    sig.assign(T * T, 0.0);
+    for (int i = 0; i < T; ++i)
+      for (int j = 0; j < T; ++j) {
+        if (f.by_atom) {
+          const double ei = i < (int)f.epsilon_atom.size() ? f.epsilon_atom[i] : 0.0;
+          const double ej = j < (int)f.epsilon_atom.size() ? f.epsilon_atom[j] : 0.0;
+          const double si = i < (int)f.sigma_atom.size() ? f.sigma_atom[i] : 0.0;
+          const double sj = j < (int)f.sigma_atom.size() ? f.sigma_atom[j] : 0.0;
+          eps[i * T + j] = (i == j) ? ei : std::sqrt(ei * ej);
+          sig[i * T + j] = (i == j) ? si : 0.5 * (si + sj);
+        } else {
+          eps[i * T + j] = elem(f.epsilon, i, j, 0.0);
+          sig[i * T + j] = elem(f.sigma, i, j, 0.0);
+        }
+      }
+    for (int i = 0; i < T; ++i)
+      for (int j = 0; j < T; ++j) {
+        sig[i * T + j] *= elem(f.lambda_s, i, j, 1.0);
+        eps[i * T + j] *= elem(f.lambda_e, i, j, 1.0);
+      }
+    use_cut = f.cutoff_list_on;
+    cut.assign(T * T, 0.0);
+    for (int i = 0; i < T; ++i)
+      for (int j = 0; j < T; ++j)
+        cut[i * T + j] = f.wca ? std::pow(2.0, 1.0 / 6.0) * sig[i * T + j] : elem(f.cutoff_list, i, j, 0.0);
+    // the GPU list is full (each pair from both atoms), so the tables must be
+    // symmetric; the reference evaluates each pair from one end only
+    for (int i = 0; i < T; ++i)
+      for (int j = 0; j < i; ++j)
+        if (eps[i * T + j] != eps[j * T + i] || sig[i * T + j] != sig[j * T + i] ||
+            (use_cut && cut[i * T + j] != cut[j * T + i]))
+          err("lj: epsilon, sigma and cutoff_list must be symmetric on the B200 path");
+  }
+
+  void run(Md_simulator &m) {
+    Atom_data *a = m.atom_data;
+    if (!a) err("md_simulator: set_atom_data first");
+    if (!m.vv) err("md_simulator: set 'integrator_type velocity_verlet' (the reference leaves it unset)");
+    if (m.dt < 0) err("expected 'dt' input");
+    if (!m.use_step) err("simulator md: verify_settings: please assign 'time' or 'step' variables.");
+    if (m.neighborlist.size() != 1) err("the B200 path takes exactly one neighborlist");
+    Neighborlist *nl = m.neighborlist[0];
+    Domain *d = a->domain ? a->domain : nl->domain;
+    if (!d) err("atom_data: set_domain first");
+    if (a->n() == 0) err("no atoms");
+    int T = (int)std::max(a->mass.size(), a->charge.size());
+    for (int32_t t : a->type) T = std::max(T, t + 1);
+    std::vector<double> mass(T, 0.0), charge(T, 0.0);
+    for (int t = 0; t < T; ++t) {
+      mass[t] = t < (int)a->mass.size() ? a->mass[t] : 0.0;
+      charge[t] = t < (int)a->charge.size() ? a->charge[t] : 0.0;
+    }
+    cvr_ctx *ctx = nullptr;
+    int rc = cvr_create(&ctx, d->lo, d->hi, d->bc, T, mass.data(), charge.data(), 0);
+    if (rc) err("cvr_create failed (" + std::to_string(rc) + ")");
+    auto check = [&](int r) {
+      if (r) {
+        char buf[512];
+        cvr_last_error(ctx, buf, sizeof(buf));
+        const std::string msg = buf;
+        cvr_destroy(ctx);
+        err("B200 path: " + msg);
+      }
+    };
+    check(cvr_set_precision(ctx, m.precision));
+    const int policy = nl->rebuild_test ? CVR_REBUILD_EVERY_STEP : m.policy;
+    check(cvr_set_neighborlist(ctx, nl->cutoff, nl->coef, a->ghost_cutoff, policy));
+    for (Force_field *f : m.force_field) {
+      if (auto *lj = dynamic_cast<Lj *>(f)) {
+        std::vector<double> eps, sig, cut;
+        bool use_cut = false;
+        lj_tables(*lj, T, eps, sig, cut, use_cut);
+        check(cvr_set_lj(ctx, lj->cutoff, eps.data(), sig.data(), use_cut ? cut.data() : nullptr,
+                         lj->ignore_intra ? 1 : 0));
+      } else if (auto *er = dynamic_cast<Ewald_r *>(f)) {
+        std::vector<double> lam(T * T, 1.0);
+        for (int i = 0; i < T; ++i)
+          for (int j = 0; j < T; ++j) lam[i * T + j] = elem(er->lambda, i, j, 1.0);
+        check(cvr_set_ewald_r(ctx, er->alpha, er->k_e, er->lambda_on ? lam.data() : nullptr, -1.0));
+      } else if (auto *ek = dynamic_cast<Ewald_k *>(f)) {
+        check(cvr_set_ewald_k(ctx, ek->alpha, ek->kmax[0], ek->kmax[1], ek->kmax[2], ek->k_e));
+      }
+    }
+    check(cvr_set_integrator(ctx, m.dt, a->k_b > 0 ? a->k_b : 1.0));
+    bool any_mol = false;
+    for (int32_t v : a->mol) any_mol = any_mol || v >= 0;
+    check(cvr_set_state(ctx, a->n(), a->pos.data(), a->vel.data(), a->type.data(), any_mol ? a->mol.data() : nullptr));
+    const int64_t nsteps = m.final_step - m.initial_step;
+    const int64_t every = m.thermo_step > 0 ? m.thermo_step : 0;
+    std::vector<double> thermo((size_t)std::max<int64_t>(1, every > 0 ? nsteps / every : 1) * CVR_N_THERMO);
+    check(cvr_run(ctx, nsteps, every, every > 0 ? thermo.data() : nullptr));
+    check(cvr_get_state(ctx, a->pos.data(), a->vel.data(), nullptr));
+    if (!m.thermo_file.empty() && every > 0) {
+      const std::string p = (m.thermo_file[0] == '/') ? m.thermo_file : dir + "/" + m.thermo_file;
+      FILE *tf = std::fopen(p.c_str(), "w");
+      if (!tf) err("cannot write " + p);
+      std::fprintf(tf, "# step ke temperature e_lj e_ewald_r e_ewald_k e_self virial pressure builds\n");
+      for (int64_t r = 0; r < nsteps / every; ++r) {
+        for (int q = 0; q < CVR_N_THERMO; ++q)
+          std::fprintf(tf, q ? " %.17g" : "%.17g", thermo[(size_t)r * CVR_N_THERMO + q]);
+        std::fprintf(tf, "\n");
+      }
+      std::fclose(tf);
+    }
+    if (!m.state_file.empty()) {
+      std::vector<double> acc((size_t)a->n() * 3);
+      check(cvr_get_state(ctx, nullptr, nullptr, acc.data()));
+      const std::string p = (m.state_file[0] == '/') ? m.state_file : dir + "/" + m.state_file;
+      FILE *sf = std::fopen(p.c_str(), "wb");
+      if (!sf) err("cannot write " + p);
+      const int64_t n = a->n();
+      std::fwrite(&n, 8, 1, sf);
+      std::fwrite(a->pos.data(), 8, (size_t)n * 3, sf);
+      std::fwrite(a->vel.data(), 8, (size_t)n * 3, sf);
+      std::fwrite(acc.data(), 8, (size_t)n * 3, sf);
+      std::fclose(sf);
+    }
+    cvr_destroy(ctx);
+    m.initial_step = m.final_step;
+  }
+
+  void execute() {
+    std::vector<Line> lines = lex(path);
+    for (Line &L : lines) {
+      cur = &L;
+      const std::string first = word();
+      if (first == "exit") break;
+      if (first == "real" || first == "int") {
+        const std::string nm = word();
+        double v = real();
+        if (first == "int") v = std::floor(v);
+        vars[nm] = v;
+        continue;
+      }
+      if (first == "domain" || first == "atom_data" || first == "neighborlist" || first == "force_field" ||
+          first == "md_simulator" || first == "writer" || first == "constraint" || first == "unique") {
+        const std::string type = word();
+        const std::string nm = word();
+        create(first, type, nm);
+        cur->pos = cur->tok.size();
+        continue;
+      }
+      auto it = objects.find(first);
+      if (it == objects.end()) err("unknown command or object '" + first + "'");
+      Object *o = it->second.get();
+      if (auto *d = dynamic_cast<Domain *>(o)) read_domain(*d);
+      else if (auto *a = dynamic_cast<Atom_data *>(o)) read_atom_data(*a);
+      else if (auto *nl = dynamic_cast<Neighborlist *>(o)) read_neighborlist(*nl);
+      else if (auto *lj = dynamic_cast<Lj *>(o)) read_lj(*lj);
+      else if (auto *er = dynamic_cast<Ewald_r *>(o)) read_ewald_r(*er);
+      else if (auto *ek = dynamic_cast<Ewald_k *>(o)) read_ewald_k(*ek);
+      else if (auto *m = dynamic_cast<Md_simulator *>(o)) read_md(*m);
+    }
+  }
+};
+
+}  // namespace
+
+extern "C" int cvr_casl_run_file(const char *path, char *err, size_t err_len) {
+  if (err && err_len) err[0] = '\0';
+  if (!path) return CVR_ERR_INVALID;
+  try {
+    Script s;
+    s.path = path;
+    s.dir = dir_of(path);
+    s.execute();
+  } catch (const std::exception &e) {
+    if (err && err_len) std::snprintf(err, err_len, "%s", e.what());
+    return CVR_ERR_INVALID;
+  }
+  return CVR_OK;
+}

@@ -162,6 +162,19 @@ int cvr_get_info(const cvr_ctx *ctx, int64_t *out, int len);
 int cvr_set_kernel_timing(cvr_ctx *ctx, int on);
 int cvr_kernel_time(cvr_ctx *ctx, int kind, double *ms, int64_t *launches);
 
+/* ------------------------------------------------------------------ CASL */
+/* Run a CASL script that uses the hot-path objects with the reference's own
+ * keywords (domain box, atom_data basic, neighborlist basic, force_field lj /
+ * electrostatic_ewald_r / electrostatic_ewald_k, md_simulator basic, real/int
+ * variables); `sim run` advances the system on the GPU.  Extensions on
+ * md_simulator: precision mixed|fp64, rebuild_policy displacement|reference,
+ * thermo_step N, thermo_file "f", state_file "f" (binary: int64 n, then n*3
+ * FP64 positions, velocities, accelerations in id order).  Off-path objects
+ * and keywords are rejected with a message in err.
+ * Replaces: CAVIAR::execute -> Input::read for these objects
+ * (src/caviar/CAVIAR.cpp:70-88, interpreter/input.cpp:128-199). */
+int cvr_casl_run_file(const char *path, char *err, size_t err_len);
+
 /* ---------------------------------------------------------- no allocation */
 /* Capacity, in complex doubles (16 B each), of the fixed device array behind
  * cvr_structure_factor_noalloc: 262144 = 4 MiB per GPU that loads the library. */
