@@ -27,7 +27,9 @@ EXPORTED = ["cvr_create", "cvr_destroy", "cvr_set_neighborlist", "cvr_set_lj", "
             "cvr_set_integrator", "cvr_set_precision", "cvr_set_state", "cvr_build_neighbors", "cvr_compute_forces",
             "cvr_run", "cvr_get_state", "cvr_get_pairs", "cvr_get_sk", "cvr_get_scalars", "cvr_last_error",
             "cvr_launch_count", "cvr_get_stream", "cvr_get_info", "cvr_set_kernel_timing", "cvr_kernel_time",
-            "cvr_structure_factor_noalloc", "cvr_casl_run_file"]
+            "cvr_structure_factor_noalloc", "cvr_casl_run_file", "cvr_batch_create", "cvr_batch_destroy",
+            "cvr_batch_set_forces", "cvr_batch_set_state", "cvr_batch_run", "cvr_batch_get_state", "cvr_batch_info",
+            "cvr_batch_last_error", "cvr_batch_stream"]
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int32)
@@ -256,3 +258,91 @@ class Simulation:
         n = ctypes.c_int64(0)
         self._check(self.L.cvr_kernel_time(self.h, kind, ctypes.byref(ms), ctypes.byref(n)))
         return ms.value, n.value
+
+
+class Batch:
+    """Many small periodic replicas on one GPU (cvr_batch_* of the C ABI)."""
+
+    N_OUT = 8
+    OUT_KEYS = ["ke", "e_lj", "e_ewald_r", "e_ewald_k", "e_self", "virial", "temperature", "steps"]
+
+    def __init__(self, n_atoms, box, mass, charge, device: int = 0):
+        L = load()
+        vp = ctypes.c_void_p
+        L.cvr_batch_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int, vp, vp, ctypes.c_int, vp, vp, ctypes.c_int]
+        L.cvr_batch_destroy.argtypes = [vp]
+        L.cvr_batch_destroy.restype = None
+        L.cvr_batch_set_forces.argtypes = [vp, vp, vp, vp, vp, ctypes.c_double, ctypes.c_int, ctypes.c_double,
+                                           ctypes.c_double]
+        L.cvr_batch_set_state.argtypes = [vp, vp, vp, vp]
+        L.cvr_batch_run.argtypes = [vp, ctypes.c_int64, vp]
+        L.cvr_batch_get_state.argtypes = [vp, vp, vp, vp]
+        L.cvr_batch_info.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), ctypes.c_int]
+        L.cvr_batch_last_error.argtypes = [vp, ctypes.c_char_p, ctypes.c_size_t]
+        L.cvr_batch_stream.argtypes = [vp]
+        L.cvr_batch_stream.restype = vp
+        self.L = L
+        self.n = np.ascontiguousarray(n_atoms, np.int64)
+        self.box = np.ascontiguousarray(box, np.float64)
+        self.n_rep = len(self.n)
+        self.n_total = int(self.n.sum())
+        m = np.ascontiguousarray(mass, np.float64)
+        q = np.ascontiguousarray(charge, np.float64)
+        h = vp()
+        rc = L.cvr_batch_create(ctypes.byref(h), self.n_rep, _ptr(self.n), _ptr(self.box), len(m), _ptr(m), _ptr(q),
+                                device)
+        if rc != OK:
+            raise CvrError(rc, "cvr_batch_create failed")
+        self.h = h
+
+    def _check(self, rc):
+        if rc != OK:
+            buf = ctypes.create_string_buffer(512)
+            self.L.cvr_batch_last_error(self.h, buf, 512)
+            raise CvrError(rc, buf.value.decode(errors="replace"))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.cvr_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_forces(self, eps, sigma, rc_lj, rc_r, alpha, kmax, k_e=1.0, dt=0.005):
+        self._keep = [np.ascontiguousarray(x, np.float64) for x in (eps, sigma, rc_lj, rc_r)]
+        e, sg, rl, rr = self._keep
+        self._check(self.L.cvr_batch_set_forces(self.h, _ptr(e), _ptr(sg), _ptr(rl), _ptr(rr), alpha, kmax, k_e, dt))
+
+    def set_state(self, pos, vel, typ):
+        pos = np.ascontiguousarray(pos, np.float64)
+        vel = np.ascontiguousarray(vel, np.float64)
+        typ = np.ascontiguousarray(typ, np.int32)
+        self._check(self.L.cvr_batch_set_state(self.h, _ptr(pos), _ptr(vel), _ptr(typ)))
+
+    def run(self, nsteps: int):
+        out = np.zeros((self.n_rep, self.N_OUT))
+        self._check(self.L.cvr_batch_run(self.h, nsteps, _ptr(out)))
+        return out
+
+    def state(self):
+        pos = np.zeros((self.n_total, 3))
+        vel = np.zeros((self.n_total, 3))
+        acc = np.zeros((self.n_total, 3))
+        self._check(self.L.cvr_batch_get_state(self.h, _ptr(pos), _ptr(vel), _ptr(acc)))
+        return pos, vel, acc
+
+    def info(self):
+        v = (ctypes.c_int64 * 64)()
+        self._check(self.L.cvr_batch_info(self.h, v, 64))
+        n_cls = int(v[2])
+        classes = [dict(replicas=int(v[3 + 4 * c]), nmax=int(v[4 + 4 * c]), threads=int(v[5 + 4 * c]),
+                        atoms_per_thread=int(v[6 + 4 * c])) for c in range(n_cls)]
+        return {"n_rep": int(v[0]), "atoms": int(v[1]), "classes": classes}
+
+    @property
+    def stream(self) -> int:
+        return int(self.L.cvr_batch_stream(self.h) or 0)

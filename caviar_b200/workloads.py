@@ -188,3 +188,61 @@ def config_ions_8000(seed: int = 2) -> MDSystem:
 def config_lj_1m(seed: int = 3) -> MDSystem:
     """1,048,576 LJ atoms, FCC 64^3 cells, rho* = 0.8442, T* = 0.72, rc 2.5, skin 0.3."""
     return fcc_lattice(64, 0.8442, 0.72, seed)
+
+
+@dataclasses.dataclass
+class ReplicaBatch:
+    """Many small periodic LJ + charge replicas (one system per box)."""
+    n: np.ndarray  # (R,) atoms per replica
+    box: np.ndarray  # (R,) cube edge
+    pos: np.ndarray  # (sum n, 3), replica order
+    vel: np.ndarray
+    type: np.ndarray  # 0 neutral, 1 q=+1, 2 q=-1
+    temperature: np.ndarray  # (R,)
+    rc_lj: np.ndarray
+    rc_r: np.ndarray
+    mass: np.ndarray = dataclasses.field(default_factory=lambda: np.ones(3))
+    charge: np.ndarray = dataclasses.field(default_factory=lambda: np.array([0.0, 1.0, -1.0]))
+    epsilon: np.ndarray = dataclasses.field(default_factory=lambda: np.ones((3, 3)))
+    sigma: np.ndarray = dataclasses.field(default_factory=lambda: np.ones((3, 3)))
+    alpha: float = 0.35
+    kmax: int = 6
+    k_e: float = 1.0
+    dt: float = 0.005
+
+    @property
+    def offsets(self) -> np.ndarray:
+        return np.concatenate([[0], np.cumsum(self.n)])
+
+
+def replica_batch(n_rep: int = 1024, seed: int = 4, n_min: int = 64, n_max: int = 2048, density: float = 0.8,
+                  lj_cutoff: float = 2.5, sizes=None) -> ReplicaBatch:
+    """n_rep replicas, atom counts uniform in [n_min, n_max], rho* = 0.8, half
+    the atoms charged +-1 (net neutral), T uniform in [0.7, 1.5].  Atoms start
+    on a simple-cubic grid (random subset of sites, small jitter).  Cutoffs:
+    LJ min(2.5, L/2); Ewald real space L/2 (the minimum image; every box here
+    is smaller than twice a 9-sigma real-space cutoff).  sizes, when given,
+    fixes the atom counts (and n_rep)."""
+    rng = np.random.default_rng(seed)
+    ns = rng.integers(n_min, n_max + 1, size=n_rep) if sizes is None else np.asarray(sizes, np.int64)
+    boxes = (ns / density) ** (1.0 / 3.0)
+    pos, vel, typ = [], [], []
+    temps = rng.uniform(0.7, 1.5, size=len(ns))
+    for n, L, T in zip(ns, boxes, temps):
+        m = int(np.ceil(n ** (1.0 / 3.0)))
+        g = (np.arange(m) + 0.5) * (L / m)
+        sites = np.stack(np.meshgrid(g, g, g, indexing="ij"), axis=-1).reshape(-1, 3)
+        p = sites[rng.choice(len(sites), size=n, replace=False)]
+        p = (p + rng.uniform(-0.05, 0.05, size=p.shape)) % L
+        t = np.zeros(n, np.int32)
+        nq = (n // 2) // 2
+        idx = rng.permutation(n)
+        t[idx[:nq]] = 1
+        t[idx[nq:2 * nq]] = 2
+        v = maxwell_boltzmann(n, T, rng)
+        pos.append(p)
+        vel.append(v)
+        typ.append(t)
+    return ReplicaBatch(n=ns.astype(np.int64), box=boxes, pos=np.concatenate(pos), vel=np.concatenate(vel),
+                        type=np.concatenate(typ), temperature=temps, rc_lj=np.minimum(lj_cutoff, boxes / 2),
+                        rc_r=boxes / 2)

@@ -162,6 +162,41 @@ int cvr_get_info(const cvr_ctx *ctx, int64_t *out, int len);
 int cvr_set_kernel_timing(cvr_ctx *ctx, int on);
 int cvr_kernel_time(cvr_ctx *ctx, int kind, double *ms, int64_t *launches);
 
+/* -------------------------------------------------------- batched replicas */
+/* Many small independent periodic boxes advanced together: one persistent
+ * CTA per replica for all steps, every replica in one CUDA graph launch, the
+ * threads per CTA of each size class picked by timing candidates on the
+ * state (autotuner).  No reference counterpart: the reference runs one system
+ * per process and its one-ghost-image scheme cannot hold boxes smaller than
+ * twice the list radius (exchange_ghost_single_md_domain.cpp:59-99).
+ * Physics per replica: LJ with the reference's linear force shift
+ * (lj.cpp:439-448) up to rc_lj, Ewald real space (electrostatic_ewald_r.cpp:196-198)
+ * up to rc_r, both <= L/2 (minimum image), Ewald k space over the reference's
+ * k-set (initialize.cpp:184-222, electrostatic_ewald_k.cpp:197-234), velocity
+ * Verlet.  Mixed precision: FP32 pair and k-space math on hi/lo FP32
+ * coordinates, FP64 positions, velocities, S(k) and energies.
+ * Limits: 2048 atoms per replica, 4 types, k_max <= 6. */
+typedef struct cvr_batch cvr_batch;
+#define CVR_BATCH_N_OUT 8 /* per replica: ke, e_lj, e_ewald_r, e_ewald_k, e_self, virial, temperature, steps */
+/* n_atoms, box_len: n_rep each (cubes [0, L)); mass, charge: n_types. */
+int cvr_batch_create(cvr_batch **out, int n_rep, const int64_t *n_atoms, const double *box_len, int n_types,
+                     const double *mass, const double *charge, int device);
+void cvr_batch_destroy(cvr_batch *b);
+/* eps, sigma: n_types^2; rc_lj, rc_r: n_rep each (<= L/2); alpha; k_max; k_e; dt. */
+int cvr_batch_set_forces(cvr_batch *b, const double *eps, const double *sigma, const double *rc_lj,
+                         const double *rc_r, double alpha, int kmax, double k_e, double dt);
+/* All replicas' atoms concatenated in replica order: pos, vel n*3 (host), type n. */
+int cvr_batch_set_state(cvr_batch *b, const double *pos, const double *vel, const int32_t *type);
+/* nsteps steps of every replica in one graph launch (the first call tunes the
+ * launch shapes); out (host, nullable): n_rep * CVR_BATCH_N_OUT at the end. */
+int cvr_batch_run(cvr_batch *b, int64_t nsteps, double *out);
+/* pos, vel, acc (each nullable) n*3; acc = FP32 force / mass of the current positions (after a run). */
+int cvr_batch_get_state(cvr_batch *b, double *pos, double *vel, double *acc);
+/* n_rep, atoms, classes, then per class: replicas, largest replica, threads per CTA, atoms per thread. */
+int cvr_batch_info(const cvr_batch *b, int64_t *out, int len);
+int cvr_batch_last_error(const cvr_batch *b, char *buf, size_t len);
+void *cvr_batch_stream(const cvr_batch *b);
+
 /* ------------------------------------------------------------------ CASL */
 /* Run a CASL script that uses the hot-path objects with the reference's own
  * keywords (domain box, atom_data basic, neighborlist basic, force_field lj /

@@ -37,6 +37,7 @@
 #include <string.h>
 
 /* reference constants: include/caviar/utility/macro_constants.h:20-30 */
+#define ORC_PI 3.14159265358979323846
 #define ORC_2PI 6.28318530717958647692
 #define ORC_4PI 12.56637061435917295384
 #define ORC_PIS_INV 0.56418958354775628695
@@ -861,4 +862,109 @@ int orc_get_scalars(orc_sys *s, double *out) {
   out[7] = (double)s->ng;
   out[8] = (double)(3 * s->n - n_r_df);
   return 0;
+}
+
+/* ------------------------------------------------------------- replicas */
+
+/* Minimum-image all-pairs forces for one small periodic box.  The pair
+ * formulas are the reference's (lj.cpp:439-448, electrostatic_ewald_r.cpp:196-198);
+ * the k space is the reference's k-set and force (initialize.cpp:184-222,
+ * electrostatic_ewald_k.cpp:197-234), with S(k) summed over all atoms. */
+void orc_replica_forces(int64_t n, const double *pos, const int32_t *type, double L, int nt, const double *mass,
+                        const double *charge, const double *eps, const double *sigma, double rc_lj, double alpha,
+                        double rc_r, int kmax, double k_e, double *acc, double *energy) {
+  double e_lj = 0, e_r = 0, e_k = 0, e_self = 0, vir = 0;
+  const double rc2 = rc_lj * rc_lj, rr2 = rc_r * rc_r, alpha_sq = alpha * alpha;
+  for (int64_t i = 0; i < 3 * n; ++i) acc[i] = 0;
+  for (int64_t i = 0; i < n; ++i) {
+    const int ti = type[i];
+    double f[3] = {0, 0, 0};
+    for (int64_t j = 0; j < n; ++j) {
+      if (j == i) continue;
+      const int tj = type[j];
+      double d[3];
+      for (int a = 0; a < 3; ++a) {
+        d[a] = pos[3 * j + a] - pos[3 * i + a];
+        d[a] -= L * rint(d[a] / L);
+      }
+      const double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+      double c = 0;
+      const double e = eps[ti * nt + tj], sg = sigma[ti * nt + tj];
+      if (r2 <= rc2 && e != 0) {
+        const double rcinv = 1 / rc2;
+        const double c2 = sg * sg * rcinv, c6 = c2 * c2 * c2, c12 = c6 * c6;
+        const double r2i = 1 / r2, s2 = sg * sg * r2i, s6 = s2 * s2 * s2, s12 = s6 * s6;
+        c += 4 * e * (-12 * s12 * r2i + 6 * s6 * r2i + 12 * c12 * rcinv - 6 * c6 * rcinv);
+        const double g = 4 * e * (12 * c12 - 6 * c6);
+        e_lj += 0.5 * (4 * e * (s12 - s6) - 4 * e * (c12 - c6) + g * (r2 - rc2) / (2 * rc2));
+      }
+      const double qq = k_e * charge[ti] * charge[tj];
+      if (qq != 0 && r2 <= rr2 && r2 > 0) {
+        const double r = sqrt(r2);
+        const double s = (2 * alpha * ORC_PIS_INV * exp(-alpha_sq * r2) + erfc(alpha * r) / r) / r2;
+        c -= qq * s;
+        e_r += 0.5 * qq * erfc(alpha * r) / r;
+      }
+      for (int a = 0; a < 3; ++a) f[a] += c * d[a];
+      vir += -0.5 * c * r2;
+    }
+    const double mi = mass[ti] == 0 ? 0 : 1 / mass[ti];
+    for (int a = 0; a < 3; ++a) acc[3 * i + a] = f[a] * mi;
+  }
+  if (kmax > 0) {
+    const double two_pi = ORC_2PI, V = L * L * L;
+    const double four_alpha2_inv = 1.0 / (4.0 * alpha_sq);
+    const int64_t used = (int64_t)(2 * kmax) * (2 * kmax) * (2 * kmax);
+    int64_t m = 0;
+    for (int a = -kmax; a <= kmax && m < used; ++a)
+      for (int b = -kmax; b <= kmax && m < used; ++b)
+        for (int cz = -kmax; cz <= kmax && m < used; ++cz) {
+          const double k0 = two_pi * a / L, k1 = two_pi * b / L, k2 = two_pi * cz / L;
+          const double ksq = k0 * k0 + k1 * k1 + k2 * k2;
+          if (ksq == 0) continue;
+          ++m;
+          const double fk = (1.0 / ksq) * exp(-ksq * four_alpha2_inv);
+          double complex S = 0;
+          for (int64_t j = 0; j < n; ++j) {
+            const double kr = k0 * pos[3 * j] + k1 * pos[3 * j + 1] + k2 * pos[3 * j + 2];
+            S += charge[type[j]] * cexp(I * kr);
+          }
+          e_k += (2 * ORC_PI / V) * k_e * fk * (creal(S) * creal(S) + cimag(S) * cimag(S));
+          for (int64_t i = 0; i < n; ++i) {
+            const int ti = type[i];
+            const double kr = k0 * pos[3 * i] + k1 * pos[3 * i + 1] + k2 * pos[3 * i + 2];
+            const double t = cimag(conj(S) * cexp(I * kr));
+            const double coef = k_e * charge[ti] * (4 * ORC_PI / V) * fk * t;
+            const double mi = mass[ti] == 0 ? 0 : 1 / mass[ti];
+            acc[3 * i] += coef * k0 * mi;
+            acc[3 * i + 1] += coef * k1 * mi;
+            acc[3 * i + 2] += coef * k2 * mi;
+          }
+        }
+    double q2 = 0;
+    for (int64_t j = 0; j < n; ++j) q2 += charge[type[j]] * charge[type[j]];
+    e_self = -ORC_PIS_INV * alpha * q2 * k_e;
+  }
+  if (energy) {
+    energy[0] = e_lj;
+    energy[1] = e_r;
+    energy[2] = e_k;
+    energy[3] = e_self;
+    energy[4] = vir;
+  }
+}
+
+void orc_replica_run(int64_t n, double *pos, double *vel, double *acc, const int32_t *type, double L, int nt,
+                     const double *mass, const double *charge, const double *eps, const double *sigma, double rc_lj,
+                     double alpha, double rc_r, int kmax, double k_e, double dt, int64_t nsteps) {
+  orc_replica_forces(n, pos, type, L, nt, mass, charge, eps, sigma, rc_lj, alpha, rc_r, kmax, k_e, acc, NULL);
+  for (int64_t s = 0; s < nsteps; ++s) {
+    for (int64_t i = 0; i < 3 * n; ++i) {
+      vel[i] += 0.5 * dt * acc[i];
+      pos[i] += dt * vel[i];
+      pos[i] -= L * floor(pos[i] / L);
+    }
+    orc_replica_forces(n, pos, type, L, nt, mass, charge, eps, sigma, rc_lj, alpha, rc_r, kmax, k_e, acc, NULL);
+    for (int64_t i = 0; i < 3 * n; ++i) vel[i] += 0.5 * dt * acc[i];
+  }
 }

@@ -81,6 +81,22 @@ int orc_get_scalars(orc_sys *s, double *out);
 /* Evaluate energies (scalars 2..5) at the current positions and list. */
 int orc_energy(orc_sys *s);
 
+/* ---------------------------------------------------------------- replicas
+ * Small periodic boxes (L < 2 rl, which the reference's one-ghost-image
+ * scheme cannot represent): minimum-image all-pairs LJ (linear force shift,
+ * cutoff rc_lj) + Ewald real space with cutoff rc_r (<= L/2), Ewald k space
+ * over the reference's k-set (first (2k)^3 vectors of [-k,k]^3 \ {0}), FP64.
+ * pos/vel/acc: n*3; type: n; box: L (cube [0, L)).  Writes acc and, when
+ * energy is non-NULL, {e_lj, e_ewald_r, e_ewald_k, e_self, virial}. */
+void orc_replica_forces(int64_t n, const double *pos, const int32_t *type, double L, int n_types,
+                        const double *mass, const double *charge, const double *eps, const double *sigma,
+                        double rc_lj, double alpha, double rc_r, int kmax, double k_e, double *acc,
+                        double *energy);
+/* nsteps velocity-Verlet steps (kick, drift, wrap into [0, L), force, kick). */
+void orc_replica_run(int64_t n, double *pos, double *vel, double *acc, const int32_t *type, double L, int n_types,
+                     const double *mass, const double *charge, const double *eps, const double *sigma,
+                     double rc_lj, double alpha, double rc_r, int kmax, double k_e, double dt, int64_t nsteps);
+
 #ifdef __cplusplus
 }
 #endif

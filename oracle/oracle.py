@@ -171,6 +171,41 @@ class Oracle:
         return dict(zip(keys, out.tolist()))
 
 
+def replica_forces(n, pos, typ, L, mass, charge, eps, sigma, rc_lj, alpha, rc_r, kmax, k_e=1.0):
+    """FP64 minimum-image forces of one small replica; returns (acc, energies)."""
+    Lb = lib()
+    f = Lb.orc_replica_forces
+    f.argtypes = [ctypes.c_int64, _dp, _ip, ctypes.c_double, ctypes.c_int, _dp, _dp, _dp, _dp, ctypes.c_double,
+                  ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_double, _dp, _dp]
+    f.restype = None
+    pos = np.ascontiguousarray(pos, np.float64)
+    typ = np.ascontiguousarray(typ, np.int32)
+    acc = np.zeros((n, 3))
+    en = np.zeros(5)
+    arrs = [np.ascontiguousarray(x, np.float64) for x in (mass, charge, eps, sigma)]
+    f(n, _d(pos), typ.ctypes.data_as(_ip), L, len(arrs[0]), *[_d(a) for a in arrs], rc_lj, alpha, rc_r, kmax, k_e,
+      _d(acc), _d(en))
+    return acc, dict(zip(["e_lj", "e_ewald_r", "e_ewald_k", "e_self", "virial"], en.tolist()))
+
+
+def replica_run(n, pos, vel, typ, L, mass, charge, eps, sigma, rc_lj, alpha, rc_r, kmax, k_e, dt, nsteps):
+    """FP64 velocity-Verlet run of one small replica; returns (pos, vel, acc)."""
+    Lb = lib()
+    f = Lb.orc_replica_run
+    f.argtypes = [ctypes.c_int64, _dp, _dp, _dp, _ip, ctypes.c_double, ctypes.c_int, _dp, _dp, _dp, _dp,
+                  ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                  ctypes.c_int64]
+    f.restype = None
+    p = np.array(pos, np.float64)
+    v = np.array(vel, np.float64)
+    a = np.zeros((n, 3))
+    typ = np.ascontiguousarray(typ, np.int32)
+    arrs = [np.ascontiguousarray(x, np.float64) for x in (mass, charge, eps, sigma)]
+    f(n, _d(p), _d(v), _d(a), typ.ctypes.data_as(_ip), L, len(arrs[0]), *[_d(x) for x in arrs], rc_lj, alpha, rc_r,
+      kmax, k_e, dt, nsteps)
+    return p, v, a
+
+
 # --------------------------------------------------------------- reference
 
 
