@@ -71,6 +71,16 @@ __device__ __forceinline__ float2 conjf_if(float2 a, bool c) {
   return a;
 }
 
+// erfc(x) for x >= 0 from its rational-exponential approximation
+// erfc(x) = t (a1 + t (a2 + t (a3 + t (a4 + t a5)))) exp(-x^2), t = 1 / (1 + p x),
+// absolute error below 1.5e-7 (Abramowitz & Stegun, Handbook of Mathematical
+// Functions, 1964, eq. 7.1.26).  ex = exp(-x^2), which the force needs anyway.
+__device__ __forceinline__ float erfc_as(float x, float ex) {
+  const float t = __fdividef(1.f, fmaf(0.3275911f, x, 1.f));
+  return t * fmaf(t, fmaf(t, fmaf(t, fmaf(t, 1.061405429f, -1.453152027f), 1.421413741f), -0.284496736f),
+                  0.254829592f) * ex;
+}
+
 template <int TPB, int NV>
 __device__ __forceinline__ void block_sum(double (&v)[NV], double *red, double *out) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -143,8 +153,9 @@ __device__ void batch_forces(const BatchDev &p, const Smem &S, int r, int n, dou
       }
       if (le.w != 0.f && r2 <= rr2) {
         const float rinv = rsqrtf(r2), rr = r2 * rinv;
-        const float er = erfcf(alpha * rr);
-        c -= le.w * (tas * __expf(-alpha2 * r2) + er * rinv) * (rinv * rinv);
+        const float ex = __expf(-alpha2 * r2);
+        const float er = erfc_as(alpha * rr, ex);
+        c -= le.w * (tas * ex + er * rinv) * (rinv * rinv);
         if (EV) ev[1] += 0.5 * (double)(le.w * er * rinv);
       }
       f[m].x += c * d[0];
@@ -243,19 +254,20 @@ __device__ void batch_forces(const BatchDev &p, const Smem &S, int r, int n, dou
         if (mm == abs(run.nx)) px = tx[mm];
         if (mm == abs(run.ny)) py = ty[mm];
       }
-      const float2 pxy = cmulf(conjf_if(px, run.nx < 0), conjf_if(py, run.ny < 0));
+      float2 pz = tz[0];
+#pragma unroll
+      for (int mm = 0; mm < KP; ++mm)
+        if (mm == abs(run.nz0)) pz = tz[mm];
+      // e^{i k.r} along the run: start at nz0, then one step of e^{i 2 pi z / L} per k
+      float2 ph = cmulf(cmulf(conjf_if(px, run.nx < 0), conjf_if(py, run.ny < 0)), conjf_if(pz, run.nz0 < 0));
+      const float2 ez = tz[1];
       float tsum = 0.f;
       for (int u = 0; u < run.len; ++u) {
-        const int nz = run.nz0 + u;
-        float2 pz = tz[0];
-#pragma unroll
-        for (int mm = 0; mm < KP; ++mm)
-          if (mm == abs(nz)) pz = tz[mm];
-        const float2 ph = cmulf(pxy, conjf_if(pz, nz < 0));
         const float2 A = S.ak[run.k0 + u];
         const float t = A.x * ph.y + A.y * ph.x;
         tsum += t;
-        fz += (float)nz * t;
+        fz += (float)(run.nz0 + u) * t;
+        ph = cmulf(ph, ez);
       }
       fx += (float)run.nx * tsum;
       fy += (float)run.ny * tsum;

@@ -246,3 +246,43 @@ def replica_batch(n_rep: int = 1024, seed: int = 4, n_min: int = 64, n_max: int 
     return ReplicaBatch(n=ns.astype(np.int64), box=boxes, pos=np.concatenate(pos), vel=np.concatenate(vel),
                         type=np.concatenate(typ), temperature=temps, rc_lj=np.minimum(lj_cutoff, boxes / 2),
                         rc_r=boxes / 2)
+
+
+@dataclasses.dataclass
+class AdjointSystem:
+    """One periodic cube for the trajectory adjoint: LJ + Ewald (explicit
+    real-space cutoff, minimum image), parameters per type."""
+    box: float
+    pos: np.ndarray  # (N, 3)
+    vel: np.ndarray
+    type: np.ndarray  # (N,) int32
+    mass: np.ndarray  # (T,)
+    charge: np.ndarray  # (T,)
+    epsilon: np.ndarray  # (T, T) symmetric
+    sigma: np.ndarray  # (T, T) symmetric
+    rc_lj: float = 2.5
+    alpha: float = 0.4
+    rc_r: float = 8.0
+    kmax: int = 7
+    k_e: float = 1.0
+    dt: float = 0.002
+
+
+def adjoint_mixture(ncell: int = 10, density: float = 0.8442, temperature: float = 1.0, seed: int = 5,
+                    jitter: float = 0.05, rc_lj: float = 2.5, alpha: float = 0.4, rc_r: float = 8.0,
+                    kmax: int = 7) -> AdjointSystem:
+    """Two-species LJ + charge mixture: 4 ncell^3 atoms on an FCC lattice at
+    rho* = 0.8442 (ncell = 10 gives N = 4000, L = 16.796), half A (q = +0.5),
+    half B (q = -0.5) at random sites; eps_AA 1.0, eps_BB 0.5, eps_AB 0.75,
+    sigma_AA 1.0, sigma_BB 0.88, sigma_AB 0.94 (Lorentz-Berthelot mean);
+    Maxwell-Boltzmann velocities at T*; dt 0.002.  Ewald alpha 0.4 with a
+    real-space cutoff of 8 sigma (erfc(3.2) = 6e-6) and k_max 7."""
+    base = fcc_lattice(ncell, density, temperature, seed, jitter=jitter)
+    n = base.n
+    rng = np.random.default_rng(seed + 1000)
+    typ = np.zeros(n, np.int32)
+    typ[rng.permutation(n)[: n // 2]] = 1
+    L = float(base.box[0])
+    return AdjointSystem(box=L, pos=base.pos % L, vel=base.vel, type=typ, mass=np.ones(2), charge=np.array([0.5, -0.5]),
+                         epsilon=np.array([[1.0, 0.75], [0.75, 0.5]]), sigma=np.array([[1.0, 0.94], [0.94, 0.88]]),
+                         rc_lj=min(rc_lj, L / 2), alpha=alpha, rc_r=min(rc_r, L / 2), kmax=kmax)

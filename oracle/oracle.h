@@ -97,6 +97,31 @@ void orc_replica_run(int64_t n, double *pos, double *vel, double *acc, const int
                      const double *mass, const double *charge, const double *eps, const double *sigma,
                      double rc_lj, double alpha, double rc_r, int kmax, double k_e, double dt, int64_t nsteps);
 
+/* ----------------------------------------------------------------- adjoint
+ * FP64 gradient of the trajectory loss J = (1/M) sum_{t=1..M} U(r_t) of M
+ * velocity-Verlet steps on one periodic cube (minimum image, cutoffs <= L/2):
+ * LJ (linear force shift, cutoff rc_lj), Ewald real space with an explicit
+ * cutoff rc_r, Ewald k space over the reference's k-set, self energy.
+ * eps/sigma: nt*nt symmetric; gradients of a shared off-diagonal value are
+ * written to both entries.  Forces here are F (not F/m). */
+#define ORC_ADJ_TMAX 4
+typedef struct orc_adj orc_adj;
+orc_adj *orc_adj_create(int64_t n, double L, int nt, const double *mass, const double *charge, const double *eps,
+                        const double *sigma, double rc_lj, double alpha, double rc_r, int kmax, double k_e, double dt,
+                        const int32_t *type);
+void orc_adj_destroy(orc_adj *a);
+void orc_adj_set_params(orc_adj *a, const double *eps, const double *sigma, const double *charge);
+/* energy: {lj, ewald_r, ewald_k, self}; dU_*: dU/dtheta.  Outputs nullable. */
+void orc_adj_forces(orc_adj *a, const double *pos, double *force, double *energy, double *dU_eps, double *dU_sig,
+                    double *dU_q);
+/* w = (dF/dr)^T u and u . dF/dtheta. */
+void orc_adj_force_vjp(orc_adj *a, const double *pos, const double *u, double *w, double *g_eps, double *g_sig,
+                       double *g_q);
+double orc_adj_loss(orc_adj *a, const double *pos0, const double *vel0, int64_t M, double *pos_out, double *vel_out);
+/* Checkpoints (r, v) every K steps; the reverse sweep re-runs each segment. */
+double orc_adj_loss_grad(orc_adj *a, const double *pos0, const double *vel0, int64_t M, int64_t K, double *g_pos,
+                         double *g_vel, double *g_eps, double *g_sig, double *g_q);
+
 #ifdef __cplusplus
 }
 #endif

@@ -206,6 +206,77 @@ def replica_run(n, pos, vel, typ, L, mass, charge, eps, sigma, rc_lj, alpha, rc_
     return p, v, a
 
 
+class AdjOracle:
+    """FP64 trajectory adjoint restatement (adjoint.c) for one periodic cube."""
+
+    def __init__(self, sysd):
+        """sysd: caviar_b200.workloads.AdjointSystem (or anything with its fields)."""
+        L = lib()
+        vp = ctypes.c_void_p
+        L.orc_adj_create.restype = vp
+        L.orc_adj_create.argtypes = [ctypes.c_int64, ctypes.c_double, ctypes.c_int, _dp, _dp, _dp, _dp,
+                                     ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_double,
+                                     ctypes.c_double, _ip]
+        L.orc_adj_destroy.argtypes = [vp]
+        L.orc_adj_set_params.argtypes = [vp, _dp, _dp, _dp]
+        L.orc_adj_forces.argtypes = [vp, _dp, _dp, _dp, _dp, _dp, _dp]
+        L.orc_adj_force_vjp.argtypes = [vp, _dp, _dp, _dp, _dp, _dp, _dp]
+        L.orc_adj_loss.restype = ctypes.c_double
+        L.orc_adj_loss.argtypes = [vp, _dp, _dp, ctypes.c_int64, _dp, _dp]
+        L.orc_adj_loss_grad.restype = ctypes.c_double
+        L.orc_adj_loss_grad.argtypes = [vp, _dp, _dp, ctypes.c_int64, ctypes.c_int64, _dp, _dp, _dp, _dp, _dp]
+        self.L = L
+        self.s = sysd
+        self.n = int(sysd.pos.shape[0])
+        self.nt = len(sysd.mass)
+        self._typ = np.ascontiguousarray(sysd.type, np.int32)
+        a = [np.ascontiguousarray(x, np.float64) for x in (sysd.mass, sysd.charge, sysd.epsilon, sysd.sigma)]
+        self.h = L.orc_adj_create(self.n, float(sysd.box), self.nt, *[_d(x) for x in a], sysd.rc_lj, sysd.alpha,
+                                  sysd.rc_r, sysd.kmax, sysd.k_e, sysd.dt, self._typ.ctypes.data_as(_ip))
+        if not self.h:
+            raise ValueError("orc_adj_create rejected the system")
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.L.orc_adj_destroy(self.h)
+            self.h = None
+
+    def set_params(self, eps=None, sigma=None, charge=None):
+        arr = [None if x is None else np.ascontiguousarray(x, np.float64) for x in (eps, sigma, charge)]
+        self.L.orc_adj_set_params(self.h, *[None if x is None else _d(x) for x in arr])
+
+    def forces(self, pos):
+        pos = np.ascontiguousarray(pos, np.float64)
+        nt = self.nt
+        f, e = np.zeros((self.n, 3)), np.zeros(4)
+        ge, gs, gq = np.zeros((nt, nt)), np.zeros((nt, nt)), np.zeros(nt)
+        self.L.orc_adj_forces(self.h, _d(pos), _d(f), _d(e), _d(ge), _d(gs), _d(gq))
+        return f, e, {"eps": ge, "sigma": gs, "charge": gq}
+
+    def force_vjp(self, pos, u):
+        pos = np.ascontiguousarray(pos, np.float64)
+        u = np.ascontiguousarray(u, np.float64)
+        nt = self.nt
+        w = np.zeros((self.n, 3))
+        ge, gs, gq = np.zeros((nt, nt)), np.zeros((nt, nt)), np.zeros(nt)
+        self.L.orc_adj_force_vjp(self.h, _d(pos), _d(u), _d(w), _d(ge), _d(gs), _d(gq))
+        return w, {"eps": ge, "sigma": gs, "charge": gq}
+
+    def loss(self, pos0, vel0, M):
+        p = np.ascontiguousarray(pos0, np.float64)
+        v = np.ascontiguousarray(vel0, np.float64)
+        return self.L.orc_adj_loss(self.h, _d(p), _d(v), M, None, None)
+
+    def loss_grad(self, pos0, vel0, M, K):
+        p = np.ascontiguousarray(pos0, np.float64)
+        v = np.ascontiguousarray(vel0, np.float64)
+        nt = self.nt
+        gp, gv = np.zeros((self.n, 3)), np.zeros((self.n, 3))
+        ge, gs, gq = np.zeros((nt, nt)), np.zeros((nt, nt)), np.zeros(nt)
+        J = self.L.orc_adj_loss_grad(self.h, _d(p), _d(v), M, K, _d(gp), _d(gv), _d(ge), _d(gs), _d(gq))
+        return J, {"pos": gp, "vel": gv, "eps": ge, "sigma": gs, "charge": gq}
+
+
 # --------------------------------------------------------------- reference
 
 
