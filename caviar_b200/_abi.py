@@ -29,7 +29,9 @@ EXPORTED = ["cvr_create", "cvr_destroy", "cvr_set_neighborlist", "cvr_set_lj", "
             "cvr_launch_count", "cvr_get_stream", "cvr_get_info", "cvr_set_kernel_timing", "cvr_kernel_time",
             "cvr_structure_factor_noalloc", "cvr_casl_run_file", "cvr_batch_create", "cvr_batch_destroy",
             "cvr_batch_set_forces", "cvr_batch_set_state", "cvr_batch_run", "cvr_batch_get_state", "cvr_batch_info",
-            "cvr_batch_last_error", "cvr_batch_stream"]
+            "cvr_batch_last_error", "cvr_batch_stream", "cvr_adj_create", "cvr_adj_destroy", "cvr_adj_set_params",
+            "cvr_adj_set_state", "cvr_adj_forces", "cvr_adj_force_vjp", "cvr_adj_loss", "cvr_adj_loss_grad",
+            "cvr_adj_last_error", "cvr_adj_stream"]
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int32)
@@ -346,3 +348,99 @@ class Batch:
     @property
     def stream(self) -> int:
         return int(self.L.cvr_batch_stream(self.h) or 0)
+
+
+class Adjoint:
+    """Trajectory-loss gradient on the GPU (cvr_adj_* of the C ABI).
+
+    theta vectors are laid out eps[T*T], sigma[T*T], charge[T]."""
+
+    def __init__(self, n: int, box: float, mass, precision: int = PREC_MIXED, device: int = 0):
+        L = load()
+        vp, dp = ctypes.c_void_p, ctypes.c_double
+        L.cvr_adj_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int64, dp, ctypes.c_int, vp, ctypes.c_int,
+                                     ctypes.c_int]
+        L.cvr_adj_destroy.argtypes = [vp]
+        L.cvr_adj_destroy.restype = None
+        L.cvr_adj_set_params.argtypes = [vp, vp, vp, vp, dp, dp, dp, ctypes.c_int, dp, dp]
+        L.cvr_adj_set_state.argtypes = [vp, vp, vp, vp]
+        L.cvr_adj_forces.argtypes = [vp, vp, vp, vp]
+        L.cvr_adj_force_vjp.argtypes = [vp, vp, vp, vp]
+        L.cvr_adj_loss.argtypes = [vp, ctypes.c_int64, vp, vp, vp]
+        L.cvr_adj_loss_grad.argtypes = [vp, ctypes.c_int64, ctypes.c_int64, vp, vp, vp, vp]
+        L.cvr_adj_last_error.argtypes = [vp, ctypes.c_char_p, ctypes.c_size_t]
+        L.cvr_adj_stream.argtypes = [vp]
+        L.cvr_adj_stream.restype = vp
+        self.L = L
+        self.n = int(n)
+        m = np.ascontiguousarray(mass, np.float64)
+        self.nt = len(m)
+        h = vp()
+        rc = L.cvr_adj_create(ctypes.byref(h), self.n, float(box), self.nt, _ptr(m), precision, device)
+        if rc != OK:
+            raise CvrError(rc, "cvr_adj_create failed")
+        self.h = h
+
+    @classmethod
+    def from_system(cls, s, precision: int = PREC_MIXED, device: int = 0) -> "Adjoint":
+        """From a workloads.AdjointSystem: parameters and initial state set."""
+        a = cls(len(s.pos), s.box, s.mass, precision, device)
+        a.set_params(s.charge, s.epsilon, s.sigma, s.rc_lj, s.alpha, s.rc_r, s.kmax, s.k_e, s.dt)
+        a.set_state(s.pos, s.vel, s.type)
+        return a
+
+    def _check(self, rc):
+        if rc != OK:
+            buf = ctypes.create_string_buffer(512)
+            self.L.cvr_adj_last_error(self.h, buf, 512)
+            raise CvrError(rc, buf.value.decode(errors="replace"))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.cvr_adj_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def split(self, g):
+        t = self.nt
+        return {"eps": g[:t * t].reshape(t, t), "sigma": g[t * t:2 * t * t].reshape(t, t), "charge": g[2 * t * t:]}
+
+    def set_params(self, charge, eps, sigma, rc_lj, alpha, rc_r, kmax, k_e=1.0, dt=0.002):
+        q, e, sg = (np.ascontiguousarray(x, np.float64) for x in (charge, eps, sigma))
+        self._check(self.L.cvr_adj_set_params(self.h, _ptr(q), _ptr(e), _ptr(sg), rc_lj, alpha, rc_r, kmax, k_e, dt))
+
+    def set_state(self, pos, vel, typ):
+        pos = np.ascontiguousarray(pos, np.float64)
+        vel = np.ascontiguousarray(vel, np.float64)
+        typ = np.ascontiguousarray(typ, np.int32)
+        self._check(self.L.cvr_adj_set_state(self.h, _ptr(pos), _ptr(vel), _ptr(typ)))
+
+    def forces(self):
+        f, e, g = np.zeros((self.n, 3)), np.zeros(4), np.zeros(2 * self.nt * self.nt + self.nt)
+        self._check(self.L.cvr_adj_forces(self.h, _ptr(f), _ptr(e), _ptr(g)))
+        return f, e, self.split(g)
+
+    def force_vjp(self, u):
+        u = np.ascontiguousarray(u, np.float64)
+        w, g = np.zeros((self.n, 3)), np.zeros(2 * self.nt * self.nt + self.nt)
+        self._check(self.L.cvr_adj_force_vjp(self.h, _ptr(u), _ptr(w), _ptr(g)))
+        return w, self.split(g)
+
+    def loss(self, nsteps: int):
+        J = np.zeros(1)
+        self._check(self.L.cvr_adj_loss(self.h, nsteps, _ptr(J), None, None))
+        return float(J[0])
+
+    def loss_grad(self, nsteps: int, checkpoint_every: int = 50):
+        J = np.zeros(1)
+        gp, gv = np.zeros((self.n, 3)), np.zeros((self.n, 3))
+        g = np.zeros(2 * self.nt * self.nt + self.nt)
+        self._check(self.L.cvr_adj_loss_grad(self.h, nsteps, checkpoint_every, _ptr(J), _ptr(gp), _ptr(gv), _ptr(g)))
+        out = {"pos": gp, "vel": gv}
+        out.update(self.split(g))
+        return float(J[0]), out

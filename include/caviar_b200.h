@@ -197,6 +197,41 @@ int cvr_batch_info(const cvr_batch *b, int64_t *out, int len);
 int cvr_batch_last_error(const cvr_batch *b, char *buf, size_t len);
 void *cvr_batch_stream(const cvr_batch *b);
 
+/* ---------------------------------------------------------------- adjoint */
+/* Gradient of the trajectory loss J = (1/M) sum_{t=1..M} U(r_t) of M
+ * velocity-Verlet steps (md_simulator.cpp:555-668) with respect to the
+ * initial positions and velocities, eps/sigma per type pair and per-type
+ * charges.  No reference counterpart (the reference has no gradients).
+ * One periodic cube [0, L)^3, minimum image (rc_lj, rc_r <= L/2), at most 2
+ * types; U = LJ with the reference's linear force shift (lj.cpp:439-448) +
+ * Ewald real space with cutoff rc_r (electrostatic_ewald_r.cpp:196-198) +
+ * Ewald k space over the reference's k-set (initialize.cpp:184-222) + self
+ * energy (electrostatic_ewald_k/energy.cpp:31-50).  CVR_PREC_MIXED: FP32 pair
+ * and k-space terms, FP64 sums, state and cotangents; CVR_PREC_FP64: all FP64.
+ * Parameter vectors theta: eps[T*T], sigma[T*T], charge[T]; the gradient of a
+ * shared off-diagonal value is written to both of its entries.
+ * Forces here are F (not F/m); pos/vel/force/u/w arrays are n*3 (host). */
+typedef struct cvr_adj cvr_adj;
+int cvr_adj_create(cvr_adj **out, int64_t n, double box_len, int n_types, const double *mass, int precision,
+                   int device);
+void cvr_adj_destroy(cvr_adj *a);
+/* charge[T], eps[T*T], sigma[T*T] symmetric; k_max <= 10. */
+int cvr_adj_set_params(cvr_adj *a, const double *charge, const double *eps, const double *sigma, double rc_lj,
+                       double alpha, double rc_r, int kmax, double k_e, double dt);
+/* The initial state of the loss (and the positions of the force calls). */
+int cvr_adj_set_state(cvr_adj *a, const double *pos, const double *vel, const int32_t *type);
+/* Forces at the state's positions; energy[4] = {lj, ewald_r, ewald_k, self}; dU = dU/dtheta.  Outputs nullable. */
+int cvr_adj_forces(cvr_adj *a, double *force, double *energy, double *dU);
+/* The hand-written VJP: w = (dF/dr)^T u and g = u . dF/dtheta at the state's positions. */
+int cvr_adj_force_vjp(cvr_adj *a, const double *u, double *w, double *g);
+/* J of nsteps steps (forward only); final pos/vel nullable. */
+int cvr_adj_loss(cvr_adj *a, int64_t nsteps, double *loss, double *pos_out, double *vel_out);
+/* J and dJ/d(pos0, vel0, theta), checkpoints every checkpoint_every steps. */
+int cvr_adj_loss_grad(cvr_adj *a, int64_t nsteps, int64_t checkpoint_every, double *loss, double *g_pos,
+                      double *g_vel, double *g_theta);
+int cvr_adj_last_error(const cvr_adj *a, char *buf, size_t len);
+void *cvr_adj_stream(const cvr_adj *a);
+
 /* ------------------------------------------------------------------ CASL */
 /* Run a CASL script that uses the hot-path objects with the reference's own
  * keywords (domain box, atom_data basic, neighborlist basic, force_field lj /

@@ -117,3 +117,131 @@ def test_mixture_generator():
     assert np.all((s.pos >= 0) & (s.pos < s.box))
     assert s.rc_r <= s.box / 2 and s.rc_lj <= s.box / 2
     assert s.epsilon[0, 1] == 0.75 and s.sigma[1, 1] == 0.88 and abs(s.sigma[0, 1] - 0.94) < 1e-15
+
+
+# ------------------------------------------------------------------ GPU
+
+def gpu_engine(abi, s, prec):
+    return abi.Adjoint.from_system(s, prec)
+
+
+def medium_system():
+    # 256 atoms (FCC 4^3), L = 6.72; rc_lj 2.5, rc_r 3.3 (< L/2), alpha 0.9, k_max 5
+    return W.adjoint_mixture(ncell=4, alpha=0.9, rc_r=3.3, kmax=5)
+
+
+def rel(a, b):
+    return float(np.linalg.norm(np.ravel(a) - np.ravel(b)) / max(np.linalg.norm(np.ravel(b)), 1e-300))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec,tol", [(1, 1e-11), (0, 1e-5)])
+@pytest.mark.parametrize("which", ["medium", "mixture4000"])
+def test_gpu_forces_energy_dU(cuda_lib, oracle_lib, prec, tol, which):
+    s = medium_system() if which == "medium" else W.adjoint_mixture()
+    a = gpu_engine(cuda_lib, s, prec)
+    f, e, dU = a.forces()
+    o = oracle_lib.AdjOracle(s)
+    f0, e0, dU0 = o.forces(s.pos)
+    assert rel(f, f0) < tol
+    for k in range(4):
+        assert abs(e[k] - e0[k]) <= tol * max(1.0, abs(e0[k])), (k, e[k], e0[k])
+    for k in ("eps", "sigma", "charge"):
+        assert rel(dU[k], dU0[k]) < tol, k
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec,tol", [(1, 1e-10), (0, 1e-5)])
+def test_gpu_force_vjp(cuda_lib, oracle_lib, prec, tol):
+    s = medium_system()
+    a = gpu_engine(cuda_lib, s, prec)
+    u = np.random.default_rng(3).normal(size=s.pos.shape)
+    w, g = a.force_vjp(u)
+    w0, g0 = oracle_lib.AdjOracle(s).force_vjp(s.pos, u)
+    assert rel(w, w0) < tol
+    for k in ("eps", "sigma", "charge"):
+        assert rel(g[k], g0[k]) < tol, k
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec,tol", [(1, 1e-9), (0, 1e-4)])
+def test_gpu_trajectory_gradient_matches_oracle(cuda_lib, oracle_lib, prec, tol):
+    s = medium_system()
+    M, K = 40, 15
+    J0, g0 = oracle_lib.AdjOracle(s).loss_grad(s.pos, s.vel, M, K)
+    a = gpu_engine(cuda_lib, s, prec)
+    J, g = a.loss_grad(M, K)
+    assert abs(J - J0) <= tol * abs(J0)
+    for k in ("pos", "vel", "eps", "sigma", "charge"):
+        assert rel(g[k], g0[k]) < tol, (k, rel(g[k], g0[k]))
+    assert abs(a.loss(M) - J) <= 1e-12 * abs(J)
+
+
+@pytest.mark.gpu
+def test_gpu_mixture4000_gradient_matches_fd(cuda_lib):
+    """The 4000-atom mixture, 500 steps (dt 0.002), checkpoints every 50: the
+    mixed-precision and FP64 adjoint gradients against central differences
+    (h = 1e-4) of the FP64 GPU loss, along a random position direction, a
+    random velocity direction and every parameter."""
+    s = W.adjoint_mixture()
+    M, K = 500, 50
+    mixed = gpu_engine(cuda_lib, s, 0)
+    J_m, g_m = mixed.loss_grad(M, K)
+    f64 = gpu_engine(cuda_lib, s, 1)
+    J_d, g_d = f64.loss_grad(M, K)
+    assert abs(J_m - J_d) <= 1e-5 * abs(J_d)
+    rng = np.random.default_rng(11)
+
+    def loss_at(pos, vel, eps, sig, q):
+        f64.set_params(q, eps, sig, s.rc_lj, s.alpha, s.rc_r, s.kmax, s.k_e, s.dt)
+        f64.set_state(pos, vel, s.type)
+        return f64.loss(M)
+
+    checks = []
+    for which in ("pos", "vel"):
+        dirn = rng.normal(size=s.pos.shape)
+        dirn /= np.linalg.norm(dirn)
+        vals = []
+        for sg in (1, -1):
+            p = s.pos + sg * H * dirn if which == "pos" else s.pos
+            v = s.vel + sg * H * dirn if which == "vel" else s.vel
+            vals.append(loss_at(p, v, s.epsilon, s.sigma, s.charge))
+        fd = (vals[0] - vals[1]) / (2 * H)
+        checks.append((which, float(np.sum(g_d[which] * dirn)), float(np.sum(g_m[which] * dirn)), fd,
+                       np.linalg.norm(g_d[which])))
+    for name, idx in PARAMS:
+        vals = []
+        for sg in (1, -1):
+            m = perturbed(s, name, idx, sg * H)
+            vals.append(loss_at(s.pos, s.vel, m["eps"], m["sigma"], m["charge"]))
+        fd = (vals[0] - vals[1]) / (2 * H)
+        checks.append((name + str(idx), float(g_d[name][idx]), float(g_m[name][idx]), fd, np.abs(g_d[name]).max()))
+    for name, gd, gm, fd, scale in checks:
+        assert abs(gd - fd) <= 1e-5 * scale + 1e-5 * abs(fd), (name, gd, fd)
+        assert abs(gm - fd) <= 1e-4 * scale + 1e-4 * abs(fd), (name, gm, fd)
+
+
+@pytest.mark.gpu
+def test_torch_autograd_binding(cuda_lib):
+    import torch
+    from torch_adjoint import Engine, Forces, TrajectoryLoss, sym2
+    s = small_system()
+    eng = Engine(s, precision=1, nsteps=8, checkpoint_every=3)
+    pos = torch.tensor(s.pos, requires_grad=True)
+    vel = torch.tensor(s.vel, requires_grad=True)
+    ev = torch.tensor([s.epsilon[0, 0], s.epsilon[0, 1], s.epsilon[1, 1]], requires_grad=True)
+    sv = torch.tensor([s.sigma[0, 0], s.sigma[0, 1], s.sigma[1, 1]], requires_grad=True)
+    q = torch.tensor(s.charge, requires_grad=True)
+    J = TrajectoryLoss.apply(pos, vel, sym2(ev), sym2(sv), q, eng)
+    J.backward()
+    J_ref, g = eng.a.loss_grad(8, 3)
+    assert abs(J.item() - J_ref) <= 1e-12 * abs(J_ref)
+    assert np.allclose(pos.grad.numpy(), g["pos"], rtol=1e-12, atol=0)
+    assert np.allclose(vel.grad.numpy(), g["vel"], rtol=1e-12, atol=0)
+    assert np.allclose(ev.grad.numpy(), [g["eps"][0, 0], g["eps"][0, 1], g["eps"][1, 1]], rtol=1e-12, atol=0)
+    assert np.allclose(q.grad.numpy(), g["charge"], rtol=1e-12, atol=0)
+    # Forces: the full Jacobian by finite differences against the VJP kernel (FP64)
+    args = (torch.tensor(s.pos, requires_grad=True), ev.detach().clone().requires_grad_(),
+            sv.detach().clone().requires_grad_(), q.detach().clone().requires_grad_())
+    assert torch.autograd.gradcheck(lambda p, e, sg, qq: Forces.apply(p, sym2(e), sym2(sg), qq, eng), args,
+                                    eps=1e-6, atol=1e-5, rtol=1e-4)
