@@ -342,7 +342,7 @@ class Batch:
         self._check(self.L.cvr_batch_info(self.h, v, 64))
         n_cls = int(v[2])
         classes = [dict(replicas=int(v[3 + 4 * c]), nmax=int(v[4 + 4 * c]), threads=int(v[5 + 4 * c]),
-                        atoms_per_thread=int(v[6 + 4 * c])) for c in range(n_cls)]
+                        sk_groups=int(v[6 + 4 * c])) for c in range(n_cls)]
         return {"n_rep": int(v[0]), "atoms": int(v[1]), "classes": classes}
 
     @property

@@ -38,9 +38,11 @@ namespace {
 constexpr int NMAX = 2048;  // atoms per replica
 constexpr int KMAXB = 6;    // k_max per axis
 constexpr int KP = KMAXB + 1;
+constexpr int RUNMAX = 2 * KMAXB + 1;  // longest nz run of the k-set
 constexpr int TMAX = 4;
-constexpr int CH = 64;  // atoms per phase-table stage of S(k)
-constexpr int NTH = 8;  // per-replica results: ke, e_lj, e_ewr, e_k, e_self, virial, temperature, steps
+constexpr int CH = 64;   // atoms per phase-table stage of S(k)
+constexpr int GMAX = 4;  // atom groups per k-run in S(k)
+constexpr int NTH = 8;   // per-replica results: ke, e_lj, e_ewr, e_k, e_self, virial, temperature, steps
 
 struct KRunB {
   int nx, ny, nz0, len, k0;
@@ -49,7 +51,7 @@ struct KRunB {
 struct BatchDev {
   const int *order;
   const long long *off;
-  const int *n;
+  const int *n, *nq;  // atoms, charged atoms (stored first) per replica
   const double *L, *rc_lj, *rc_r;
   double *x, *y, *z, *vx, *vy, *vz;
   float *fx, *fy, *fz;  // FP32 forces of the current positions (carried between launches)
@@ -101,135 +103,297 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double *red, double *
   __syncthreads();
 }
 
-// Shared-memory state of one replica.
+// Shared-memory state of one replica (np = atoms rounded up to 32).
 struct Smem {
   float4 *ljc;      // per type pair: sig2, eps24, eps48, K (this replica's LJ cutoff)
   float4 *lje;      // per type pair: e4, C0, C1, k_e q_i q_j
   float4 *xh, *xl;  // hi, lo of the box-centred position; type in xh.w, charge in xl.w
-  float2 *ak;       // (4 pi / V) f_k conj(S_k) for the k-force
-  float *fk;
-  float2 *tab;      // phase tables of a stage of CH atoms
+  double2 *skd;     // FP64 S(k) accumulators
   double *red;
+  float2 *ak;   // (4 pi / V) f_k conj(S_k) for the k-force
+  float2 *skp;  // FP32 S(k) partials of one stage, per atom group
+  float2 *tab;  // phase tables of a stage of CH atoms
+  float *fsx, *fsy, *fsz;  // force accumulators
+  float *fk;
 };
 
-// Forces on this thread's MPT atoms (all pairs, minimum image, then k space).
-// EV: energies and virial into ev[0..4] (this thread's share).
-template <int TPB, int MPT, bool EV>
-__device__ void batch_forces(const BatchDev &p, const Smem &S, int r, int n, double L, float3 (&f)[MPT],
-                             double (&ev)[5]) {
-  const float Lh = (float)L, Ll = (float)(L - (double)Lh), iL = (float)(1.0 / L);
-  const float rc2 = (float)(p.rc_lj[r] * p.rc_lj[r]), rr2 = (float)(p.rc_r[r] * p.rc_r[r]);
-  const float alpha = (float)p.alpha, alpha2 = alpha * alpha, tas = (float)(2.0 * p.alpha * 0.56418958354775628695);
-  float4 ih[MPT], il[MPT];
+__host__ __device__ inline int groups_for(int tpb, int nruns) {
+  const int g = nruns > 0 ? tpb / nruns : 1;
+  return g < 1 ? 1 : (g > GMAX ? GMAX : g);
+}
+
+__host__ __device__ inline size_t smem_bytes(int nk, int np, int G) {
+  return (size_t)2 * TMAX * TMAX * 16 + (size_t)2 * np * 16 + (size_t)nk * 16 + 9 * 32 * 8 + (size_t)nk * 8 +
+         (size_t)G * nk * 8 + (size_t)CH * 3 * KP * 8 + (size_t)3 * np * 4 + (size_t)((nk + 3) & ~3) * 4;
+}
+
+__device__ inline Smem carve(unsigned char *raw, int nk, int np, int G) {
+  Smem S;
+  S.ljc = reinterpret_cast<float4 *>(raw);
+  S.lje = S.ljc + TMAX * TMAX;
+  S.xh = S.lje + TMAX * TMAX;
+  S.xl = S.xh + np;
+  S.skd = reinterpret_cast<double2 *>(S.xl + np);
+  S.red = reinterpret_cast<double *>(S.skd + nk);
+  S.ak = reinterpret_cast<float2 *>(S.red + 9 * 32);
+  S.skp = S.ak + nk;
+  S.tab = S.skp + (size_t)G * nk;
+  S.fsx = reinterpret_cast<float *>(S.tab + CH * 3 * KP);
+  S.fsy = S.fsx + np;
+  S.fsz = S.fsy + np;
+  S.fk = S.fsz + np;
+  return S;
+}
+
+// Per-replica pair constants and cutoffs.
+struct PairK {
+  float Lh, Ll, iL, rc2, rr2, alpha2, alpha, tas, ke;
+  float4 lc, le;  // uniform LJ constants (UNI)
+};
+
+// One ordered pair (i, j): c with F_i += c d, d = r_j - r_i (minimum image).
+// EWR: this pair may carry charge on both ends.  Energies into e[0..2] (lj, ewr, virial) scaled by w.
+template <bool UNI, bool EWR, bool EV>
+__device__ __forceinline__ float pair_c(const Smem &S, const PairK &K, const float4 &ih, const float4 &il,
+                                        const float4 &jh, const float4 &jl, float (&d)[3], double (&e)[3], double w) {
+  const float hh[3] = {jh.x - ih.x, jh.y - ih.y, jh.z - ih.z};
+  const float ll[3] = {jl.x - il.x, jl.y - il.y, jl.z - il.z};
 #pragma unroll
-  for (int m = 0; m < MPT; ++m) {
-    const int i = threadIdx.x + m * TPB;
-    ih[m] = (i < n) ? S.xh[i] : make_float4(0, 0, 0, 0);
-    il[m] = (i < n) ? S.xl[i] : make_float4(0, 0, 0, 0);
-    f[m] = make_float3(0, 0, 0);
+  for (int a = 0; a < 3; ++a) {
+    const float k = rintf(hh[a] * K.iL);
+    d[a] = fmaf(-k, K.Lh, hh[a]) + fmaf(-k, K.Ll, ll[a]);
   }
-  for (int j = 0; j < n; ++j) {
-    const float4 jh = S.xh[j], jl = S.xl[j];
-#pragma unroll
-    for (int m = 0; m < MPT; ++m) {
-      const int i = threadIdx.x + m * TPB;
-      if (i >= n || i == j) continue;
+  const float r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+  float4 lc, le;
+  if (UNI) {
+    lc = K.lc;
+    le = K.le;
+  } else {
+    const int tp = __float_as_int(ih.w) * TMAX + __float_as_int(jh.w);
+    lc = S.ljc[tp];
+    le = S.lje[tp];
+  }
+  float c = 0.f;
+  if (r2 <= K.rc2 && lc.y != 0.f) {
+    const float r2i = __fdividef(1.f, r2), s2 = lc.x * r2i, s6 = s2 * s2 * s2;
+    c = r2i * s6 * (lc.y - lc.z * s6) + lc.w;
+    if (EV) e[0] += w * (double)(le.x * (s6 * s6 - s6) + le.z * r2 + le.y);
+  }
+  if (EWR) {
+    const float qq = UNI ? K.ke * il.w * jl.w : le.w;
+    if (qq != 0.f && r2 <= K.rr2) {
+      const float rinv = rsqrtf(r2), rr = r2 * rinv;
+      const float ex = __expf(-K.alpha2 * r2);
+      const float er = erfc_as(K.alpha * rr, ex);
+      c -= qq * (K.tas * ex + er * rinv) * (rinv * rinv);
+      if (EV) e[1] += w * (double)(qq * er * rinv);
+    }
+  }
+  if (EV) e[2] -= w * (double)(c * r2);
+  return c;
+}
+
+// Off-diagonal tile: atoms of block I (one per lane) with atoms of block J,
+// each unordered pair once (Newton's third law).  Lane l meets atom
+// J*32 + (l + s) % 32 at step s; the reaction force on that atom travels with
+// it (shuffled one lane down per step) and is home after 32 steps.
+template <bool UNI, bool EWR, bool EV>
+__device__ __forceinline__ void tile(const Smem &S, const PairK &K, int I, int J, int n, double (&e)[3]) {
+  const int lane = threadIdx.x & 31;
+  const int i = I * 32 + lane;
+  const bool vi = i < n;
+  const float4 ih = S.xh[i], il = S.xl[i];
+  float fi[3] = {0.f, 0.f, 0.f}, fj[3] = {0.f, 0.f, 0.f};
+#pragma unroll 4
+  for (int s = 0; s < 32; ++s) {
+    const int j = J * 32 + ((lane + s) & 31);
+    if (vi && j < n) {
+      const float4 jh = S.xh[j], jl = S.xl[j];
       float d[3];
-      const float hh[3] = {jh.x - ih[m].x, jh.y - ih[m].y, jh.z - ih[m].z};
-      const float ll[3] = {jl.x - il[m].x, jl.y - il[m].y, jl.z - il[m].z};
+      const float c = pair_c<UNI, EWR, EV>(S, K, ih, il, jh, jl, d, e, 1.0);
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
-        const float k = rintf(hh[a] * iL);
-        d[a] = fmaf(-k, Lh, hh[a]) + fmaf(-k, Ll, ll[a]);
+        fi[a] = fmaf(c, d[a], fi[a]);
+        fj[a] = fmaf(-c, d[a], fj[a]);
       }
-      const float r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
-      const int tp = __float_as_int(ih[m].w) * TMAX + __float_as_int(jh.w);
-      const float4 lc = S.ljc[tp], le = S.lje[tp];
-      float c = 0.f;
-      if (r2 <= rc2 && lc.y != 0.f) {
-        const float r2i = __fdividef(1.f, r2), s2 = lc.x * r2i, s6 = s2 * s2 * s2;
-        c = r2i * s6 * (lc.y - lc.z * s6) + lc.w;
-        if (EV) ev[0] += 0.5 * (double)(le.x * (s6 * s6 - s6) + le.z * r2 + le.y);
-      }
-      if (le.w != 0.f && r2 <= rr2) {
-        const float rinv = rsqrtf(r2), rr = r2 * rinv;
-        const float ex = __expf(-alpha2 * r2);
-        const float er = erfc_as(alpha * rr, ex);
-        c -= le.w * (tas * ex + er * rinv) * (rinv * rinv);
-        if (EV) ev[1] += 0.5 * (double)(le.w * er * rinv);
-      }
-      f[m].x += c * d[0];
-      f[m].y += c * d[1];
-      f[m].z += c * d[2];
-      if (EV) ev[4] -= 0.5 * (double)(c * r2);
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a) fj[a] = __shfl_sync(0xffffffffu, fj[a], (lane + 1) & 31);
+  }
+  S.fsx[i] += fi[0];
+  S.fsy[i] += fi[1];
+  S.fsz[i] += fi[2];
+  const int jj = J * 32 + lane;
+  S.fsx[jj] += fj[0];
+  S.fsy[jj] += fj[1];
+  S.fsz[jj] += fj[2];
+}
+
+// Diagonal tile: ordered pairs inside block I (each pair from both ends).
+template <bool UNI, bool EWR, bool EV>
+__device__ __forceinline__ void tile_diag(const Smem &S, const PairK &K, int I, int n, double (&e)[3]) {
+  const int lane = threadIdx.x & 31;
+  const int i = I * 32 + lane;
+  const bool vi = i < n;
+  const float4 ih = S.xh[i], il = S.xl[i];
+  float fi[3] = {0.f, 0.f, 0.f};
+  for (int s = 1; s < 32; ++s) {
+    const int j = I * 32 + ((lane + s) & 31);
+    if (vi && j < n) {
+      const float4 jh = S.xh[j], jl = S.xl[j];
+      float d[3];
+      const float c = pair_c<UNI, EWR, EV>(S, K, ih, il, jh, jl, d, e, 0.5);
+#pragma unroll
+      for (int a = 0; a < 3; ++a) fi[a] = fmaf(c, d[a], fi[a]);
     }
   }
-  // ---- k space: S(k) in passes of TPB k-vectors over stages of CH atoms
-  const int kmax = p.kmax;
-  const double Vd = L * L * L;
-  for (int k0 = 0; k0 < p.nk; k0 += TPB) {
-    const int k = k0 + threadIdx.x;
-    int4 kn = make_int4(0, 0, 0, 0);
-    if (k < p.nk) kn = p.kint[k];
-    double sr = 0, si = 0;
-    for (int a0 = 0; a0 < n; a0 += CH) {
-      const int na = min(CH, n - a0);
-      __syncthreads();
-      for (int t = threadIdx.x; t < na * 3 * KP; t += TPB) {
-        const int at = t / (3 * KP), rem = t % (3 * KP), dd = rem / KP, m = rem % KP;
-        float2 v = make_float2(0.f, 0.f);
-        if (m <= kmax) {
-          const float4 h = S.xh[a0 + at], lo = S.xl[a0 + at];
-          const float hx = dd == 0 ? h.x : (dd == 1 ? h.y : h.z);
-          const float lx = dd == 0 ? lo.x : (dd == 1 ? lo.y : lo.z);
-          // phase of the box-centred coordinate; e^{ik.(x - L/2)} = e^{ik.x} (-1)^n
-          const double u = (double)m * (((double)hx + (double)lx) / L);
-          float sn, cs;
-          sincospif((float)(2.0 * (u - rint(u))), &sn, &cs);
-          if (m & 1) {
-            sn = -sn;
-            cs = -cs;
-          }
-          v = make_float2(cs, sn);
-        }
-        S.tab[t] = v;
+  S.fsx[i] += fi[0];
+  S.fsy[i] += fi[1];
+  S.fsz[i] += fi[2];
+}
+
+// Forces of the replica's current positions into S.fs* (all pairs under the
+// minimum image, then k space).  EV: energies and virial into ev[0..4]
+// (this thread's share: lj, ewald_r, ewald_k, -, virial).
+template <int TPB, bool UNI, bool EV>
+__device__ void batch_forces(const BatchDev &p, const Smem &S, int r, int n, int nq, double L, int G,
+                             double (&ev)[5]) {
+  constexpr int W = TPB / 32;
+  const int warp = threadIdx.x >> 5;
+  PairK K;
+  K.Lh = (float)L;
+  K.Ll = (float)(L - (double)K.Lh);
+  K.iL = (float)(1.0 / L);
+  K.rc2 = (float)(p.rc_lj[r] * p.rc_lj[r]);
+  K.rr2 = (float)(p.rc_r[r] * p.rc_r[r]);
+  K.alpha = (float)p.alpha;
+  K.alpha2 = K.alpha * K.alpha;
+  K.tas = (float)(2.0 * p.alpha * 0.56418958354775628695);
+  K.ke = (float)p.k_e;
+  K.lc = S.ljc[0];
+  K.le = S.lje[0];
+  const int nb = (n + 31) >> 5;
+  for (int i = threadIdx.x; i < nb * 32; i += TPB) S.fsx[i] = S.fsy[i] = S.fsz[i] = 0.f;
+  __syncthreads();
+  double e[3] = {0, 0, 0};
+  // ---- pairs: round-robin schedule of block pairs (circle method), every
+  // block in at most one tile per round, a barrier between rounds
+  const int nbe = nb + (nb & 1), m = nbe - 1, half = nbe >> 1;
+  for (int round = 0; round < m; ++round) {
+    for (int q = warp; q < half; q += W) {
+      int I, J;
+      if (q == 0) {
+        I = m;
+        J = round;
+      } else {
+        I = (round + q) % m;
+        J = (round - q + m) % m;
       }
-      __syncthreads();
-      if (k < p.nk) {
-        const int mx = abs(kn.x), my = abs(kn.y), mz = abs(kn.z);
-        float pr = 0.f, pim = 0.f;
-        for (int at = 0; at < na; ++at) {
-          const float2 *tb = S.tab + at * 3 * KP;
-          const float2 ph = cmulf(cmulf(conjf_if(tb[mx], kn.x < 0), conjf_if(tb[KP + my], kn.y < 0)),
-                                  conjf_if(tb[2 * KP + mz], kn.z < 0));
-          const float q = S.xl[a0 + at].w;
-          pr += q * ph.x;
-          pim += q * ph.y;
-        }
-        sr += (double)pr;
-        si += (double)pim;
-      }
+      if (I >= nb || J >= nb) continue;
+      const bool ewr = (I * 32 < nq) && (J * 32 < nq);  // warp-uniform: charged atoms come first
+      if (ewr)
+        tile<UNI, true, EV>(S, K, I, J, n, e);
+      else
+        tile<UNI, false, EV>(S, K, I, J, n, e);
     }
-    if (k < p.nk) {
-      const double fkk = (double)S.fk[k];
-      const double cf = 12.56637061435917295384 / Vd * fkk;
-      S.ak[k] = make_float2((float)(cf * sr), (float)(-cf * si));
-      if (EV) ev[2] += 6.28318530717958647692 / Vd * p.k_e * fkk * (sr * sr + si * si);
+    __syncthreads();
+  }
+  for (int I = warp; I < nb; I += W) {
+    if (I * 32 < nq)
+      tile_diag<UNI, true, EV>(S, K, I, n, e);
+    else
+      tile_diag<UNI, false, EV>(S, K, I, n, e);
+  }
+  if (EV) {
+    ev[0] += e[0];
+    ev[1] += e[1];
+    ev[4] += e[2];
+  }
+  // ---- k space: S(k) along the k-set's nz runs, G atom groups per run, per
+  // stage of CH atoms: FP32 sums of at most CH/G atoms, then FP64 per k
+  const int nk = p.nk, kmax = p.kmax;
+  for (int k = threadIdx.x; k < nk; k += TPB) S.skd[k] = make_double2(0.0, 0.0);
+  const int items = p.nruns * G;
+  for (int a0 = 0; a0 < nq; a0 += CH) {  // neutral atoms (stored after the charged ones) add nothing
+    const int na = min(CH, nq - a0);
+    __syncthreads();
+    for (int t = threadIdx.x; t < na * 3 * KP; t += TPB) {
+      const int at = t / (3 * KP), rem = t % (3 * KP), dd = rem / KP, mm = rem % KP;
+      float2 v = make_float2(0.f, 0.f);
+      if (mm <= kmax) {
+        const float4 h = S.xh[a0 + at], lo = S.xl[a0 + at];
+        const float hx = dd == 0 ? h.x : (dd == 1 ? h.y : h.z);
+        const float lx = dd == 0 ? lo.x : (dd == 1 ? lo.y : lo.z);
+        // phase of the box-centred coordinate; e^{ik.(x - L/2)} = e^{ik.x} (-1)^m
+        const double u = (double)mm * (((double)hx + (double)lx) / L);
+        float sn, cs;
+        sincospif((float)(2.0 * (u - rint(u))), &sn, &cs);
+        if (mm & 1) {
+          sn = -sn;
+          cs = -cs;
+        }
+        v = make_float2(cs, sn);
+      }
+      S.tab[t] = v;
+    }
+    __syncthreads();
+    for (int it = threadIdx.x; it < items; it += TPB) {
+      const int ri = it % p.nruns, g = it / p.nruns;
+      const KRunB run = p.runs[ri];
+      float2 acc[RUNMAX];
+#pragma unroll
+      for (int u = 0; u < RUNMAX; ++u) acc[u] = make_float2(0.f, 0.f);
+      const int mx = abs(run.nx), my = abs(run.ny), mz = abs(run.nz0);
+      for (int at = g; at < na; at += G) {
+        const float2 *tb = S.tab + at * 3 * KP;
+        const float q = S.xl[a0 + at].w;
+        float2 ph = cmulf(cmulf(conjf_if(tb[mx], run.nx < 0), conjf_if(tb[KP + my], run.ny < 0)),
+                          conjf_if(tb[2 * KP + mz], run.nz0 < 0));
+        ph.x *= q;
+        ph.y *= q;
+        const float2 ez = tb[2 * KP + 1];
+#pragma unroll
+        for (int u = 0; u < RUNMAX; ++u)
+          if (u < run.len) {
+            acc[u].x += ph.x;
+            acc[u].y += ph.y;
+            ph = cmulf(ph, ez);
+          }
+      }
+#pragma unroll
+      for (int u = 0; u < RUNMAX; ++u)
+        if (u < run.len) S.skp[(size_t)g * nk + run.k0 + u] = acc[u];
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < nk; k += TPB) {
+      double2 a = S.skd[k];
+      for (int g = 0; g < G; ++g) {
+        const float2 v = S.skp[(size_t)g * nk + k];
+        a.x += (double)v.x;
+        a.y += (double)v.y;
+      }
+      S.skd[k] = a;
     }
   }
   __syncthreads();
-  // ---- k-force: each of this thread's atoms with its own phase table in registers
+  const double Vd = L * L * L;
+  for (int k = threadIdx.x; k < nk; k += TPB) {
+    const double2 sk = S.skd[k];
+    const double fkk = (double)S.fk[k];
+    const double cf = 12.56637061435917295384 / Vd * fkk;
+    S.ak[k] = make_float2((float)(cf * sk.x), (float)(-cf * sk.y));
+    if (EV) ev[2] += 6.28318530717958647692 / Vd * p.k_e * fkk * (sk.x * sk.x + sk.y * sk.y);
+  }
+  __syncthreads();
+  // ---- k-force of each charged atom, phases along the nz runs
   const float tpl = (float)(6.28318530717958647692 / L);
-#pragma unroll 1
-  for (int m = 0; m < MPT; ++m) {
-    const int i = threadIdx.x + m * TPB;
-    if (i >= n) continue;
+  for (int i = threadIdx.x; i < nq; i += TPB) {
     float2 tx[KP], ty[KP], tz[KP];
     const float4 h = S.xh[i], lo = S.xl[i];
     const double pc[3] = {(double)h.x + lo.x, (double)h.y + lo.y, (double)h.z + lo.z};
 #pragma unroll
     for (int mm = 0; mm < KP; ++mm) {
-      float2 e[3];
+      float2 e3[3];
 #pragma unroll
       for (int dd = 0; dd < 3; ++dd) {
         const double u = (double)mm * (pc[dd] / L);
@@ -239,25 +403,22 @@ __device__ void batch_forces(const BatchDev &p, const Smem &S, int r, int n, dou
           sn = -sn;
           cs = -cs;
         }
-        e[dd] = make_float2(cs, sn);
+        e3[dd] = make_float2(cs, sn);
       }
-      tx[mm] = e[0];
-      ty[mm] = e[1];
-      tz[mm] = e[2];
+      tx[mm] = e3[0];
+      ty[mm] = e3[1];
+      tz[mm] = e3[2];
     }
     float fx = 0, fy = 0, fz = 0;
     for (int rr = 0; rr < p.nruns; ++rr) {
       const KRunB run = p.runs[rr];
-      float2 px = tx[0], py = ty[0];
+      float2 px = tx[0], py = ty[0], pz = tz[0];
 #pragma unroll
       for (int mm = 0; mm < KP; ++mm) {
         if (mm == abs(run.nx)) px = tx[mm];
         if (mm == abs(run.ny)) py = ty[mm];
-      }
-      float2 pz = tz[0];
-#pragma unroll
-      for (int mm = 0; mm < KP; ++mm)
         if (mm == abs(run.nz0)) pz = tz[mm];
+      }
       // e^{i k.r} along the run: start at nz0, then one step of e^{i 2 pi z / L} per k
       float2 ph = cmulf(cmulf(conjf_if(px, run.nx < 0), conjf_if(py, run.ny < 0)), conjf_if(pz, run.nz0 < 0));
       const float2 ez = tz[1];
@@ -273,13 +434,9 @@ __device__ void batch_forces(const BatchDev &p, const Smem &S, int r, int n, dou
       fy += (float)run.ny * tsum;
     }
     const float qk = (float)p.k_e * lo.w * tpl;
-#pragma unroll
-    for (int mm = 0; mm < MPT; ++mm)  // static indices keep f in registers
-      if (mm == m) {
-        f[mm].x += qk * fx;
-        f[mm].y += qk * fy;
-        f[mm].z += qk * fz;
-      }
+    S.fsx[i] += qk * fx;
+    S.fsy[i] += qk * fy;
+    S.fsz[i] += qk * fz;
   }
 }
 
@@ -303,23 +460,18 @@ __device__ __forceinline__ void to_smem(const BatchDev &p, const Smem &S, int i,
 // (written by the previous launch), so runs split over several launches are
 // bit-identical to one run.  Energies and virial come from a separate
 // evaluation at the final positions (the stepping forces never depend on
-// whether energies are wanted).
-template <int TPB, int MPT>
-__global__ void __launch_bounds__(TPB, 1) k_batch(BatchDev p, int first, int nsteps, int nmax, int compute_first) {
+// whether energies are wanted).  Each thread owns atoms tid, tid + TPB, ...
+// for the integrator and the k-space force; the pair tiles write forces of
+// any atom, ordered by barriers.
+template <int TPB, bool UNI>
+__global__ void __launch_bounds__(TPB, 1) k_batch(BatchDev p, int first, int nsteps, int np, int G,
+                                                   int compute_first) {
   extern __shared__ __align__(16) unsigned char smraw[];
   const int r = p.order[first + blockIdx.x];
-  const int n = p.n[r];
+  const int n = p.n[r], nq = p.nq[r];
   const long long o = p.off[r];
   const double L = p.L[r];
-  Smem S;
-  S.ljc = reinterpret_cast<float4 *>(smraw);
-  S.lje = S.ljc + TMAX * TMAX;
-  S.xh = S.lje + TMAX * TMAX;
-  S.xl = S.xh + nmax;
-  S.ak = reinterpret_cast<float2 *>(S.xl + nmax);
-  S.fk = reinterpret_cast<float *>(S.ak + p.nk);
-  S.tab = reinterpret_cast<float2 *>(S.fk + ((p.nk + 3) & ~3));
-  S.red = reinterpret_cast<double *>(S.tab + CH * 3 * KP);
+  const Smem S = carve(smraw, p.nk, np, G);
   // LJ constants for this replica's cutoff (lj.cpp:439-448) and k_e q_i q_j
   if (threadIdx.x < TMAX * TMAX) {
     const int a = threadIdx.x / TMAX, b = threadIdx.x % TMAX, T = p.n_types;
@@ -339,30 +491,33 @@ __global__ void __launch_bounds__(TPB, 1) k_batch(BatchDev p, int first, int nst
     const double ksq = tpl * tpl * (double)(kn.x * kn.x + kn.y * kn.y + kn.z * kn.z);
     S.fk[k] = (float)(exp(-ksq * fa) / ksq);
   }
-  for (int i = threadIdx.x; i < n; i += TPB) to_smem(p, S, i, o + i, L);
+  for (int i = threadIdx.x; i < np; i += TPB) {
+    if (i < n) {
+      to_smem(p, S, i, o + i, L);
+    } else {
+      S.xh[i] = make_float4(0.f, 0.f, 0.f, __int_as_float(0));
+      S.xl[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+  }
   __syncthreads();
-  float3 f[MPT];
   double ev[5] = {0, 0, 0, 0, 0};
   if (compute_first) {
-    batch_forces<TPB, MPT, false>(p, S, r, n, L, f, ev);
+    batch_forces<TPB, UNI, false>(p, S, r, n, nq, L, G, ev);
   } else {
-#pragma unroll
-    for (int m = 0; m < MPT; ++m) {
-      const int i = threadIdx.x + m * TPB;
-      f[m] = (i < n) ? make_float3(p.fx[o + i], p.fy[o + i], p.fz[o + i]) : make_float3(0.f, 0.f, 0.f);
+    for (int i = threadIdx.x; i < n; i += TPB) {
+      S.fsx[i] = p.fx[o + i];
+      S.fsy[i] = p.fy[o + i];
+      S.fsz[i] = p.fz[o + i];
     }
   }
   const double dt = p.dt, h = 0.5 * dt;
   for (int step = 0; step < nsteps; ++step) {
     __syncthreads();
-#pragma unroll
-    for (int m = 0; m < MPT; ++m) {
-      const int i = threadIdx.x + m * TPB;
-      if (i >= n) continue;
+    for (int i = threadIdx.x; i < n; i += TPB) {
       const long long gi = o + i;
       const double mi = p.mass_inv[p.type[gi]];
       double *X[3] = {p.x, p.y, p.z}, *V[3] = {p.vx, p.vy, p.vz};
-      const float fv[3] = {f[m].x, f[m].y, f[m].z};
+      const float fv[3] = {S.fsx[i], S.fsy[i], S.fsz[i]};
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
         const double v = V[a][gi] + h * (double)fv[a] * mi;
@@ -374,35 +529,29 @@ __global__ void __launch_bounds__(TPB, 1) k_batch(BatchDev p, int first, int nst
       to_smem(p, S, i, gi, L);
     }
     __syncthreads();
-    batch_forces<TPB, MPT, false>(p, S, r, n, L, f, ev);
-#pragma unroll
-    for (int m = 0; m < MPT; ++m) {
-      const int i = threadIdx.x + m * TPB;
-      if (i >= n) continue;
+    batch_forces<TPB, UNI, false>(p, S, r, n, nq, L, G, ev);
+    for (int i = threadIdx.x; i < n; i += TPB) {
       const long long gi = o + i;
       const double mi = p.mass_inv[p.type[gi]];
-      p.vx[gi] += h * (double)f[m].x * mi;
-      p.vy[gi] += h * (double)f[m].y * mi;
-      p.vz[gi] += h * (double)f[m].z * mi;
+      p.vx[gi] += h * (double)S.fsx[i] * mi;
+      p.vy[gi] += h * (double)S.fsy[i] * mi;
+      p.vz[gi] += h * (double)S.fsz[i] * mi;
     }
   }
-  {
-    __syncthreads();
-    float3 fe[MPT];
-    batch_forces<TPB, MPT, true>(p, S, r, n, L, fe, ev);
+  // forces of the final positions, carried to the next launch
+  for (int i = threadIdx.x; i < n; i += TPB) {
+    p.fx[o + i] = S.fsx[i];
+    p.fy[o + i] = S.fsy[i];
+    p.fz[o + i] = S.fsz[i];
   }
   __syncthreads();
-  // forces, kinetic energy (COM removed), energies
-  double kv[9] = {0, 0, 0, 0, 0, ev[0], ev[1], ev[4], 0};
-#pragma unroll
-  for (int m = 0; m < MPT; ++m) {
-    const int i = threadIdx.x + m * TPB;
-    if (i >= n) continue;
+  batch_forces<TPB, UNI, true>(p, S, r, n, nq, L, G, ev);  // energies only; S.fs* is scratch here
+  __syncthreads();
+  // kinetic energy (COM removed), energies
+  double kv[9] = {0, 0, 0, 0, 0, ev[0], ev[1], ev[4], ev[2]};
+  for (int i = threadIdx.x; i < n; i += TPB) {
     const long long gi = o + i;
     const double ms = p.mass[p.type[gi]];
-    p.fx[gi] = f[m].x;
-    p.fy[gi] = f[m].y;
-    p.fz[gi] = f[m].z;
     const double v0 = p.vx[gi], v1 = p.vy[gi], v2 = p.vz[gi];
     kv[0] += ms * (v0 * v0 + v1 * v1 + v2 * v2);
     kv[1] += ms * v0;
@@ -410,7 +559,6 @@ __global__ void __launch_bounds__(TPB, 1) k_batch(BatchDev p, int first, int nst
     kv[3] += ms * v2;
     kv[4] += ms;
   }
-  kv[8] = ev[2];  // k-space energy: each k counted by exactly one thread
   double tot[9];
   block_sum<TPB, 9>(kv, S.red, tot);
   if (threadIdx.x == 0) {
@@ -432,23 +580,18 @@ __global__ void __launch_bounds__(TPB, 1) k_batch(BatchDev p, int first, int nst
   }
 }
 
-size_t smem_bytes(int nk, int nmax) {
-  return (size_t)2 * TMAX * TMAX * sizeof(float4) + (size_t)2 * nmax * sizeof(float4) + (size_t)nk * sizeof(float2) +
-         (size_t)((nk + 3) & ~3) * sizeof(float) + (size_t)CH * 3 * KP * sizeof(float2) + 9 * 32 * sizeof(double);
-}
-
-using KernelFn = void (*)(BatchDev, int, int, int, int);
+using KernelFn = void (*)(BatchDev, int, int, int, int, int);
 
 struct Shape {
-  int tpb, mpt;
-  KernelFn fn;
+  int tpb;
+  KernelFn fn, fn_uni;
 };
 
-// Launch shapes per size class: (threads per CTA, atoms per thread)
+// Launch shapes (threads per CTA); the uniform-LJ form when every type pair has the same eps and sigma
 const Shape kShapes[] = {
-    {128, 1, k_batch<128, 1>}, {128, 2, k_batch<128, 2>}, {128, 4, k_batch<128, 4>},
-    {256, 1, k_batch<256, 1>}, {256, 2, k_batch<256, 2>}, {256, 4, k_batch<256, 4>},
-    {512, 1, k_batch<512, 1>}, {512, 2, k_batch<512, 2>}, {512, 4, k_batch<512, 4>},
+    {128, k_batch<128, false>, k_batch<128, true>},
+    {256, k_batch<256, false>, k_batch<256, true>},
+    {512, k_batch<512, false>, k_batch<512, true>},
 };
 
 }  // namespace
@@ -458,9 +601,12 @@ struct cvr_batch {
   cudaStream_t stream = nullptr;
   int n_rep = 0, n_types = 0;
   long long n_total = 0;
-  std::vector<int> n;
+  std::vector<int> n, nq;
   std::vector<long long> off;
   std::vector<double> L, rc_lj, rc_r;
+  std::vector<int> slot_of;  // caller's atom index -> stored slot (charged atoms first within a replica)
+  std::vector<double> charge_h;
+  bool uniform = false;      // every type pair has the same eps and sigma
   BatchDev dev{};
   std::vector<void *> allocs;
   // size classes: [first, count) in the order array, chosen shape
@@ -497,8 +643,10 @@ int balloc(cvr_batch *b, T **p, size_t count) {
 int launch_class(cvr_batch *b, const cvr_batch::Class &c, int shape, int nsteps, int compute_first,
                  cudaStream_t st) {
   const Shape &s = kShapes[shape];
-  const int nmax = (c.nmax + 3) & ~3;
-  s.fn<<<c.count, s.tpb, smem_bytes(b->dev.nk, nmax), st>>>(b->dev, c.first, nsteps, nmax, compute_first);
+  const int np = (c.nmax + 31) & ~31;
+  const int G = groups_for(s.tpb, b->dev.nruns);
+  (b->uniform ? s.fn_uni : s.fn)<<<c.count, s.tpb, smem_bytes(b->dev.nk, np, G), st>>>(b->dev, c.first, nsteps, np,
+                                                                                         G, compute_first);
   return cudaGetLastError() == cudaSuccess ? CVR_OK : CVR_ERR_CUDA;
 }
 
@@ -519,7 +667,9 @@ int cvr_batch_create(cvr_batch **out, int n_rep, const int64_t *n_atoms, const d
   b->n_rep = n_rep;
   b->n_types = n_types;
   b->n.assign(n_atoms, n_atoms + n_rep);
+  b->nq.assign(n_rep, 0);
   b->L.assign(box_len, box_len + n_rep);
+  b->charge_h.assign(charge, charge + n_types);
   b->off.resize(n_rep);
   long long o = 0;
   for (int r = 0; r < n_rep; ++r) {
@@ -546,7 +696,7 @@ int cvr_batch_create(cvr_batch **out, int n_rep, const int64_t *n_atoms, const d
   long long *doff;
   int *dorder;
   double *dL;
-  if ((rc = balloc(b, &dn, n_rep)) || (rc = balloc(b, &doff, n_rep)) || (rc = balloc(b, &dorder, n_rep)) ||
+  if ((rc = balloc(b, &dn, 2 * n_rep)) || (rc = balloc(b, &doff, n_rep)) || (rc = balloc(b, &dorder, n_rep)) ||
       (rc = balloc(b, &dL, 3 * n_rep)))
     return rc;
   const size_t N = (size_t)o;
@@ -570,6 +720,7 @@ int cvr_batch_create(cvr_batch **out, int n_rep, const int64_t *n_atoms, const d
   d.type = dtype;
   d.out = dout;
   d.n = dn;
+  d.nq = dn + n_rep;
   d.off = doff;
   d.order = dorder;
   d.L = dL;
@@ -588,6 +739,7 @@ int cvr_batch_create(cvr_batch **out, int n_rep, const int64_t *n_atoms, const d
     if (k > first) b->classes.push_back({first, k - first, b->n[order[first]], -1});
   }
   cudaMemcpy(dn, b->n.data(), n_rep * sizeof(int), cudaMemcpyHostToDevice);
+  cudaMemset(dn + n_rep, 0, n_rep * sizeof(int));
   cudaMemcpy(doff, b->off.data(), n_rep * sizeof(long long), cudaMemcpyHostToDevice);
   cudaMemcpy(dorder, order.data(), n_rep * sizeof(int), cudaMemcpyHostToDevice);
   cudaMemcpy(dL, b->L.data(), n_rep * sizeof(double), cudaMemcpyHostToDevice);
@@ -617,9 +769,11 @@ int cvr_batch_set_forces(cvr_batch *b, const double *eps, const double *sigma, c
   if (!(alpha > 0) || !(dt >= 0)) return bfail(b, CVR_ERR_INVALID, "alpha > 0, dt >= 0");
   cudaSetDevice(b->device);
   const int T = b->n_types;
+  b->uniform = true;
   for (int t = 0; t < T * T; ++t) {
     b->dev.eps[t] = (float)eps[t];
     b->dev.sig[t] = (float)sigma[t];
+    if (eps[t] != eps[0] || sigma[t] != sigma[0]) b->uniform = false;
   }
   for (int r = 0; r < b->n_rep; ++r)
     if (!(rc_r[r] <= 0.5 * b->L[r] * (1 + 1e-12)) || !(rc_lj[r] <= 0.5 * b->L[r] * (1 + 1e-12)))
@@ -658,10 +812,12 @@ int cvr_batch_set_forces(cvr_batch *b, const double *eps, const double *sigma, c
   cudaMemcpy(dr, runs.data(), runs.size() * sizeof(KRunB), cudaMemcpyHostToDevice);
   b->dev.kint = dk;
   b->dev.runs = dr;
-  const int sm = (int)smem_bytes(b->dev.nk, NMAX);
-  for (const Shape &s : kShapes)
-    if (cudaFuncSetAttribute(s.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, sm) != cudaSuccess)
+  for (const Shape &s : kShapes) {
+    const int sm = (int)smem_bytes(b->dev.nk, NMAX, groups_for(s.tpb, b->dev.nruns));
+    if (cudaFuncSetAttribute(s.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, sm) != cudaSuccess ||
+        cudaFuncSetAttribute(s.fn_uni, cudaFuncAttributeMaxDynamicSharedMemorySize, sm) != cudaSuccess)
       return bfail(b, CVR_ERR_CUDA, "shared memory attribute");
+  }
   b->tuned = false;
   b->forces_valid = false;
   if (b->graph) {
@@ -675,23 +831,43 @@ int cvr_batch_set_state(cvr_batch *b, const double *pos, const double *vel, cons
   if (!b || !pos || !type) return CVR_ERR_INVALID;
   cudaSetDevice(b->device);
   const size_t N = (size_t)b->n_total;
-  std::vector<double> soa(6 * N, 0.0);
-  for (size_t i = 0; i < N; ++i)
-    for (int a = 0; a < 3; ++a) {
-      soa[a * N + i] = pos[3 * i + a];
-      soa[(3 + a) * N + i] = vel ? vel[3 * i + a] : 0.0;
-    }
   for (size_t i = 0; i < N; ++i)
     if (type[i] < 0 || type[i] >= b->n_types) return bfail(b, CVR_ERR_INVALID, "atom type out of range");
+  // within each replica, charged atoms first (stable): the pair tiles then
+  // know from the block index alone whether Ewald terms can occur
+  b->slot_of.assign(N, 0);
+  for (int r = 0; r < b->n_rep; ++r) {
+    const long long o = b->off[r];
+    int k = 0;
+    for (int pass = 0; pass < 2; ++pass)
+      for (int i = 0; i < b->n[r]; ++i) {
+        const bool charged = b->charge_h[type[o + i]] != 0.0;
+        if (charged == (pass == 0)) b->slot_of[o + i] = (int)(o + k++);
+      }
+    int q = 0;
+    for (int i = 0; i < b->n[r]; ++i) q += b->charge_h[type[o + i]] != 0.0;
+    b->nq[r] = q;
+  }
+  std::vector<double> soa(6 * N, 0.0);
+  std::vector<int32_t> ts(N);
+  for (size_t i = 0; i < N; ++i) {
+    const size_t sl = (size_t)b->slot_of[i];
+    ts[sl] = type[i];
+    for (int a = 0; a < 3; ++a) {
+      soa[a * N + sl] = pos[3 * i + a];
+      soa[(3 + a) * N + sl] = vel ? vel[3 * i + a] : 0.0;
+    }
+  }
   cudaMemcpyAsync(b->dev.x, soa.data(), 6 * N * sizeof(double), cudaMemcpyHostToDevice, b->stream);
-  cudaMemcpyAsync((void *)b->dev.type, type, N * sizeof(int32_t), cudaMemcpyHostToDevice, b->stream);
+  cudaMemcpyAsync((void *)b->dev.type, ts.data(), N * sizeof(int32_t), cudaMemcpyHostToDevice, b->stream);
+  cudaMemcpyAsync((void *)b->dev.nq, b->nq.data(), b->n_rep * sizeof(int), cudaMemcpyHostToDevice, b->stream);
   b->forces_valid = false;
   return cudaStreamSynchronize(b->stream) == cudaSuccess ? CVR_OK : bfail(b, CVR_ERR_CUDA, "upload");
 }
 
-// Autotuner: for each size class, time every shape whose atoms-per-thread
-// covers the class's largest replica on 2 steps of the real state (restored
-// afterwards), keep the fastest.
+// Autotuner: for each size class, time every launch shape (threads per CTA,
+// which also sets the atom groups per k-run of S(k)) that fits the shared
+// memory on 2 steps of the real state (restored afterwards); keep the fastest.
 static int batch_tune(cvr_batch *b) {
   const size_t N = (size_t)b->n_total;
   double *save = nullptr;
@@ -706,7 +882,9 @@ static int batch_tune(cvr_batch *b) {
     int best_s = -1;
     for (int si = 0; si < (int)(sizeof(kShapes) / sizeof(kShapes[0])); ++si) {
       const Shape &s = kShapes[si];
-      if (s.tpb * s.mpt < c.nmax || s.tpb * s.mpt >= 4 * c.nmax + 512) continue;
+      const int np = (c.nmax + 31) & ~31;
+      if (smem_bytes(b->dev.nk, np, groups_for(s.tpb, b->dev.nruns)) > 227 * 1024) continue;
+      if (s.tpb > 2 * np) continue;  // more threads than pair-tile warps and atoms can use
       cudaEventRecord(e0, b->stream);
       if (launch_class(b, c, si, 2, 1, b->stream)) {
         cudaFree(save);
@@ -742,6 +920,7 @@ int cvr_batch_run(cvr_batch *b, int64_t nsteps, double *out) {
   if (!b) return CVR_ERR_INVALID;
   if (nsteps < 0 || nsteps > (1 << 30)) return bfail(b, CVR_ERR_INVALID, "bad step count");
   if (!b->dev.kint) return bfail(b, CVR_ERR_STATE, "cvr_batch_set_forces has not been called");
+  if (b->slot_of.empty()) return bfail(b, CVR_ERR_STATE, "cvr_batch_set_state has not been called");
   cudaSetDevice(b->device);
   if (!b->tuned)
     if (int rc = batch_tune(b)) return rc;
@@ -791,12 +970,14 @@ int cvr_batch_get_state(cvr_batch *b, double *pos, double *vel, double *acc) {
   cudaMemcpyAsync(a.data(), b->dev.fx, 3 * N * sizeof(float), cudaMemcpyDeviceToHost, b->stream);
   cudaMemcpyAsync(t.data(), b->dev.type, N * sizeof(int32_t), cudaMemcpyDeviceToHost, b->stream);
   if (cudaStreamSynchronize(b->stream) != cudaSuccess) return bfail(b, CVR_ERR_CUDA, "download");
-  for (size_t i = 0; i < N; ++i)
+  for (size_t i = 0; i < N; ++i) {
+    const size_t sl = b->slot_of.empty() ? i : (size_t)b->slot_of[i];
     for (int d = 0; d < 3; ++d) {
-      if (pos) pos[3 * i + d] = soa[d * N + i];
-      if (vel) vel[3 * i + d] = soa[(3 + d) * N + i];
-      if (acc) acc[3 * i + d] = (double)a[d * N + i] * b->dev.mass_inv[t[i]];
+      if (pos) pos[3 * i + d] = soa[d * N + sl];
+      if (vel) vel[3 * i + d] = soa[(3 + d) * N + sl];
+      if (acc) acc[3 * i + d] = (double)a[d * N + sl] * b->dev.mass_inv[t[sl]];
     }
+  }
   return CVR_OK;
 }
 
@@ -807,7 +988,7 @@ int cvr_batch_info(const cvr_batch *b, int64_t *out, int len) {
     v.push_back(c.count);
     v.push_back(c.nmax);
     v.push_back(c.shape >= 0 ? kShapes[c.shape].tpb : 0);
-    v.push_back(c.shape >= 0 ? kShapes[c.shape].mpt : 0);
+    v.push_back(c.shape >= 0 ? groups_for(kShapes[c.shape].tpb, b->dev.nruns) : 0);
   }
   for (int k = 0; k < len && k < (int)v.size(); ++k) out[k] = v[k];
   return CVR_OK;

@@ -192,7 +192,7 @@ int cvr_batch_set_state(cvr_batch *b, const double *pos, const double *vel, cons
 int cvr_batch_run(cvr_batch *b, int64_t nsteps, double *out);
 /* pos, vel, acc (each nullable) n*3; acc = FP32 force / mass of the current positions (after a run). */
 int cvr_batch_get_state(cvr_batch *b, double *pos, double *vel, double *acc);
-/* n_rep, atoms, classes, then per class: replicas, largest replica, threads per CTA, atoms per thread. */
+/* n_rep, atoms, classes, then per class: replicas, largest replica, threads per CTA, atom groups per k-run. */
 int cvr_batch_info(const cvr_batch *b, int64_t *out, int len);
 int cvr_batch_last_error(const cvr_batch *b, char *buf, size_t len);
 void *cvr_batch_stream(const cvr_batch *b);

@@ -101,7 +101,7 @@ def test_batch_forces_and_energies(cuda_lib, oracle_lib):
     info = bt.info()
     assert sum(c["replicas"] for c in info["classes"]) == len(SIZES)
     for c in info["classes"]:
-        assert c["threads"] * c["atoms_per_thread"] >= c["nmax"]
+        assert c["threads"] in (128, 256, 512) and 1 <= c["sk_groups"] <= 4
 
 
 @pytest.mark.gpu
