@@ -205,7 +205,7 @@ def replica_line(abi, W, torch, nsteps: int):
             "note": "rc_r = L/2 (minimum image), rc_lj = min(2.5, L/2)"}
 
 
-def adjoint_line(abi, W, torch):
+def adjoint_line(abi, W, torch, nsteps: int = 500):
     """Loss + gradient of the 4000-atom two-species mixture over 500 steps
     (dt 0.002), checkpoints every 50, mixed and FP64; wall time of the
     synchronous C-ABI call (forward, re-run segments, reverse sweep)."""
@@ -213,12 +213,12 @@ def adjoint_line(abi, W, torch):
     out = {}
     for nm, prec in (("mixed", abi.PREC_MIXED), ("fp64", abi.PREC_FP64)):
         a = abi.Adjoint.from_system(s, prec)
-        a.loss_grad(20, 10)
+        a.loss_grad(min(20, nsteps), 10)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        J, g = a.loss_grad(500, 50)
+        J, g = a.loss_grad(nsteps, 50)
         dt = time.perf_counter() - t0
-        out[nm] = {"seconds": dt, "gradient_atom_steps_per_s": 4000 * 500 / dt, "loss": J}
+        out[nm] = {"seconds": dt, "steps": nsteps, "gradient_atom_steps_per_s": 4000 * nsteps / dt, "loss": J}
         a.close()
     out["fp64_over_mixed_time"] = out["fp64"]["seconds"] / out["mixed"]["seconds"]
     return out
@@ -432,9 +432,22 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--replica-steps", type=int, default=1000)
+    ap.add_argument("--adjoint-steps", type=int, default=500)
+    ap.add_argument("--only", default="all", choices=["all", "replicas", "adjoint"],
+                    help="run one secondary workload alone and print its JSON (profiling runs)")
     args = ap.parse_args()
     if args.impl == "reference":
         reference_arm(args)
+    elif args.only != "all":
+        import torch
+        torch.cuda.set_device(0)
+        from caviar_b200 import build as B
+        B.build()
+        from caviar_b200 import _abi as abi
+        from caviar_b200 import workloads as W
+        res = replica_line(abi, W, torch, args.replica_steps) if args.only == "replicas" else adjoint_line(abi, W, torch,
+                                                                                                  args.adjoint_steps)
+        print(json.dumps({"only": args.only, **res}), flush=True)
     else:
         gpu_arm(args)
 
