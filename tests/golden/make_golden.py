@@ -14,6 +14,14 @@ GPU tests never need the reference at run time).
    systems: accelerations, canonical pair set, virial, kinetic energy, S(k),
    k-space and self energies, and a short trajectory.
 
+3. nve_lj500.json -- the reference's NVE energy record over 10^4 steps of a
+   500-atom LJ fluid (FCC 5^3 cells, rho* 0.8442, T* 0.72, rc 2.5, skin 0.3,
+   dt 0.005): ten harness runs of 1000 steps, each continuing from the
+   previous run's final positions and velocities; total energy = the
+   reference's kinetic energy + the LJ energy of its linear force-shifted
+   potential (which the reference lacks; the restatement's formula) at the
+   reference's positions.
+
 Usage:  python tests/golden/make_golden.py [/path/to/reference]
 """
 import json
@@ -100,6 +108,29 @@ def save_ref(name, s, nsteps=20):
     np.savez_compressed(os.path.join(HERE, f"ref_{name}.npz"), **d)
 
 
+def nve_lj500(nblocks: int = 10, block: int = 1000) -> dict:
+    s = W.fcc_lattice(5, 0.8442, 0.72, seed=7, jitter=0.05)
+    cur = s.copy()
+    e = []
+    o = O.Oracle(cur, policy=O.POLICY_REFERENCE)
+    for b in range(nblocks + 1):
+        o.set_atoms(cur.pos, cur.vel, cur.type)
+        o.build_list()
+        sc = o.energy()
+        e.append(sc["ke"] + sc["e_lj"])
+        if b == nblocks:
+            break
+        r = O.run_reference(cur, "run", block)
+        order = np.argsort(r["id"].astype(np.int64))
+        cur = cur.copy()
+        cur.pos = r["pos"].reshape(-1, 3)[order]
+        cur.vel = r["vel"].reshape(-1, 3)[order]
+    e = np.array(e)
+    return {"system": "fcc_lattice(5, 0.8442, 0.72, seed=7, jitter=0.05)", "steps_per_record": block,
+            "total_energy": e.tolist(), "n": s.n,
+            "max_abs_dev_per_atom": float(np.abs(e - e[0]).max() / s.n)}
+
+
 def main():
     ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     g = ewald_n100(ref_root)
@@ -108,6 +139,8 @@ def main():
     O.build(ref_root)
     for name, s in small_systems().items():
         save_ref(name, s)
+    with open(os.path.join(HERE, "nve_lj500.json"), "w") as f:
+        json.dump(nve_lj500(), f, indent=0)
     print("golden fixtures written to", HERE)
 
 
