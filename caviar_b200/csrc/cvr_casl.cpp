@@ -25,17 +25,37 @@
 //   force_field electrostatic_ewald_k <name>  alpha, k_max, kx_max, ky_max, kz_max,
 //                              k_electrostatic, set_atom_data, set_domain (electrostatic_ewald_k.cpp:48-143)
 //   md_simulator basic <name>  set_atom_data, add_force_field|force_field,
-//                              add_neighborlist|neighborlist, integrator_type velocity_verlet,
-//                              dt, initial_step, final_step, final_step_add, run
-//                              (md_simulator.cpp:58-233)
+//                              add_neighborlist|neighborlist, add_writer|writer,
+//                              integrator_type velocity_verlet, dt, initial_step,
+//                              final_step, final_step_add, run (md_simulator.cpp:58-233)
+//   writer atom_data <name>    set_atom_data|atom_data, set_domain|domain, energy_step,
+//                              temperature_step, pressure_step, volume_step, xyz_step,
+//                              file_name_energy|_temperature|_pressure|_volume|_xyz,
+//                              xyz_output_id, xyz_output_velocity, xyz_output_acceleration,
+//                              open_files, close_files, *_mpi_rank0, *_mpi_per_process
+//                              (writer/atom_data.cpp:84-331, dump_energy.cpp, dump_xyz_serial.cpp)
 // plus the variables `real name value` / `int name value`, comments (#) and
-// `exit`.  Keywords of these objects that sit off the hot path (writers,
-// constraints, Langevin, slab/dipole Ewald, jump_tol) are rejected with a
-// message instead of being ignored.
+// `exit`.  Keywords of these objects that sit off the hot path (constraints,
+// Langevin, slab/dipole Ewald, jump_tol, msd/povray/ghost writers) are
+// rejected with a message instead of being ignored.
+//
+// Writers follow the reference: a line "step time value" (default stream
+// format, 6 significant digits) at setup as (0, 0) and after every step i
+// with i % <x>_step == 0 as (i, time at the start of the step); energy =
+// kinetic energy, temperature and pressure only when atom_data has
+// temperature_process / pressure_process (0 otherwise; the pressure is not
+// finalised at setup, so its setup line is 0), xyz frames "N / Atom /
+// type [id] x y z [v] [a]" with positions wrapped into the box.  File names
+// get ".txt" / ".xyz" and are relative to the script's directory.
 //
 // Extensions for the B200 path (md_simulator): precision mixed|fp64,
 // rebuild_policy displacement|reference, thermo_step N, thermo_file "<f>",
-// state_file "<f>" (FP64 binary dump of the final state, id order).
+// state_file "<f>" (FP64 binary dump of the final state, id order);
+// (atom_data) add_state_file file_name "<f>" [replace_data] (reads that dump
+// back: positions and velocities bit for bit); (writer) potential_energy_step
+// N and file_name_potential_energy "<f>" (LJ + Ewald potential energy, which
+// the reference writer lacks), precision N (significant digits of every
+// writer number; 17 makes an xyz frame an exact FP64 restart file).
 //
 // Errors come back as CVR_ERR_INVALID with "file:line: message"; nothing here
 // exits the process (the reference prints and exits, interpreter/error.cpp:27-31).
@@ -129,6 +149,7 @@ struct Domain : Object {
 struct Atom_data : Object {
   Domain *domain = nullptr;
   double ghost_cutoff = -1.0, k_b = -1.0;
+  bool temperature_process = false, pressure_process = false;
   std::vector<double> mass, charge;
   std::vector<int32_t> type, mol;
   std::vector<double> pos, vel;
@@ -180,8 +201,28 @@ struct Ewald_k : Force_field {
   int kmax[3] = {1, 1, 1};
 };
 
+struct Writer : Object {
+  Atom_data *atom_data = nullptr;
+  Domain *domain = nullptr;
+  // writer/atom_data.h:114-165 defaults
+  int64_t step[6] = {100, 100, 100, 100, 100, 100};  // energy, temperature, pressure, volume, potential energy, xyz
+  bool on[6] = {false, false, false, false, false, false};
+  std::string file[6] = {"o_energy", "o_temperature", "o_pressure", "o_volume", "o_potential_energy", "o_xyz"};
+  bool xyz_id = false, xyz_vel = false, xyz_acc = false;
+  int digits = 6;
+  FILE *fp[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  ~Writer() override {
+    for (FILE *f : fp)
+      if (f) std::fclose(f);
+  }
+};
+enum { W_ENERGY = 0, W_TEMPERATURE, W_PRESSURE, W_VOLUME, W_PE, W_XYZ };
+
 struct Md_simulator : Object {
   Atom_data *atom_data = nullptr;
+  std::vector<Writer *> writer;
+  bool initialized = false;  // the reference's setup (and its (0, 0) writer call) happens once
+  double time = 0.0;
   std::vector<Force_field *> force_field;
   std::vector<Neighborlist *> neighborlist;
   double dt = -1.0;
@@ -239,6 +280,7 @@ struct Script {
     else if (cls == "force_field" && type == "electrostatic_ewald_r") o.reset(new Ewald_r);
     else if (cls == "force_field" && type == "electrostatic_ewald_k") o.reset(new Ewald_k);
     else if (cls == "md_simulator" && type == "basic") o.reset(new Md_simulator);
+    else if (cls == "writer" && type == "atom_data") o.reset(new Writer);
     else err("'" + cls + " " + type + "' is not on the B200 hot path");
     o->name = nm;
     objects[nm] = std::move(o);
@@ -323,6 +365,68 @@ struct Script {
     }
   }
 
+  // FP64 binary state written by md_simulator state_file: n, pos[3n], vel[3n], acc[3n]
+  void add_state_file(Atom_data &a) {
+    std::string file;
+    bool replace = false;
+    while (!cur->done()) {
+      const std::string t = word();
+      if (t == "file_name") file = word();
+      else if (t == "replace_data") replace = true;
+      else err("add_state_file: unknown keyword '" + t + "'");
+    }
+    if (file.empty()) err("add_state_file needs file_name");
+    const std::string full = (file[0] == '/') ? file : dir + "/" + file;
+    FILE *f = std::fopen(full.c_str(), "rb");
+    if (!f) err("file does not exist : " + full);
+    int64_t n = 0;
+    bool ok = std::fread(&n, 8, 1, f) == 1 && n > 0;
+    std::vector<double> p((size_t)std::max<int64_t>(n, 0) * 3), v(p.size());
+    ok = ok && std::fread(p.data(), 8, p.size(), f) == p.size() && std::fread(v.data(), 8, v.size(), f) == v.size();
+    std::fclose(f);
+    if (!ok) err("bad state file " + full);
+    if (!replace) err("add_state_file: the file carries no types; load atoms first and use replace_data");
+    if (n != a.n()) err("state file is not compatible: different number of existing atoms");
+    a.pos = p;
+    a.vel = v;
+  }
+
+  void read_writer(Writer &w) {
+    static const char *stepk[6] = {"energy_step", "temperature_step", "pressure_step", "volume_step",
+                                   "potential_energy_step", "xyz_step"};
+    static const char *filek[6] = {"file_name_energy", "file_name_temperature", "file_name_pressure",
+                                   "file_name_volume", "file_name_potential_energy", "file_name_xyz"};
+    while (!cur->done()) {
+      const std::string t = word();
+      bool done = false;
+      for (int k = 0; k < 6 && !done; ++k) {
+        if (t == stepk[k]) {
+          w.step[k] = integer();
+          w.on[k] = w.step[k] > 0;
+          done = true;
+        } else if (t == filek[k]) {
+          w.file[k] = word();
+          done = true;
+        }
+      }
+      if (done) continue;
+      if (t == "set_atom_data" || t == "atom_data") w.atom_data = find<Atom_data>(word());
+      else if (t == "set_domain" || t == "domain") w.domain = find<Domain>(word());
+      else if (t == "xyz_output_id") w.xyz_id = integer() != 0;
+      else if (t == "xyz_output_velocity") w.xyz_vel = integer() != 0;
+      else if (t == "xyz_output_acceleration") w.xyz_acc = integer() != 0;
+      else if (t == "precision") {
+        w.digits = integer();
+        if (w.digits < 1 || w.digits > 17) err("writer precision: 1..17 significant digits");
+      } else if (t == "open_files" || t == "close_files") {
+        // no effect in the reference either (writer/atom_data.cpp:485-486)
+      } else if (t.size() > 10 && (t.compare(t.size() - 10, 10, "_mpi_rank0") == 0 ||
+                                   (t.size() > 16 && t.compare(t.size() - 16, 16, "_mpi_per_process") == 0))) {
+        integer();  // MPI output switches: one process here
+      } else err("writer atom_data: '" + t + "' is not supported on the B200 path");
+    }
+  }
+
   void read_atom_data(Atom_data &a) {
     while (!cur->done()) {
       const std::string t = word();
@@ -346,8 +450,13 @@ struct Script {
         if (i < 0 || i >= a.n()) err(t + ": atom index out of range");
         auto &dst = (t == "set_owned_position") ? a.pos : a.vel;
         for (int d = 0; d < 3; ++d) dst[3 * (size_t)i + d] = real();
-      } else if (t == "temperature_process" || t == "pressure_process") {
-        // thermo is always computed on the GPU path
+      } else if (t == "temperature_process") {
+        // atom_data.cpp:147-151; the writer's temperature (and the pressure's kinetic part) is 0 without it
+        a.temperature_process = integer() != 0;
+      } else if (t == "pressure_process") {
+        a.pressure_process = integer() != 0;  // atom_data.cpp:137-146
+      } else if (t == "add_state_file") {
+        add_state_file(a);
       } else err("atom_data: '" + t + "' is not on the B200 hot path");
     }
   }
@@ -459,6 +568,7 @@ struct Script {
       if (t == "set_atom_data" || t == "atom_data") m.atom_data = find<Atom_data>(word());
       else if (t == "add_force_field" || t == "force_field") m.force_field.push_back(find<Force_field>(word()));
       else if (t == "add_neighborlist" || t == "neighborlist") m.neighborlist.push_back(find<Neighborlist>(word()));
+      else if (t == "add_writer" || t == "writer") m.writer.push_back(find<Writer>(word()));
       else if (t == "integrator_type") {
         const std::string v = word();
         if (v != "velocity_verlet") err("integrator_type '" + v + "' is not on the B200 hot path");
@@ -524,6 +634,104 @@ struct Script {
           err("lj: epsilon, sigma and cutoff_list must be symmetric on the B200 path");
   }
 
+  FILE *wfile(Writer &w, int k) {
+    if (!w.fp[k]) {
+      std::string f = w.file[k] + (k == W_XYZ ? ".xyz" : ".txt");
+      if (f[0] != '/') f = dir + "/" + f;
+      w.fp[k] = std::fopen(f.c_str(), "w");
+      if (!w.fp[k]) err("cannot write " + f);
+    }
+    return w.fp[k];
+  }
+
+  // Writer::write(i, t) for the scalar outputs (dump_energy.cpp): th is the
+  // thermo record of the state after step i (or of the initial state).
+  void write_scalars(Md_simulator &m, const Atom_data &a, const Domain &d, int64_t i, double t, const double *th,
+                     bool setup) {
+    const double V = (d.hi[0] - d.lo[0]) * (d.hi[1] - d.lo[1]) * (d.hi[2] - d.lo[2]);
+    const double T = a.temperature_process ? th[CVR_TH_TEMP] : 0.0;
+    const double kb = a.k_b > 0 ? a.k_b : 1.0;
+    // finalize_pressure_mpi_domain (kinetic_energy.cpp:242-292); not called at setup
+    const double P = (a.pressure_process && !setup) ? (double)a.n() * kb * T / V + th[CVR_TH_VIRIAL] / (3.0 * V) : 0.0;
+    const double val[5] = {th[CVR_TH_KE], T, P, V,
+                           th[CVR_TH_E_LJ] + th[CVR_TH_E_EWR] + th[CVR_TH_E_K] + th[CVR_TH_E_SELF]};
+    for (Writer *w : m.writer)
+      for (int k = 0; k < 5; ++k)
+        if (w->on[k] && i % w->step[k] == 0)
+          std::fprintf(wfile(*w, k), "%lld %.*g %.*g\n", (long long)i, w->digits, t, w->digits, val[k]);
+  }
+
+  // dump_xyz_serial (dump_xyz_serial.cpp:34-67): positions wrapped into the box
+  void write_xyz(Md_simulator &m, const Domain &d, int64_t i, const std::vector<int32_t> &type,
+                 std::vector<double> pos, const std::vector<double> &vel, const std::vector<double> &acc) {
+    const size_t n = type.size();
+    for (size_t q = 0; q < n; ++q)
+      for (int a = 0; a < 3; ++a)
+        if (d.bc[a]) {
+          const double L = d.hi[a] - d.lo[a];
+          double &x = pos[3 * q + a];
+          x -= L * std::floor((x - d.lo[a]) / L);
+        }
+    for (Writer *w : m.writer) {
+      if (!w->on[W_XYZ] || i % w->step[W_XYZ] != 0) continue;
+      FILE *f = wfile(*w, W_XYZ);
+      const int g = w->digits;
+      std::fprintf(f, "%zu\nAtom\n", n);
+      for (size_t q = 0; q < n; ++q) {
+        std::fprintf(f, "%d", (int)type[q]);
+        if (w->xyz_id) std::fprintf(f, " %zu", q);
+        std::fprintf(f, " %.*g %.*g %.*g", g, pos[3 * q], g, pos[3 * q + 1], g, pos[3 * q + 2]);
+        if (w->xyz_vel) std::fprintf(f, " %.*g %.*g %.*g", g, vel[3 * q], g, vel[3 * q + 1], g, vel[3 * q + 2]);
+        if (w->xyz_acc) std::fprintf(f, " %.*g %.*g %.*g", g, acc[3 * q], g, acc[3 * q + 1], g, acc[3 * q + 2]);
+        std::fprintf(f, "\n");
+      }
+      std::fflush(f);
+    }
+  }
+
+  // The reference's writer calls (md_simulator.cpp:548, :664): (0, 0) after
+  // setup, then (i, time before the step) after every step i.  Runs in chunks
+  // that end where an xyz frame is due; one thermo record per step.
+  template <typename Check>
+  void run_with_writers(Md_simulator &m, const Atom_data &a, const Domain &d, cvr_ctx *ctx, Check &check) {
+    const size_t n = (size_t)a.n();
+    std::vector<double> pos(3 * n), vel(3 * n), acc(3 * n), th(CVR_N_THERMO);
+    int64_t xs = 0;  // smallest xyz step
+    for (Writer *w : m.writer)
+      if (w->on[W_XYZ]) xs = xs ? std::min(xs, w->step[W_XYZ]) : w->step[W_XYZ];
+    if (!m.initialized) {
+      check(cvr_compute_forces(ctx, acc.data(), th.data()));
+      write_scalars(m, a, d, 0, 0.0, th.data(), true);
+      if (xs) {
+        check(cvr_get_state(ctx, pos.data(), vel.data(), nullptr));
+        write_xyz(m, d, 0, a.type, pos, vel, acc);
+      }
+      m.time = m.dt * (double)m.initial_step;
+      m.initialized = true;
+    }
+    std::vector<double> rec;
+    int64_t i = m.initial_step;
+    while (i < m.final_step) {
+      int64_t e = std::min(m.final_step, i + 4096);
+      if (xs) e = std::min(e, ((i + xs - 1) / xs) * xs + 1);
+      const int64_t len = e - i;
+      rec.assign((size_t)len * CVR_N_THERMO, 0.0);
+      check(cvr_run(ctx, len, 1, rec.data()));
+      for (int64_t r = 0; r < len; ++r) {
+        write_scalars(m, a, d, i + r, m.time, &rec[(size_t)r * CVR_N_THERMO], false);
+        m.time += m.dt;
+      }
+      if (xs && (e - 1) % xs == 0) {
+        check(cvr_get_state(ctx, pos.data(), vel.data(), acc.data()));
+        write_xyz(m, d, e - 1, a.type, pos, vel, acc);
+      }
+      i = e;
+    }
+    for (Writer *w : m.writer)
+      for (FILE *f : w->fp)
+        if (f) std::fflush(f);
+  }
+
   void run(Md_simulator &m) {
     Atom_data *a = m.atom_data;
     if (!a) err("md_simulator: set_atom_data first");
@@ -580,7 +788,18 @@ struct Script {
     const int64_t nsteps = m.final_step - m.initial_step;
     const int64_t every = m.thermo_step > 0 ? m.thermo_step : 0;
     std::vector<double> thermo((size_t)std::max<int64_t>(1, every > 0 ? nsteps / every : 1) * CVR_N_THERMO);
-    check(cvr_run(ctx, nsteps, every, every > 0 ? thermo.data() : nullptr));
+    bool writers = false;
+    for (Writer *w : m.writer)
+      for (int k = 0; k < 6; ++k) writers = writers || w->on[k];
+    if (!writers) {
+      check(cvr_run(ctx, nsteps, every, every > 0 ? thermo.data() : nullptr));
+      if (!m.initialized) m.time = m.dt * (double)m.initial_step;
+      m.initialized = true;
+      m.time += m.dt * (double)nsteps;
+    } else {
+      if (every > 0) err("thermo_step with writers: use the writers' outputs");
+      run_with_writers(m, *a, *d, ctx, check);
+    }
     check(cvr_get_state(ctx, a->pos.data(), a->vel.data(), nullptr));
     if (!m.thermo_file.empty() && every > 0) {
       const std::string p = (m.thermo_file[0] == '/') ? m.thermo_file : dir + "/" + m.thermo_file;
@@ -642,6 +861,7 @@ struct Script {
       else if (auto *er = dynamic_cast<Ewald_r *>(o)) read_ewald_r(*er);
       else if (auto *ek = dynamic_cast<Ewald_k *>(o)) read_ewald_k(*ek);
       else if (auto *m = dynamic_cast<Md_simulator *>(o)) read_md(*m);
+      else if (auto *w = dynamic_cast<Writer *>(o)) read_writer(*w);
     }
   }
 };

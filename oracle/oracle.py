@@ -280,7 +280,7 @@ class AdjOracle:
 # --------------------------------------------------------------- reference
 
 
-def casl_script(system, nsteps: int = 1, rebuild_test: bool = False) -> str:
+def casl_script(system, nsteps: int = 1, rebuild_test: bool = False, extra: str = "") -> str:
     """The CASL objects of the hot path, with the reference's own keywords
     (domain.cpp:206-266, atom_data.cpp:78-306, neighborlist.cpp:193-251,
     lj.cpp:42-147, electrostatic_ewald_r.cpp:38-88, electrostatic_ewald_k.cpp:48-143,
@@ -332,7 +332,7 @@ def casl_script(system, nsteps: int = 1, rebuild_test: bool = False) -> str:
         lines.append(f"sim add_force_field {f}")
     lines += ["sim add_neighborlist neigh", "sim initial_step 0", f"sim final_step {max(1, nsteps)}",
               f"sim dt {r(float(s.dt))}"]
-    return "\n".join(lines) + "\n"
+    return "\n".join(lines) + "\n" + extra
 
 
 def write_state(path: str, system) -> None:
@@ -375,10 +375,14 @@ def harness_available() -> bool:
 
 
 def run_reference(system, mode: str = "forces", nsteps: int = 0, rebuild_test: bool = False,
-                  timeout: Optional[float] = None, budget_s: float = 0.0) -> Dict[str, np.ndarray]:
+                  timeout: Optional[float] = None, budget_s: float = 0.0, extra: str = "",
+                  collect=()) -> Dict[str, np.ndarray]:
     """Run the unmodified reference on `system` ("forces" or "run") and return
     its FP64 output blocks plus the harness's own wall time.  budget_s > 0
-    stops a run after the step that crosses the budget (at least 2 steps)."""
+    stops a run after the step that crosses the budget (at least 2 steps).
+    `extra` is appended to the script (e.g. writer objects); the text of the
+    files named in `collect` (written by the reference in its working
+    directory) comes back under "files"."""
     if not harness_available():
         raise FileNotFoundError(f"reference harness not built: {HARNESS_PATH}")
     with tempfile.TemporaryDirectory() as d:
@@ -386,7 +390,7 @@ def run_reference(system, mode: str = "forces", nsteps: int = 0, rebuild_test: b
         state = os.path.join(d, "state.bin")
         out = os.path.join(d, "out.bin")
         with open(script, "w") as f:
-            f.write(casl_script(system, nsteps, rebuild_test))
+            f.write(casl_script(system, nsteps, rebuild_test, extra))
         write_state(state, system)
         args = [HARNESS_PATH, script, state, mode, out] + ([str(nsteps), repr(float(budget_s))] if mode == "run" else [])
         t0 = time.perf_counter()
@@ -396,4 +400,11 @@ def run_reference(system, mode: str = "forces", nsteps: int = 0, rebuild_test: b
             raise RuntimeError(f"reference harness failed ({p.returncode}): {p.stdout[-2000:]}\n{p.stderr[-2000:]}")
         res = read_blocks(out)
         res["process_wall"] = wall
+        files = {}
+        for name in collect:
+            fp = os.path.join(d, name)
+            if os.path.exists(fp):
+                with open(fp) as fh:
+                    files[name] = fh.read()
+        res["files"] = files
         return res

@@ -22,6 +22,12 @@ GPU tests never need the reference at run time).
    potential (which the reference lacks; the restatement's formula) at the
    reference's positions.
 
+4. writer_lj500/ -- the files the reference's `writer atom_data` writes for
+   a 40-step run of that fluid (energy and temperature every 5 steps,
+   pressure every 10, volume and xyz frames with ids, velocities and
+   accelerations every 20; temperature_process and pressure_process on), with
+   the script lines that declare the writer (WRITER_SCRIPT).
+
 Usage:  python tests/golden/make_golden.py [/path/to/reference]
 """
 import json
@@ -131,6 +137,36 @@ def nve_lj500(nblocks: int = 10, block: int = 1000) -> dict:
             "max_abs_dev_per_atom": float(np.abs(e - e[0]).max() / s.n)}
 
 
+WRITER_SCRIPT = """writer atom_data w
+w set_atom_data adata
+w set_domain dom
+w energy_step 5
+w temperature_step 5
+w pressure_step 10
+w volume_step 20
+w xyz_step 20
+w xyz_output_id 1
+w xyz_output_velocity 1
+w xyz_output_acceleration 1
+adata temperature_process 1
+adata pressure_process 1
+sim add_writer w
+"""
+WRITER_FILES = ("o_energy.txt", "o_temperature.txt", "o_pressure.txt", "o_volume.txt", "o_xyz.xyz")
+
+
+def writer_lj500(nsteps: int = 40) -> None:
+    s = W.fcc_lattice(5, 0.8442, 0.72, seed=7, jitter=0.05)
+    r = O.run_reference(s, "run", nsteps, extra=WRITER_SCRIPT, collect=WRITER_FILES)
+    out = os.path.join(HERE, "writer_lj500")
+    os.makedirs(out, exist_ok=True)
+    for name in WRITER_FILES:
+        with open(os.path.join(out, name), "w") as f:
+            f.write(r["files"][name])
+    with open(os.path.join(out, "script_extra.casl"), "w") as f:
+        f.write(WRITER_SCRIPT)
+
+
 def main():
     ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     g = ewald_n100(ref_root)
@@ -141,6 +177,7 @@ def main():
         save_ref(name, s)
     with open(os.path.join(HERE, "nve_lj500.json"), "w") as f:
         json.dump(nve_lj500(), f, indent=0)
+    writer_lj500()
     print("golden fixtures written to", HERE)
 
 

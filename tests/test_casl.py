@@ -11,7 +11,8 @@ import os
 import numpy as np
 import pytest
 
-from helpers import load_ref_fixture
+from caviar_b200 import workloads as W
+from helpers import GOLDEN, load_ref_fixture
 
 
 def write_xyz(path, s):
@@ -37,7 +38,7 @@ def script_for(s, tmp, nsteps, extra=()):
 
 def test_rejects_off_path_objects(cuda_lib, tmp_path):
     p = tmp_path / "bad.casl"
-    p.write_text("domain box dom\nwriter atom_data w1\n")
+    p.write_text("domain box dom\nconstraint berendsen c1\n")
     with pytest.raises(cuda_lib.CvrError) as e:
         cuda_lib.run_casl(str(p))
     assert "not on the B200 hot path" in str(e.value) and "bad.casl:2" in str(e.value)
@@ -82,3 +83,77 @@ def test_reference_script_reproduces_reference_trajectory(cuda_lib, tmp_path, na
     th = np.loadtxt(tmp_path / "thermo.txt")
     assert th.shape == (nsteps // 5, 10)
     assert abs(th[-1, 1] - float(d["run_ke"][-1])) < 1e-8 * float(d["run_ke"][-1])
+
+
+def test_rejects_unsupported_writer_keyword(cuda_lib, tmp_path):
+    p = tmp_path / "bad.casl"
+    p.write_text("writer atom_data w\nw msd_step 10\n")
+    with pytest.raises(cuda_lib.CvrError) as e:
+        cuda_lib.run_casl(str(p))
+    assert "msd_step" in str(e.value)
+
+
+def lj500_script(tmp, nsteps, extra, tail):
+    from oracle import oracle as O
+    s = W.fcc_lattice(5, 0.8442, 0.72, seed=7, jitter=0.05)
+    body = O.casl_script(s, nsteps, extra=extra)
+    body = body.replace("adata set_domain dom\n",
+                        'adata set_domain dom\nadata add_xyz_data_file file_name "state.xyz" read_velocity\n')
+    write_xyz(os.path.join(tmp, "state.xyz"), s)
+    return body + tail
+
+
+def parse_rows(text):
+    return [line.split() for line in text.strip().splitlines()]
+
+
+@pytest.mark.gpu
+def test_writer_outputs_match_reference(cuda_lib, tmp_path):
+    """writer atom_data: the energy, temperature, pressure, volume and xyz
+    files of a 40-step run match the unmodified reference's own files
+    (tests/golden/writer_lj500, 6 significant digits: compared to 1.1e-5)."""
+    g = os.path.join(GOLDEN, "writer_lj500")
+    extra = open(os.path.join(g, "script_extra.casl")).read()
+    body = lj500_script(str(tmp_path), 40, extra, "sim precision fp64\nsim rebuild_policy reference\nsim run\nexit\n")
+    (tmp_path / "run.casl").write_text(body)
+    cuda_lib.run_casl(str(tmp_path / "run.casl"))
+    for name in ("o_energy.txt", "o_temperature.txt", "o_pressure.txt", "o_volume.txt", "o_xyz.xyz"):
+        ref = parse_rows(open(os.path.join(g, name)).read())
+        got = parse_rows((tmp_path / name).read_text())
+        assert len(got) == len(ref), name
+        for a, b in zip(got, ref):
+            assert len(a) == len(b), (name, a, b)
+            if len(b) == 1:  # xyz header lines
+                assert a == b
+                continue
+            x, y = np.array(a, float), np.array(b, float)
+            assert np.allclose(x, y, rtol=1.1e-5, atol=1e-9), (name, a, b)
+
+
+@pytest.mark.gpu
+def test_restart_round_trips_bit_exactly(cuda_lib, tmp_path):
+    """Checkpoints: an xyz frame written at 17 significant digits, read back
+    with add_xyz_data_file last_frame replace_data, and the FP64 binary
+    state_file read back with add_state_file replace_data, reproduce the
+    final positions and velocities bit for bit."""
+    t = str(tmp_path)
+    w = ("writer atom_data w\nw set_atom_data adata\nw xyz_step 20\nw xyz_output_velocity 1\nw precision 17\n"
+         "sim add_writer w\n")
+    body = lj500_script(t, 21, w, 'sim rebuild_policy reference\nsim state_file "a.bin"\nsim run\nexit\n')
+    (tmp_path / "a.casl").write_text(body)
+    cuda_lib.run_casl(str(tmp_path / "a.casl"))
+    # reload from the last xyz frame, run no step, dump
+    body = lj500_script(t, 1, 'adata add_xyz_data_file file_name "o_xyz.xyz" last_frame replace_data read_velocity\n',
+                        'sim final_step 0\nsim state_file "b.bin"\nsim run\nexit\n')
+    (tmp_path / "b.casl").write_text(body)
+    cuda_lib.run_casl(str(tmp_path / "b.casl"))
+    body = lj500_script(t, 1, 'adata add_state_file file_name "a.bin" replace_data\n',
+                        'sim final_step 0\nsim state_file "c.bin"\nsim run\nexit\n')
+    (tmp_path / "c.casl").write_text(body)
+    cuda_lib.run_casl(str(tmp_path / "c.casl"))
+    a, b, c = (np.fromfile(tmp_path / f, dtype=np.float64) for f in ("a.bin", "b.bin", "c.bin"))
+    n = 500
+    assert int(a[:1].view(np.int64)[0]) == n
+    pv = slice(1, 1 + 6 * n)  # positions and velocities
+    assert np.array_equal(a[pv], b[pv])
+    assert np.array_equal(a[pv], c[pv])
