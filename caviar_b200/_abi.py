@@ -17,6 +17,7 @@ LIB_PATH = os.environ.get("CAVIAR_B200_LIB", os.path.join(HERE, "libcaviar_b200.
 OK = 0
 ERR = {1: "INVALID", 2: "CUDA", 3: "NAN", 4: "STATE", 5: "GEOMETRY", 6: "CAPACITY", 7: "NOMEM"}
 PREC_MIXED, PREC_FP64 = 0, 1
+RNG_REFERENCE, RNG_PHILOX = 0, 1
 REBUILD_DISPLACEMENT, REBUILD_REFERENCE, REBUILD_EVERY_STEP = 0, 1, 2
 TH_KEYS = ["step", "ke", "temperature", "e_lj", "e_ewald_r", "e_ewald_k", "e_self", "virial", "pressure", "builds"]
 N_THERMO = len(TH_KEYS)
@@ -24,7 +25,7 @@ KT_PAIR, KT_KSPACE, KT_INTEGRATE, KT_BUILD = 0, 1, 2, 3
 
 # Every symbol declared in include/caviar_b200.h.
 EXPORTED = ["cvr_create", "cvr_destroy", "cvr_set_neighborlist", "cvr_set_lj", "cvr_set_ewald_r", "cvr_set_ewald_k",
-            "cvr_set_integrator", "cvr_set_precision", "cvr_set_state", "cvr_build_neighbors", "cvr_compute_forces",
+            "cvr_set_integrator", "cvr_set_langevin", "cvr_set_precision", "cvr_set_state", "cvr_build_neighbors", "cvr_compute_forces",
             "cvr_run", "cvr_get_state", "cvr_get_pairs", "cvr_get_sk", "cvr_get_scalars", "cvr_last_error",
             "cvr_launch_count", "cvr_get_stream", "cvr_get_info", "cvr_set_kernel_timing", "cvr_kernel_time",
             "cvr_structure_factor_noalloc", "cvr_casl_run_file", "cvr_batch_create", "cvr_batch_destroy",
@@ -62,6 +63,8 @@ def load(path: str = LIB_PATH):
     L.cvr_set_ewald_r.argtypes = [vp, ctypes.c_double, ctypes.c_double, _dp, ctypes.c_double]
     L.cvr_set_ewald_k.argtypes = [vp, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double]
     L.cvr_set_integrator.argtypes = [vp, ctypes.c_double, ctypes.c_double]
+    L.cvr_set_langevin.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                   ctypes.c_uint64]
     L.cvr_set_precision.argtypes = [vp, ctypes.c_int]
     L.cvr_set_state.argtypes = [vp, ctypes.c_int64, vp, vp, vp, vp]
     L.cvr_build_neighbors.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
@@ -164,6 +167,11 @@ class Simulation:
             kx, ky, kz = s.ewald_k.kmax
             self._check(self.L.cvr_set_ewald_k(self.h, s.ewald_k.alpha, kx, ky, kz, s.ewald_k.k_electrostatic))
         self._check(self.L.cvr_set_integrator(self.h, s.dt, s.k_b))
+
+    def set_langevin(self, temperature: float, friction: float, kb: float = -1.0, kbt: float = -1.0,
+                     rng: int = RNG_REFERENCE, seed: int = 0):
+        """integrator_type velocity_verlet_langevin (md_simulator.cpp:670-811)."""
+        self._check(self.L.cvr_set_langevin(self.h, temperature, friction, kb, kbt, rng, seed))
 
     def set_state(self, pos, vel=None, typ=None, mol=None):
         pos = np.ascontiguousarray(pos, np.float64)

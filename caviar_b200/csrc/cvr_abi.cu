@@ -12,6 +12,7 @@
 #include <cstring>
 #include <string>
 #include <array>
+#include <random>
 #include <tuple>
 #include <vector>
 
@@ -132,6 +133,18 @@ struct cvr_ctx {
   int64_t graph_kernels[2] = {0, 0};
   long long *counters{};
   long long counter_src[2] = {0, 0};
+  // Langevin integrator (md_simulator.cpp:670-811)
+  int integrator = 0;  // 0 velocity Verlet, 1 velocity Verlet Langevin
+  double lgv_temperature = -1, lgv_friction = 0, lgv_kb = -1, lgv_kbt = -1;
+  int lgv_rng = CVR_RNG_REFERENCE;
+  uint64_t lgv_seed = 0;
+  // the reference's three streams (md_simulator.cpp:45-47): std::mt19937 seeded 1, 2, 3, unit normals
+  std::mt19937 gen[3];
+  std::normal_distribution<double> ndist[3];
+  double *d_eta{};                          // [3][n], caller's atom order
+  double *h_eta[2] = {nullptr, nullptr};    // pinned staging, double-buffered
+  cudaEvent_t eta_done[2] = {nullptr, nullptr};
+  int64_t eta_n = 0;                        // atoms the noise buffers are sized for
   std::vector<void *> all_allocs;
 };
 
@@ -727,6 +740,19 @@ int snapshot(cvr_ctx *c, bool restore) {
 
 // The kernels of one step after the position update: list build (gated by
 // the device flag), forces, second kick, optional thermo record.
+LangevinArgs langevin_args(cvr_ctx *c) {
+  LangevinArgs lg{};
+  const double g = c->lgv_friction, dt = c->dt;
+  lg.a = (2.0 - g * dt) / (2.0 + g * dt);  // md_simulator.cpp:337-344
+  lg.b = c->lgv_kbt > 0 ? std::sqrt(c->lgv_kbt * g * 0.5 * dt) : std::sqrt(c->lgv_kb * c->lgv_temperature * g * 0.5 * dt);
+  lg.c = 2.0 * dt / (2.0 + g * dt);
+  lg.eta = c->d_eta;
+  lg.generate = c->lgv_rng == CVR_RNG_PHILOX ? 1 : 0;
+  lg.seed = c->lgv_seed;
+  lg.step = c->counters;
+  return lg;
+}
+
 template <typename real>
 int launch_step_tail(cvr_ctx *c, bool th) {
   DevState<real> s = dev_state<real>(c);
@@ -734,10 +760,17 @@ int launch_step_tail(cvr_ctx *c, bool th) {
   const int nb = grid_for(c->n, 256);
   {
     Bracket br(c, CVR_KT_INTEGRATE);
-    if (th)
+    if (c->integrator == 1) {
+      const LangevinArgs lg = langevin_args(c);
+      if (th)
+        k_lgv_kick<real, true><<<nb, 256, 0, c->stream>>>(s, c->dt, lg, c->ke_part, c->counters);
+      else
+        k_lgv_kick<real, false><<<nb, 256, 0, c->stream>>>(s, c->dt, lg, c->ke_part, c->counters);
+    } else if (th) {
       k_kick<real, true><<<nb, 256, 0, c->stream>>>(s, c->dt, c->ke_part, c->counters);
-    else
+    } else {
       k_kick<real, false><<<nb, 256, 0, c->stream>>>(s, c->dt, c->ke_part, c->counters);
+    }
   }
   c->launches++;
   if (th) launch_thermo<real>(c, c->d_thermo);
@@ -747,8 +780,31 @@ int launch_step_tail(cvr_ctx *c, bool th) {
 template <typename real>
 void launch_kick_drift(cvr_ctx *c) {
   Bracket br(c, CVR_KT_INTEGRATE);
-  k_kick_drift<real><<<grid_for(c->n, 256), 256, 0, c->stream>>>(dev_state<real>(c), c->dt);
+  if (c->integrator == 1)
+    k_lgv_kick_drift<real><<<grid_for(c->n, 256), 256, 0, c->stream>>>(dev_state<real>(c), c->dt, langevin_args(c));
+  else
+    k_kick_drift<real><<<grid_for(c->n, 256), 256, 0, c->stream>>>(dev_state<real>(c), c->dt);
   c->launches++;
+}
+
+// The reference's noise of one step: for every atom in index order, one
+// draw from each of the three streams (md_simulator.cpp:688-698), into a
+// pinned buffer, then copied to the device ahead of the step's kernels.
+int stage_reference_eta(cvr_ctx *c, int slot) {
+  const int64_t n = c->n;
+  if (!c->h_eta[slot]) {
+    if (cudaMallocHost(&c->h_eta[slot], 3 * (size_t)n * sizeof(double)) != cudaSuccess)
+      return fail(c, CVR_ERR_NOMEM, "pinned noise buffer");
+    cudaEventCreateWithFlags(&c->eta_done[slot], cudaEventDisableTiming);
+  } else {
+    CVR_CUDA(c, cudaEventSynchronize(c->eta_done[slot]));  // its previous copy has finished
+  }
+  double *h = c->h_eta[slot];
+  for (int a = 0; a < 3; ++a)
+    for (int64_t i = 0; i < n; ++i) h[a * n + i] = c->ndist[a](c->gen[a]);
+  CVR_CUDA(c, cudaMemcpyAsync(c->d_eta, h, 3 * (size_t)n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CVR_CUDA(c, cudaEventRecord(c->eta_done[slot], c->stream));
+  return CVR_OK;
 }
 
 void destroy_graphs(cvr_ctx *c) {
@@ -823,12 +879,43 @@ int run_impl(cvr_ctx *c, int64_t nsteps, int64_t every, double *thermo) {
   int f0[4];
   if (int r = read_flags(c, f0)) return r;
   const int64_t step0 = c->step;
+  std::mt19937 gen0[3];
+  std::normal_distribution<double> nd0[3];
+  if (c->integrator == 1) {
+    if (!(c->lgv_kbt > 0) && !(c->lgv_kb > 0 && c->lgv_temperature > 0))
+      return fail(c, CVR_ERR_INVALID, "expected ('temperature'  & 'kb') or 'kbt' input");
+    if (!c->d_eta || c->eta_n != c->n) {
+      if (int r = dalloc(c, &c->d_eta, 3 * (size_t)c->n)) return r;
+      for (int k = 0; k < 2; ++k)
+        if (c->h_eta[k]) {
+          cudaEventSynchronize(c->eta_done[k]);
+          cudaFreeHost(c->h_eta[k]);
+          cudaEventDestroy(c->eta_done[k]);
+          c->h_eta[k] = nullptr;
+          c->eta_done[k] = nullptr;
+        }
+      c->eta_n = c->n;
+    }
+  }
   for (int attempt = 0; attempt < 4; ++attempt) {
     c->counter_src[0] = step0;
     c->counter_src[1] = 0;
     CVR_CUDA(c, cudaMemcpyAsync(c->counters, c->counter_src, sizeof(c->counter_src), cudaMemcpyHostToDevice,
                                 c->stream));
-    const bool graphs = c->use_graphs && !c->timing;
+    // the reference's noise streams are made on the host step by step: no graphs then
+    const bool host_noise = c->integrator == 1 && c->lgv_rng == CVR_RNG_REFERENCE;
+    const bool graphs = c->use_graphs && !c->timing && !host_noise;
+    if (attempt == 0) {
+      for (int a = 0; a < 3; ++a) {
+        gen0[a] = c->gen[a];
+        nd0[a] = c->ndist[a];
+      }
+    } else {
+      for (int a = 0; a < 3; ++a) {
+        c->gen[a] = gen0[a];
+        c->ndist[a] = nd0[a];
+      }
+    }
     if (graphs && c->graph_epoch != c->epoch)
       if (int r = build_graphs<real>(c)) return r;
     const int64_t launches0 = c->launches;
@@ -837,6 +924,8 @@ int run_impl(cvr_ctx *c, int64_t nsteps, int64_t every, double *thermo) {
       if (graphs) {
         CVR_CUDA(c, cudaGraphLaunch(c->g_step[th ? 1 : 0], c->stream));
       } else {
+        if (host_noise)
+          if (int r = stage_reference_eta(c, (int)(k & 1))) return r;
         launch_kick_drift<real>(c);
         launch_build<real>(c, 0);
         if (int r = launch_step_tail<real>(c, th)) return r;
@@ -1024,6 +1113,7 @@ int cvr_create(cvr_ctx **out, const double lo[3], const double hi[3], const int 
     if (!(hi[d] > lo[d]) || (bc[d] != 0 && bc[d] != 1)) return CVR_ERR_INVALID;
   if (cudaSetDevice(device) != cudaSuccess) return CVR_ERR_CUDA;
   cvr_ctx *c = new cvr_ctx();
+  for (int a = 0; a < 3; ++a) c->gen[a].seed((unsigned)(a + 1));  // md_simulator.cpp:45-47
   c->device = device;
   for (int d = 0; d < 3; ++d) {
     c->lo[d] = lo[d];
@@ -1054,6 +1144,10 @@ void cvr_destroy(cvr_ctx *c) {
   cudaStreamSynchronize(c->stream);
   destroy_graphs(c);
   for (void *p : c->all_allocs) cudaFree(p);
+  for (int k = 0; k < 2; ++k) {
+    if (c->h_eta[k]) cudaFreeHost(c->h_eta[k]);
+    if (c->eta_done[k]) cudaEventDestroy(c->eta_done[k]);
+  }
   for (auto &k : c->kt)
     for (auto &e : k.ev) {
       cudaEventDestroy(e.first);
@@ -1133,6 +1227,25 @@ int cvr_set_integrator(cvr_ctx *c, double dt, double k_b) {
   if (!(k_b > 0)) return fail(c, CVR_ERR_INVALID, "k_b is not set.");
   c->dt = dt;
   c->k_b = k_b;
+  return CVR_OK;
+}
+
+int cvr_set_langevin(cvr_ctx *c, double temperature, double friction, double kb, double kbt, int rng,
+                     uint64_t seed) {
+  if (!c) return CVR_ERR_INVALID;
+  if (temperature < 0 && temperature != -1) return fail(c, CVR_ERR_INVALID, "Temperature have to non-negative.");
+  if (!(friction >= 0)) return fail(c, CVR_ERR_INVALID, "friction have to non-negative.");
+  if (rng != CVR_RNG_REFERENCE && rng != CVR_RNG_PHILOX) return fail(c, CVR_ERR_INVALID, "unknown noise generator");
+  if (!(kbt > 0) && !(kb > 0 && temperature > 0))
+    return fail(c, CVR_ERR_INVALID, "expected ('temperature'  & 'kb') or 'kbt' input");
+  c->integrator = 1;
+  c->lgv_temperature = temperature;
+  c->lgv_friction = friction;
+  c->lgv_kb = kb;
+  c->lgv_kbt = kbt;
+  c->lgv_rng = rng;
+  c->lgv_seed = seed;
+  c->epoch++;  // the step graphs bake the integrator's kernels in
   return CVR_OK;
 }
 

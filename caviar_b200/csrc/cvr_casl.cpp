@@ -26,7 +26,8 @@
 //                              k_electrostatic, set_atom_data, set_domain (electrostatic_ewald_k.cpp:48-143)
 //   md_simulator basic <name>  set_atom_data, add_force_field|force_field,
 //                              add_neighborlist|neighborlist, add_writer|writer,
-//                              integrator_type velocity_verlet, dt, initial_step,
+//                              integrator_type velocity_verlet|velocity_verlet_langevin,
+//                              temperature, friction, kb, kbt, dt, initial_step,
 //                              final_step, final_step_add, run (md_simulator.cpp:58-233)
 //   writer atom_data <name>    set_atom_data|atom_data, set_domain|domain, energy_step,
 //                              temperature_step, pressure_step, volume_step, xyz_step,
@@ -36,8 +37,8 @@
 //                              (writer/atom_data.cpp:84-331, dump_energy.cpp, dump_xyz_serial.cpp)
 // plus the variables `real name value` / `int name value`, comments (#) and
 // `exit`.  Keywords of these objects that sit off the hot path (constraints,
-// Langevin, slab/dipole Ewald, jump_tol, msd/povray/ghost writers) are
-// rejected with a message instead of being ignored.
+// slab/dipole Ewald, jump_tol, msd/povray/ghost writers) are rejected with a
+// message instead of being ignored.
 //
 // Writers follow the reference: a line "step time value" (default stream
 // format, 6 significant digits) at setup as (0, 0) and after every step i
@@ -48,7 +49,9 @@
 // type [id] x y z [v] [a]" with positions wrapped into the box.  File names
 // get ".txt" / ".xyz" and are relative to the script's directory.
 //
-// Extensions for the B200 path (md_simulator): precision mixed|fp64,
+// Extensions for the B200 path (md_simulator): rng reference|philox and seed N
+// (the Langevin noise: the reference's own streams, or a counter-based
+// generator on the GPU), precision mixed|fp64,
 // rebuild_policy displacement|reference, thermo_step N, thermo_file "<f>",
 // state_file "<f>" (FP64 binary dump of the final state, id order);
 // (atom_data) add_state_file file_name "<f>" [replace_data] (reads that dump
@@ -223,6 +226,10 @@ struct Md_simulator : Object {
   std::vector<Writer *> writer;
   bool initialized = false;  // the reference's setup (and its (0, 0) writer call) happens once
   double time = 0.0;
+  bool langevin = false;     // integrator_type velocity_verlet_langevin
+  double lgv_temperature = -1, lgv_friction = 0, lgv_kb = -1, lgv_kbt = -1;  // md_simulator.cpp:48-51
+  int lgv_rng = CVR_RNG_REFERENCE;
+  int64_t lgv_seed = 0;
   std::vector<Force_field *> force_field;
   std::vector<Neighborlist *> neighborlist;
   double dt = -1.0;
@@ -571,8 +578,33 @@ struct Script {
       else if (t == "add_writer" || t == "writer") m.writer.push_back(find<Writer>(word()));
       else if (t == "integrator_type") {
         const std::string v = word();
-        if (v != "velocity_verlet") err("integrator_type '" + v + "' is not on the B200 hot path");
-        m.vv = true;
+        if (v == "velocity_verlet") {
+          m.vv = true;
+          m.langevin = false;
+        } else if (v == "velocity_verlet_langevin") {
+          m.vv = true;
+          m.langevin = true;
+        } else {
+          err("integrator_type '" + v + "' is not on the B200 hot path");
+        }
+      } else if (t == "temperature") {
+        m.lgv_temperature = real();
+        if (m.lgv_temperature < 0.0) err("Temperature have to non-negative.");
+      } else if (t == "friction") {
+        m.lgv_friction = real();
+        if (m.lgv_friction < 0.0) err("friction have to non-negative.");
+      } else if (t == "kb") {
+        m.lgv_kb = real();
+        if (m.lgv_kb < 0.0) err("kb have to non-negative.");
+      } else if (t == "kbt") {
+        m.lgv_kbt = real();
+      } else if (t == "rng") {
+        const std::string v = word();
+        if (v == "reference") m.lgv_rng = CVR_RNG_REFERENCE;
+        else if (v == "philox") m.lgv_rng = CVR_RNG_PHILOX;
+        else err("rng reference|philox");
+      } else if (t == "seed") {
+        m.lgv_seed = integer();
       } else if (t == "dt") m.dt = real();
       else if (t == "initial_step") m.initial_step = integer(), m.use_step = true;
       else if (t == "final_step") m.final_step = integer(), m.use_step = true;
@@ -782,6 +814,9 @@ struct Script {
       }
     }
     check(cvr_set_integrator(ctx, m.dt, a->k_b > 0 ? a->k_b : 1.0));
+    if (m.langevin)
+      check(cvr_set_langevin(ctx, m.lgv_temperature, m.lgv_friction, m.lgv_kb, m.lgv_kbt, m.lgv_rng,
+                             (uint64_t)m.lgv_seed));
     bool any_mol = false;
     for (int32_t v : a->mol) any_mol = any_mol || v >= 0;
     check(cvr_set_state(ctx, a->n(), a->pos.data(), a->vel.data(), a->type.data(), any_mol ? a->mol.data() : nullptr));

@@ -475,6 +475,38 @@ __global__ void __launch_bounds__(256) k_kforce_reduce(DevState<real> s, KArgs<r
 // (md_simulator.cpp:591-616) without storing a_old.  The first half also
 // writes the cell-local coordinates for the pair kernel and raises the
 // rebuild flag (neighborlist.cpp:91-139 / md_simulator.cpp:487-502).
+// After a position update of atom i (cell order) to p: the cell-local
+// coordinates for the pair kernel, and whether the list must be rebuilt.
+template <typename real>
+__device__ __forceinline__ bool update_local(DevState<real> &s, int i, const double (&p)[3]) {
+  bool need = false;
+  int cc[3];
+  cell_xyz(s, s.cell[i], cc[0], cc[1], cc[2]);
+  double loc[3];
+  int code = 0, mul = 1;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    loc[d] = p[d] - (s.box.lo[d] + (cc[d] + 0.5) * s.cells.w[d]);
+    if (s.policy == 1) {
+      if (s.box.bc[d] == 1 && (p[d] < s.box.lo[d] || p[d] > s.box.hi[d])) need = true;  // owned wrap
+      code += (ghost_val(p[d], s.box.gclo[d], s.box.gchi[d], s.box.bc[d]) + 1) * mul;
+      mul *= 3;
+    }
+  }
+  typename V4<real>::t q = s.x4[i];
+  q.x = (real)loc[0];
+  q.y = (real)loc[1];
+  q.z = (real)loc[2];
+  s.x4[i] = q;
+  const float4 b = s.xb[i];
+  const float ex = (float)(p[0] - s.box.ctr[0]) - b.x, ey = (float)(p[1] - s.box.ctr[1]) - b.y,
+              ez = (float)(p[2] - s.box.ctr[2]) - b.z;
+  if (ex * ex + ey * ey + ez * ez > s.thr_sq) need = true;
+  if (s.policy == 1 && code != s.gcls[i]) need = true;  // ghost set changed
+  if (s.policy == 2) need = true;
+  return need;
+}
+
 template <typename real>
 __global__ void __launch_bounds__(256) k_kick_drift(DevState<real> s, double dt) {
   if (*s.err) return;
@@ -492,32 +524,123 @@ __global__ void __launch_bounds__(256) k_kick_drift(DevState<real> s, double dt)
     s.x[i] = p[0];
     s.y[i] = p[1];
     s.z[i] = p[2];
-    int cc[3];
-    cell_xyz(s, s.cell[i], cc[0], cc[1], cc[2]);
-    double loc[3];
-    int code = 0, mul = 1;
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      loc[d] = p[d] - (s.box.lo[d] + (cc[d] + 0.5) * s.cells.w[d]);
-      if (s.policy == 1) {
-        if (s.box.bc[d] == 1 && (p[d] < s.box.lo[d] || p[d] > s.box.hi[d])) need = true;  // owned wrap
-        code += (ghost_val(p[d], s.box.gclo[d], s.box.gchi[d], s.box.bc[d]) + 1) * mul;
-        mul *= 3;
-      }
-    }
-    typename V4<real>::t q = s.x4[i];
-    q.x = (real)loc[0];
-    q.y = (real)loc[1];
-    q.z = (real)loc[2];
-    s.x4[i] = q;
-    const float4 b = s.xb[i];
-    const float ex = (float)(p[0] - s.box.ctr[0]) - b.x, ey = (float)(p[1] - s.box.ctr[1]) - b.y,
-                ez = (float)(p[2] - s.box.ctr[2]) - b.z;
-    if (ex * ex + ey * ey + ez * ez > s.thr_sq) need = true;
-    if (s.policy == 1 && code != s.gcls[i]) need = true;  // ghost set changed
-    if (s.policy == 2) need = true;
+    need = update_local(s, i, p);
   }
   if (__any_sync(0xffffffffu, need) && (threadIdx.x & 31) == 0) *s.flag = 1;
+}
+
+// ------------------------------------------------------ Langevin (GJF-type)
+// The reference's velocity_verlet_langevin (md_simulator.cpp:670-811), per
+// step with one Gaussian vector eta per atom:
+//   v += dt/2 a + b eta;  r += c v;  forces;  v = a_c v + b eta + dt/2 a
+// with a_c = (2 - g dt)/(2 + g dt), b = sqrt(kT g dt/2), c = 2 dt/(2 + g dt)
+// (md_simulator.cpp:333-344).  eta is read from (or, with the counter-based
+// generator, written to) `eta`, SoA [3][n] in the caller's atom order.
+
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as
+// easy as 1, 2, 3", SC'11): ten rounds of two 32x32 -> 64 multiplies with a
+// Weyl-sequence key schedule; counter = (atom id, step low, step high, 0),
+// key = seed.  Box-Muller turns the four 32-bit words into normals.
+__device__ __forceinline__ uint4 philox4x32_10(uint4 ctr, uint2 key) {
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    const uint32_t lo0 = 0xD2511F53u * ctr.x, hi0 = __umulhi(0xD2511F53u, ctr.x);
+    const uint32_t lo1 = 0xCD9E8D57u * ctr.z, hi1 = __umulhi(0xCD9E8D57u, ctr.z);
+    ctr = make_uint4(hi1 ^ ctr.y ^ key.x, lo1, hi0 ^ ctr.w ^ key.y, lo0);
+    key.x += 0x9E3779B9u;
+    key.y += 0xBB67AE85u;
+  }
+  return ctr;
+}
+
+__device__ __forceinline__ void philox_normals(uint64_t seed, long long step, int id, double g[3]) {
+  const uint4 r = philox4x32_10(make_uint4((uint32_t)id, (uint32_t)step, (uint32_t)((unsigned long long)step >> 32), 0u),
+                                make_uint2((uint32_t)seed, (uint32_t)(seed >> 32)));
+  const double k = 2.3283064365386963e-10;  // 2^-32: uniforms in (0, 1)
+  const double u0 = ((double)r.x + 0.5) * k, u1 = ((double)r.y + 0.5) * k;
+  const double u2 = ((double)r.z + 0.5) * k, u3 = ((double)r.w + 0.5) * k;
+  const double r0 = sqrt(-2.0 * log(u0)), r1 = sqrt(-2.0 * log(u2));
+  double s0, c0, s1, c1;
+  sincospi(2.0 * u1, &s0, &c0);
+  sincospi(2.0 * u3, &s1, &c1);
+  g[0] = r0 * c0;
+  g[1] = r0 * s0;
+  g[2] = r1 * c1;
+}
+
+struct LangevinArgs {
+  double a, b, c;
+  double *eta;             // [3][n], the caller's atom order
+  int generate;            // 1: draw eta on the device (counter-based), 0: read the host-made eta
+  uint64_t seed;
+  const long long *step;   // counters[0]: steps done so far
+};
+
+template <typename real>
+__global__ void __launch_bounds__(256) k_lgv_kick_drift(DevState<real> s, double dt, LangevinArgs lg) {
+  if (*s.err) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  bool need = false;
+  if (i < s.n) {
+    const int id = s.id[i];
+    double eta[3];
+    if (lg.generate) {
+      philox_normals(lg.seed, *lg.step, id, eta);
+      lg.eta[id] = eta[0];
+      lg.eta[s.n + id] = eta[1];
+      lg.eta[2 * s.n + id] = eta[2];
+    } else {
+      eta[0] = lg.eta[id];
+      eta[1] = lg.eta[s.n + id];
+      eta[2] = lg.eta[2 * s.n + id];
+    }
+    const double a0 = (double)s.ax[i], a1 = (double)s.ay[i], a2 = (double)s.az[i];
+    if (isnan(a0) || isnan(a1) || isnan(a2)) atomicOr(s.err, ERR_NAN);  // md_simulator.cpp:707-713
+    // vel += 0.5 * acc * dt + b * eta (md_simulator.cpp:717); pos += vel * c (:764)
+    const double v0 = s.vx[i] + (0.5 * a0 * dt + lg.b * eta[0]);
+    const double v1 = s.vy[i] + (0.5 * a1 * dt + lg.b * eta[1]);
+    const double v2 = s.vz[i] + (0.5 * a2 * dt + lg.b * eta[2]);
+    const double p[3] = {s.x[i] + v0 * lg.c, s.y[i] + v1 * lg.c, s.z[i] + v2 * lg.c};
+    s.vx[i] = v0;
+    s.vy[i] = v1;
+    s.vz[i] = v2;
+    s.x[i] = p[0];
+    s.y[i] = p[1];
+    s.z[i] = p[2];
+    need = update_local(s, i, p);
+  }
+  if (__any_sync(0xffffffffu, need) && (threadIdx.x & 31) == 0) *s.flag = 1;
+}
+
+// vel = a vel + b eta + 0.5 acc dt (md_simulator.cpp:790); KE partials, flag
+// and step counter as k_kick.
+template <typename real, bool KE>
+__global__ void __launch_bounds__(256) k_lgv_kick(DevState<real> s, double dt, LangevinArgs lg,
+                                                  double *__restrict__ partials, long long *__restrict__ counters) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    *s.flag = 0;
+    if (counters) counters[0]++;
+  }
+  if (*s.err) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double v[4] = {0, 0, 0, 0};
+  if (i < s.n) {
+    const int id = s.id[i];
+    const double v0 = lg.a * s.vx[i] + lg.b * lg.eta[id] + 0.5 * (double)s.ax[i] * dt;
+    const double v1 = lg.a * s.vy[i] + lg.b * lg.eta[s.n + id] + 0.5 * (double)s.ay[i] * dt;
+    const double v2 = lg.a * s.vz[i] + lg.b * lg.eta[2 * s.n + id] + 0.5 * (double)s.az[i] * dt;
+    s.vx[i] = v0;
+    s.vy[i] = v1;
+    s.vz[i] = v2;
+    if (KE) {
+      const double m = s.mass[s.type[i]];
+      v[0] = m * (v0 * v0 + v1 * v1 + v2 * v2);
+      v[1] = m * v0;
+      v[2] = m * v1;
+      v[3] = m * v2;
+    }
+  }
+  if (KE) block_sum_store<4>(v, partials);
 }
 
 // Second half kick; KE partials (sum m v^2, sum m v) when KE.  Also clears

@@ -94,6 +94,21 @@ int cvr_set_ewald_k(cvr_ctx *ctx, double alpha, int kx_max, int ky_max, int kz_m
  * Replaces: Md_simulator::read dt / integrator_type velocity_verlet (md_simulator.cpp:58-233). */
 int cvr_set_integrator(cvr_ctx *ctx, double dt, double k_b);
 
+/* Langevin velocity Verlet, the reference's `integrator_type
+ * velocity_verlet_langevin` (md_simulator.cpp:670-811) with its keywords
+ * temperature, friction, kb, kbt (md_simulator.cpp:198-222): per step one
+ * Gaussian vector eta per atom, v += dt/2 a + b eta, r += c v, forces,
+ * v = a_c v + b eta + dt/2 a, a_c = (2 - g dt)/(2 + g dt),
+ * b = sqrt(kbt g dt / 2) (or kb T in place of kbt), c = 2 dt / (2 + g dt).
+ * rng: CVR_RNG_REFERENCE draws eta from the reference's own three streams
+ * (std::mt19937 seeded 1, 2, 3 with std::normal_distribution, on the host,
+ * the same numbers the reference uses); CVR_RNG_PHILOX draws it on the GPU
+ * from a counter-based generator keyed by (seed, step, atom). */
+#define CVR_RNG_REFERENCE 0
+#define CVR_RNG_PHILOX 1
+int cvr_set_langevin(cvr_ctx *c, double temperature, double friction, double kb, double kbt, int rng,
+                     uint64_t seed);
+
 /* CVR_PREC_MIXED (default) or CVR_PREC_FP64.  No reference counterpart
  * (the reference is FP64 only). */
 int cvr_set_precision(cvr_ctx *ctx, int precision);

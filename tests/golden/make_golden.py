@@ -28,6 +28,10 @@ GPU tests never need the reference at run time).
    accelerations every 20; temperature_process and pressure_process on), with
    the script lines that declare the writer (WRITER_SCRIPT).
 
+5. ref_langevin500.npz -- 20 steps of the reference's velocity_verlet_langevin
+   (T 1.2, friction 0.5, kb 1) on that fluid: final positions, velocities
+   and the kinetic-energy trace.
+
 Usage:  python tests/golden/make_golden.py [/path/to/reference]
 """
 import json
@@ -167,6 +171,21 @@ def writer_lj500(nsteps: int = 40) -> None:
         f.write(WRITER_SCRIPT)
 
 
+LANGEVIN_SCRIPT = """sim integrator_type velocity_verlet_langevin
+sim temperature 1.2
+sim friction 0.5
+sim kb 1.0
+"""
+
+
+def langevin500(nsteps: int = 20) -> None:
+    s = W.fcc_lattice(5, 0.8442, 0.72, seed=7, jitter=0.05)
+    r = O.run_reference(s, "run", nsteps, extra=LANGEVIN_SCRIPT)
+    order = np.argsort(r["id"].astype(np.int64))
+    np.savez_compressed(os.path.join(HERE, "ref_langevin500.npz"), pos=r["pos"].reshape(-1, 3)[order],
+                        vel=r["vel"].reshape(-1, 3)[order], ke=r["ke_trace"], nsteps=nsteps, script=LANGEVIN_SCRIPT)
+
+
 def main():
     ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     g = ewald_n100(ref_root)
@@ -178,6 +197,7 @@ def main():
     with open(os.path.join(HERE, "nve_lj500.json"), "w") as f:
         json.dump(nve_lj500(), f, indent=0)
     writer_lj500()
+    langevin500()
     print("golden fixtures written to", HERE)
 
 
