@@ -25,7 +25,8 @@ KT_PAIR, KT_KSPACE, KT_INTEGRATE, KT_BUILD = 0, 1, 2, 3
 
 # Every symbol declared in include/caviar_b200.h.
 EXPORTED = ["cvr_create", "cvr_destroy", "cvr_set_neighborlist", "cvr_set_lj", "cvr_set_ewald_r", "cvr_set_ewald_k",
-            "cvr_set_integrator", "cvr_set_langevin", "cvr_set_precision", "cvr_set_state", "cvr_build_neighbors", "cvr_compute_forces",
+            "cvr_set_integrator", "cvr_set_langevin", "cvr_set_berendsen", "cvr_set_nose_hoover",
+            "cvr_clear_thermostat", "cvr_set_precision", "cvr_set_state", "cvr_build_neighbors", "cvr_compute_forces",
             "cvr_run", "cvr_get_state", "cvr_get_pairs", "cvr_get_sk", "cvr_get_scalars", "cvr_last_error",
             "cvr_launch_count", "cvr_get_stream", "cvr_get_info", "cvr_set_kernel_timing", "cvr_kernel_time",
             "cvr_structure_factor_noalloc", "cvr_casl_run_file", "cvr_batch_create", "cvr_batch_destroy",
@@ -66,6 +67,11 @@ def load(path: str = LIB_PATH):
     L.cvr_set_langevin.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                    ctypes.c_uint64]
     L.cvr_set_precision.argtypes = [vp, ctypes.c_int]
+    L.cvr_set_berendsen.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                    ctypes.c_double, ctypes.c_double]
+    L.cvr_set_nose_hoover.argtypes = [vp, ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                      ctypes.c_double, ctypes.c_double]
+    L.cvr_clear_thermostat.argtypes = [vp]
     L.cvr_set_state.argtypes = [vp, ctypes.c_int64, vp, vp, vp, vp]
     L.cvr_build_neighbors.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     L.cvr_compute_forces.argtypes = [vp, vp, _dp]
@@ -172,6 +178,16 @@ class Simulation:
                      rng: int = RNG_REFERENCE, seed: int = 0):
         """integrator_type velocity_verlet_langevin (md_simulator.cpp:670-811)."""
         self._check(self.L.cvr_set_langevin(self.h, temperature, friction, kb, kbt, rng, seed))
+
+    def set_berendsen(self, temperature: float, coupling: float, dt: float, step: int = 1, lambda_min: float = 0.8,
+                      lambda_max: float = 1.25):
+        """constraint berendsen (constraint/berendsen.cpp:44-131), defaults from berendsen.h:50-60."""
+        self._check(self.L.cvr_set_berendsen(self.h, temperature, coupling, dt, step, lambda_min, lambda_max))
+
+    def set_nose_hoover(self, temperature: float, dt: float, type: int = 1, mass: float = -1.0, tau: float = -1.0,
+                        kb: float = 1.0):
+        """constraint nose_hoover (constraint/nose_hoover.cpp:36-180)."""
+        self._check(self.L.cvr_set_nose_hoover(self.h, temperature, type, mass, tau, kb, dt))
 
     def set_state(self, pos, vel=None, typ=None, mol=None):
         pos = np.ascontiguousarray(pos, np.float64)

@@ -145,6 +145,9 @@ struct cvr_ctx {
   double *h_eta[2] = {nullptr, nullptr};    // pinned staging, double-buffered
   cudaEvent_t eta_done[2] = {nullptr, nullptr};
   int64_t eta_n = 0;                        // atoms the noise buffers are sized for
+  // thermostat applied after each velocity-Verlet step (0 none, 1 Berendsen, 2 Nose-Hoover)
+  ThermostatArgs tstat{};
+  double *d_tscal{};  // [0] Berendsen factor, [1] Nose-Hoover zeta (carried across calls)
   std::vector<void *> all_allocs;
 };
 
@@ -766,10 +769,29 @@ int launch_step_tail(cvr_ctx *c, bool th) {
         k_lgv_kick<real, true><<<nb, 256, 0, c->stream>>>(s, c->dt, lg, c->ke_part, c->counters);
       else
         k_lgv_kick<real, false><<<nb, 256, 0, c->stream>>>(s, c->dt, lg, c->ke_part, c->counters);
-    } else if (th) {
+    } else if (th || c->tstat.kind) {
       k_kick<real, true><<<nb, 256, 0, c->stream>>>(s, c->dt, c->ke_part, c->counters);
     } else {
       k_kick<real, false><<<nb, 256, 0, c->stream>>>(s, c->dt, c->ke_part, c->counters);
+    }
+    if (c->tstat.kind && c->integrator == 0) {
+      ThermostatArgs t = c->tstat;
+      const int bcsum = c->bc[0] + c->bc[1] + c->bc[2];
+      const int n_r_df = (bcsum == 0) ? 6 : (bcsum == 3 ? 3 : 6 - bcsum);  // atom_data.cpp:322-349
+      t.com_removed = (n_r_df >= 1 && n_r_df <= 3) ? 1 : 0;
+      t.dof = 3.0 * (double)c->n - n_r_df;
+      t.total_mass = c->total_mass;
+      t.k_b = c->k_b;
+      t.ke_part = c->ke_part;
+      t.n_ke = c->n_ke_blocks;
+      t.counters = c->counters;
+      t.scal = c->d_tscal;
+      k_thermostat_coef<<<1, 256, 0, c->stream>>>(t);
+      if (th)
+        k_thermostat_apply<real, true><<<nb, 256, 0, c->stream>>>(s, t.kind, c->d_tscal, c->ke_part);
+      else
+        k_thermostat_apply<real, false><<<nb, 256, 0, c->stream>>>(s, t.kind, c->d_tscal, c->ke_part);
+      c->launches += 2;
     }
   }
   c->launches++;
@@ -881,6 +903,8 @@ int run_impl(cvr_ctx *c, int64_t nsteps, int64_t every, double *thermo) {
   const int64_t step0 = c->step;
   std::mt19937 gen0[3];
   std::normal_distribution<double> nd0[3];
+  if (c->integrator == 1 && c->tstat.kind)
+    return fail(c, CVR_ERR_INVALID, "a thermostat constraint with the Langevin integrator is not supported");
   if (c->integrator == 1) {
     if (!(c->lgv_kbt > 0) && !(c->lgv_kb > 0 && c->lgv_temperature > 0))
       return fail(c, CVR_ERR_INVALID, "expected ('temperature'  & 'kb') or 'kbt' input");
@@ -936,7 +960,8 @@ int run_impl(cvr_ctx *c, int64_t nsteps, int64_t every, double *thermo) {
     collect_timing(c);
     if (graphs) {
       // kernel nodes executed: per step kick_drift + condition + tail; 8 per rebuild
-      const int tail = 1 + (c->lj_on || c->ewr_on ? 1 : 0) + ((c->ewk_on && c->nk > 0) ? (c->kf_slices > 1 ? 4 : 3) : 0);
+      const int tail = 1 + (c->lj_on || c->ewr_on ? 1 : 0) + ((c->ewk_on && c->nk > 0) ? (c->kf_slices > 1 ? 4 : 3) : 0) +
+                       ((c->tstat.kind && c->integrator == 0) ? 2 : 0);
       c->launches = launches0 + nsteps * (2 + tail) + nrec + 8 * (int64_t)(f[3] - f0[3]);
     }
     if (f[1] & ERR_NAN) return fail(c, CVR_ERR_NAN, "NaN acceleration");
@@ -1246,6 +1271,69 @@ int cvr_set_langevin(cvr_ctx *c, double temperature, double friction, double kb,
   c->lgv_rng = rng;
   c->lgv_seed = seed;
   c->epoch++;  // the step graphs bake the integrator's kernels in
+  return CVR_OK;
+}
+
+namespace {
+int thermostat_buffer(cvr_ctx *c) {
+  if (!c->d_tscal) {
+    if (int r = dalloc(c, &c->d_tscal, 2)) return r;
+    const double init[2] = {1.0, 0.0};
+    CVR_CUDA(c, cudaMemcpyAsync(c->d_tscal, init, sizeof(init), cudaMemcpyHostToDevice, c->stream));
+  }
+  return CVR_OK;
+}
+}  // namespace
+
+int cvr_set_berendsen(cvr_ctx *c, double temperature, double coupling, double dt, int step, double lambda_min,
+                      double lambda_max) {
+  if (!c) return CVR_ERR_INVALID;
+  if (!(temperature > 0)) return fail(c, CVR_ERR_INVALID, "Temperature have to non-negative.");
+  if (!(coupling > 0)) return fail(c, CVR_ERR_INVALID, "coupling is not set.");
+  if (!(dt > 0)) return fail(c, CVR_ERR_INVALID, "dt is not set.");
+  if (step <= 0) return fail(c, CVR_ERR_INVALID, "step have to non-negative.");
+  if (!(lambda_min > 0) || !(lambda_max > 0)) return fail(c, CVR_ERR_INVALID, "lambda_min, lambda_max > 0");
+  if (int r = thermostat_buffer(c)) return r;
+  c->tstat = ThermostatArgs{};
+  c->tstat.kind = 1;
+  c->tstat.T0 = temperature;
+  c->tstat.tau = coupling;
+  c->tstat.dt = dt;
+  c->tstat.every = step;
+  c->tstat.lambda_min = lambda_min;
+  c->tstat.lambda_max = lambda_max;
+  c->epoch++;  // the step graphs bake the thermostat in
+  return CVR_OK;
+}
+
+int cvr_set_nose_hoover(cvr_ctx *c, double temperature, int type, double mass, double tau, double kb, double dt) {
+  if (!c) return CVR_ERR_INVALID;
+  if (!(temperature > 0)) return fail(c, CVR_ERR_INVALID, "Temperature have to non-negative.");
+  if (!(dt > 0)) return fail(c, CVR_ERR_INVALID, "dt is not set.");
+  if (type == 1 && !(mass > 0)) return fail(c, CVR_ERR_INVALID, "mass is not set.");
+  if (type == 2 && !(tau > 0)) return fail(c, CVR_ERR_INVALID, "tau is not set.");
+  if (type != 1 && type != 2)
+    return fail(c, CVR_ERR_INVALID, "this Nose-Hoover type is not implemented.  Expected type 1 or 2");
+  if (!(kb > 0)) return fail(c, CVR_ERR_INVALID, "kb have to non-negative.");
+  if (int r = thermostat_buffer(c)) return r;
+  c->tstat = ThermostatArgs{};
+  c->tstat.kind = 2;
+  c->tstat.T0 = temperature;
+  c->tstat.dt = dt;
+  c->tstat.nh_type = type;
+  c->tstat.nh_mass = mass;
+  c->tstat.nh_tau = tau;
+  c->tstat.nh_kb = kb;
+  const double zero = 0.0;
+  CVR_CUDA(c, cudaMemcpyAsync(c->d_tscal + 1, &zero, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  c->epoch++;
+  return CVR_OK;
+}
+
+int cvr_clear_thermostat(cvr_ctx *c) {
+  if (!c) return CVR_ERR_INVALID;
+  c->tstat = ThermostatArgs{};
+  c->epoch++;
   return CVR_OK;
 }
 

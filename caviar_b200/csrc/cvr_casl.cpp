@@ -35,10 +35,14 @@
 //                              xyz_output_id, xyz_output_velocity, xyz_output_acceleration,
 //                              open_files, close_files, *_mpi_rank0, *_mpi_per_process
 //                              (writer/atom_data.cpp:84-331, dump_energy.cpp, dump_xyz_serial.cpp)
+//   constraint berendsen <name>    set_atom_data, temperature, coupling, dt, step,
+//                                  lambda_min, lambda_max (constraint/berendsen.cpp:36-96)
+//   constraint nose_hoover <name>  set_atom_data, temperature, mass, tau, type, kb, dt
+//                                  (constraint/nose_hoover.cpp:39-117); md_simulator add_constraint
 // plus the variables `real name value` / `int name value`, comments (#) and
-// `exit`.  Keywords of these objects that sit off the hot path (constraints,
-// slab/dipole Ewald, jump_tol, msd/povray/ghost writers) are rejected with a
-// message instead of being ignored.
+// `exit`.  Keywords of these objects that sit off the hot path (other
+// constraints, slab/dipole Ewald, jump_tol, msd/povray/ghost writers) are
+// rejected with a message instead of being ignored.
 //
 // Writers follow the reference: a line "step time value" (default stream
 // format, 6 significant digits) at setup as (0, 0) and after every step i
@@ -221,8 +225,19 @@ struct Writer : Object {
 };
 enum { W_ENERGY = 0, W_TEMPERATURE, W_PRESSURE, W_VOLUME, W_PE, W_XYZ };
 
+// constraint berendsen / nose_hoover (constraint/berendsen.cpp:25-96, nose_hoover.cpp:25-117)
+struct Thermostat : Object {
+  bool nose_hoover = false;
+  Atom_data *atom_data = nullptr;
+  double temperature = -1, coupling = -1, dt = -1, lambda_min = 0.8, lambda_max = 1.25;  // berendsen.h:50-60
+  int step = 1;
+  int type = 1;                                // nose_hoover.cpp:27-33
+  double mass = -1, tau = -1, kb = 1.0;
+};
+
 struct Md_simulator : Object {
   Atom_data *atom_data = nullptr;
+  std::vector<Thermostat *> constraint;
   std::vector<Writer *> writer;
   bool initialized = false;  // the reference's setup (and its (0, 0) writer call) happens once
   double time = 0.0;
@@ -288,6 +303,11 @@ struct Script {
     else if (cls == "force_field" && type == "electrostatic_ewald_k") o.reset(new Ewald_k);
     else if (cls == "md_simulator" && type == "basic") o.reset(new Md_simulator);
     else if (cls == "writer" && type == "atom_data") o.reset(new Writer);
+    else if (cls == "constraint" && (type == "berendsen" || type == "nose_hoover")) {
+      auto *t = new Thermostat;
+      t->nose_hoover = type == "nose_hoover";
+      o.reset(t);
+    }
     else err("'" + cls + " " + type + "' is not on the B200 hot path");
     o->name = nm;
     objects[nm] = std::move(o);
@@ -434,6 +454,43 @@ struct Script {
     }
   }
 
+  void read_thermostat(Thermostat &c) {
+    while (!cur->done()) {
+      const std::string t = word();
+      if (t == "set_atom_data" || t == "atom_data") c.atom_data = find<Atom_data>(word());
+      else if (t == "temperature") {
+        c.temperature = real();
+        if (c.temperature <= 0.0) err("Temperature have to non-negative.");
+      } else if (t == "dt") {
+        c.dt = real();
+        if (c.dt <= 0.0) err("dt have to non-negative.");
+      } else if (!c.nose_hoover && t == "coupling") {
+        c.coupling = real();
+        if (c.coupling <= 0.0) err("coupling have to non-negative.");
+      } else if (!c.nose_hoover && t == "step") {
+        c.step = integer();
+        if (c.step <= 0) err("step have to non-negative.");
+      } else if (!c.nose_hoover && (t == "lambda_min" || t == "lambda_max")) {
+        const double v = real();
+        if (v <= 0.0) err(t + " have to non-negative.");
+        (t == "lambda_min" ? c.lambda_min : c.lambda_max) = v;
+      } else if (c.nose_hoover && t == "mass") {
+        c.mass = real();
+        if (c.mass <= 0.0) err("mass have to non-negative.");
+      } else if (c.nose_hoover && t == "tau") {
+        c.tau = real();
+        if (c.tau <= 0.0) err("dt have to non-negative.");
+      } else if (c.nose_hoover && t == "type") {
+        c.type = integer();
+        if (c.type <= 0) err("type have to non-negative.");
+      } else if (c.nose_hoover && t == "kb") {
+        c.kb = real();
+        if (c.kb <= 0.0) err("kb have to non-negative.");
+      } else err(std::string(c.nose_hoover ? "constraint nose_hoover" : "constraint berendsen") +
+                 ": Unknown variable or command '" + t + "'");
+    }
+  }
+
   void read_atom_data(Atom_data &a) {
     while (!cur->done()) {
       const std::string t = word();
@@ -576,6 +633,7 @@ struct Script {
       else if (t == "add_force_field" || t == "force_field") m.force_field.push_back(find<Force_field>(word()));
       else if (t == "add_neighborlist" || t == "neighborlist") m.neighborlist.push_back(find<Neighborlist>(word()));
       else if (t == "add_writer" || t == "writer") m.writer.push_back(find<Writer>(word()));
+      else if (t == "add_constraint" || t == "constraint") m.constraint.push_back(find<Thermostat>(word()));
       else if (t == "integrator_type") {
         const std::string v = word();
         if (v == "velocity_verlet") {
@@ -817,6 +875,16 @@ struct Script {
     if (m.langevin)
       check(cvr_set_langevin(ctx, m.lgv_temperature, m.lgv_friction, m.lgv_kb, m.lgv_kbt, m.lgv_rng,
                              (uint64_t)m.lgv_seed));
+    if (m.constraint.size() > 1) err("the B200 path takes one thermostat constraint");
+    for (Thermostat *t : m.constraint) {
+      // the reference reads temperature_ (0 unless temperature_process): its Berendsen
+      // factor would sit at lambda_max and its Nose-Hoover zeta would turn NaN
+      if (!a->temperature_process) err("thermostat constraints need 'atom_data temperature_process 1'");
+      if (t->nose_hoover)
+        check(cvr_set_nose_hoover(ctx, t->temperature, t->type, t->mass, t->tau, t->kb, t->dt));
+      else
+        check(cvr_set_berendsen(ctx, t->temperature, t->coupling, t->dt, t->step, t->lambda_min, t->lambda_max));
+    }
     bool any_mol = false;
     for (int32_t v : a->mol) any_mol = any_mol || v >= 0;
     check(cvr_set_state(ctx, a->n(), a->pos.data(), a->vel.data(), a->type.data(), any_mol ? a->mol.data() : nullptr));
@@ -897,6 +965,7 @@ struct Script {
       else if (auto *ek = dynamic_cast<Ewald_k *>(o)) read_ewald_k(*ek);
       else if (auto *m = dynamic_cast<Md_simulator *>(o)) read_md(*m);
       else if (auto *w = dynamic_cast<Writer *>(o)) read_writer(*w);
+      else if (auto *th = dynamic_cast<Thermostat *>(o)) read_thermostat(*th);
     }
   }
 };

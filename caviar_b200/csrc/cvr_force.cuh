@@ -675,6 +675,99 @@ __global__ void __launch_bounds__(256) k_kick(DevState<real> s, double dt, doubl
   if (KE) block_sum_store<4>(v, partials);
 }
 
+// ------------------------------------------------------------ thermostats
+// Applied after the velocity update of a velocity-Verlet step, where the
+// reference calls Constraint::apply_thermostat (md_simulator.cpp:619-627):
+//   Berendsen (constraint/berendsen.cpp:100-131): every `step` steps,
+//     v *= clamp(sqrt(1 + (dt/tau)(T0/T - 1)), lambda_min, lambda_max);
+//   Nose-Hoover (constraint/nose_hoover.cpp:122-180): zeta += dt zeta_dot with
+//     zeta_dot = (-kb n_df T / Q)(T0/T - 1) (type 1, mass Q) or (-1/tau)(T0/T - 1)
+//     (type 2), then a -= zeta v (the next step's drift and first kick use it).
+// T is the step's instantaneous temperature, 2 KE / (k_b n_df), KE with the
+// centre-of-mass motion removed as for the thermo record.
+struct ThermostatArgs {
+  int kind;  // 1 Berendsen, 2 Nose-Hoover
+  double T0, dt, tau, lambda_min, lambda_max;  // Berendsen: tau = coupling
+  int every;
+  int nh_type;
+  double nh_mass, nh_tau, nh_kb;
+  double total_mass, dof, k_b;
+  int com_removed;
+  const double *ke_part;
+  int n_ke;
+  const long long *counters;  // [0]: steps done, including this one
+  double *scal;               // [0] Berendsen factor of this step (1 = none), [1] zeta
+};
+
+__global__ void __launch_bounds__(256) k_thermostat_coef(ThermostatArgs a) {
+  __shared__ double acc[4][256];
+  double v[4] = {0, 0, 0, 0};
+  for (int b = threadIdx.x; b < a.n_ke; b += blockDim.x)
+    for (int q = 0; q < 4; ++q) v[q] += a.ke_part[(size_t)b * 4 + q];
+  for (int q = 0; q < 4; ++q) acc[q][threadIdx.x] = v[q];
+  __syncthreads();
+  for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+    if ((int)threadIdx.x < st)
+      for (int q = 0; q < 4; ++q) acc[q][threadIdx.x] += acc[q][threadIdx.x + st];
+    __syncthreads();
+  }
+  if (threadIdx.x != 0) return;
+  double ke = 0.5 * acc[0][0];
+  if (a.com_removed && a.total_mass > 0)
+    ke -= 0.5 * (acc[1][0] * acc[1][0] + acc[2][0] * acc[2][0] + acc[3][0] * acc[3][0]) / a.total_mass;
+  const double T = (a.dof > 0) ? 2.0 * ke / (a.k_b * a.dof) : 0.0;
+  const long long timestep = a.counters[0] - 1;  // the reference's current_step of this step
+  if (a.kind == 1) {
+    double lam = 1.0;
+    if (timestep % a.every == 0) {
+      lam = sqrt(1.0 + (a.dt / a.tau) * ((a.T0 / T) - 1.0));
+      if (lam < a.lambda_min) lam = a.lambda_min;
+      if (lam > a.lambda_max) lam = a.lambda_max;
+    }
+    a.scal[0] = lam;
+  } else {
+    const double g = a.dof;
+    double zd;
+    if (a.nh_type == 1)
+      zd = (-a.nh_kb * a.dof * T / a.nh_mass) * ((g * a.T0 / (a.dof * T)) - 1.0);
+    else
+      zd = (-1.0 / a.nh_tau) * ((g * a.T0 / (a.dof * T)) - 1.0);
+    a.scal[1] += a.dt * zd;  // Euler step of zeta
+  }
+}
+
+// Berendsen: v *= lambda (with KE partials of the scaled velocities for the
+// thermo record); Nose-Hoover: a -= zeta v.
+template <typename real, bool KE>
+__global__ void __launch_bounds__(256) k_thermostat_apply(DevState<real> s, int kind, const double *__restrict__ scal,
+                                                          double *__restrict__ partials) {
+  if (*s.err) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double v[4] = {0, 0, 0, 0};
+  if (i < s.n) {
+    if (kind == 1) {
+      const double lam = scal[0];
+      const double v0 = s.vx[i] * lam, v1 = s.vy[i] * lam, v2 = s.vz[i] * lam;
+      s.vx[i] = v0;
+      s.vy[i] = v1;
+      s.vz[i] = v2;
+      if (KE) {
+        const double m = s.mass[s.type[i]];
+        v[0] = m * (v0 * v0 + v1 * v1 + v2 * v2);
+        v[1] = m * v0;
+        v[2] = m * v1;
+        v[3] = m * v2;
+      }
+    } else {
+      const double z = scal[1];
+      s.ax[i] = (real)((double)s.ax[i] - z * s.vx[i]);
+      s.ay[i] = (real)((double)s.ay[i] - z * s.vy[i]);
+      s.az[i] = (real)((double)s.az[i] - z * s.vz[i]);
+    }
+  }
+  if (KE && kind == 1) block_sum_store<4>(v, partials);
+}
+
 // Sets the step graph's IF condition from the device rebuild flag: the list
 // build nodes run only on steps that need them.
 __global__ void k_set_rebuild_condition(const int *__restrict__ flag, cudaGraphConditionalHandle h) {

@@ -113,6 +113,21 @@ int cvr_set_langevin(cvr_ctx *c, double temperature, double friction, double kb,
  * (the reference is FP64 only). */
 int cvr_set_precision(cvr_ctx *ctx, int precision);
 
+/* Thermostat applied after the velocity update of each velocity-Verlet step,
+ * where the reference calls Constraint::apply_thermostat
+ * (md_simulator.cpp:619-627).  One at a time; not with the Langevin integrator.
+ * cvr_set_berendsen: `constraint berendsen` (constraint/berendsen.cpp:44-131):
+ *   every `step` steps v *= clamp(sqrt(1 + (dt/coupling)(T0/T - 1)), lambda_min, lambda_max)
+ *   (the reference's defaults: step 1, lambda_min 0.8, lambda_max 1.25).
+ * cvr_set_nose_hoover: `constraint nose_hoover` (constraint/nose_hoover.cpp:36-180):
+ *   zeta += dt zeta_dot, type 1: zeta_dot = (-kb n_df T / mass)(T0/T - 1),
+ *   type 2: zeta_dot = (-1/tau)(T0/T - 1); then a -= zeta v.
+ * T is the instantaneous temperature after the step's velocity update. */
+int cvr_set_berendsen(cvr_ctx *c, double temperature, double coupling, double dt, int step, double lambda_min,
+                      double lambda_max);
+int cvr_set_nose_hoover(cvr_ctx *c, double temperature, int type, double mass, double tau, double kb, double dt);
+int cvr_clear_thermostat(cvr_ctx *c);
+
 /* Atoms from HOST memory: pos, vel: n*3 (x,y,z per atom, = Vector<double> AoS);
  * type: n; mol: n molecule indices or NULL (-1 = none).  Atom i gets id i.
  * Replaces: Atom_data::add_atom (atom_data.cpp:487-521) / add_xyz_data_file

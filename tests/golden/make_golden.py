@@ -32,6 +32,11 @@ GPU tests never need the reference at run time).
    (T 1.2, friction 0.5, kb 1) on that fluid: final positions, velocities
    and the kinetic-energy trace.
 
+6. ref_berendsen500.npz, ref_nosehoover500.npz -- 30 velocity-Verlet steps
+   of that fluid with the reference's `constraint berendsen` (T0 1.2,
+   coupling 0.1, dt 0.005, every 2 steps) or `constraint nose_hoover` (type 1,
+   T0 1.2, mass 20, kb 1, dt 0.005), temperature_process on.
+
 Usage:  python tests/golden/make_golden.py [/path/to/reference]
 """
 import json
@@ -186,6 +191,39 @@ def langevin500(nsteps: int = 20) -> None:
                         vel=r["vel"].reshape(-1, 3)[order], ke=r["ke_trace"], nsteps=nsteps, script=LANGEVIN_SCRIPT)
 
 
+THERMOSTAT_SCRIPTS = {
+    "berendsen500": """constraint berendsen c1
+c1 set_atom_data adata
+c1 temperature 1.2
+c1 coupling 0.1
+c1 dt 0.005
+c1 step 2
+adata temperature_process 1
+sim add_constraint c1
+""",
+    "nosehoover500": """constraint nose_hoover c1
+c1 set_atom_data adata
+c1 temperature 1.2
+c1 type 1
+c1 mass 20.0
+c1 kb 1.0
+c1 dt 0.005
+adata temperature_process 1
+sim add_constraint c1
+""",
+}
+
+
+def thermostats(nsteps: int = 30) -> None:
+    s = W.fcc_lattice(5, 0.8442, 0.72, seed=7, jitter=0.05)
+    for name, extra in THERMOSTAT_SCRIPTS.items():
+        r = O.run_reference(s, "run", nsteps, extra=extra)
+        order = np.argsort(r["id"].astype(np.int64))
+        np.savez_compressed(os.path.join(HERE, f"ref_{name}.npz"), pos=r["pos"].reshape(-1, 3)[order],
+                            vel=r["vel"].reshape(-1, 3)[order], acc=r["acc"].reshape(-1, 3)[order],
+                            ke=r["ke_trace"], nsteps=nsteps, script=extra)
+
+
 def main():
     ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     g = ewald_n100(ref_root)
@@ -198,6 +236,7 @@ def main():
         json.dump(nve_lj500(), f, indent=0)
     writer_lj500()
     langevin500()
+    thermostats()
     print("golden fixtures written to", HERE)
 
 

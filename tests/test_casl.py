@@ -38,7 +38,7 @@ def script_for(s, tmp, nsteps, extra=()):
 
 def test_rejects_off_path_objects(cuda_lib, tmp_path):
     p = tmp_path / "bad.casl"
-    p.write_text("domain box dom\nconstraint berendsen c1\n")
+    p.write_text("domain box dom\nconstraint shake c1\n")
     with pytest.raises(cuda_lib.CvrError) as e:
         cuda_lib.run_casl(str(p))
     assert "not on the B200 hot path" in str(e.value) and "bad.casl:2" in str(e.value)
