@@ -66,6 +66,13 @@ struct cvr_ctx {
   bool ewk_on = false;
   double ewk_alpha = 1, ewk_ke = 1;
   int kmax[3] = {1, 1, 1};
+  int slab_axis = -1;     // Ewald k-space slab geometry: this axis' length is slab_lz (initialize.cpp:49-79)
+  double slab_lz = 1.0;
+  int dipole_mode = 0;    // 0 off, CVR_DIPOLE_REFERENCE (n_k times), CVR_DIPOLE_ONCE
+  double eps_dipole = 0;
+  double *d_dipole{};     // E[3], M[3]
+  double *d_dip_part{};
+  int dip_parts = 0;
   // integrator
   double dt = 0.001, k_b = 1.0;
   int precision = CVR_PREC_MIXED;
@@ -403,6 +410,10 @@ int upload_tables(cvr_ctx *c) {
 // k-vectors of the reference (initialize.cpp:184-222): kx, ky, kz nested over
 // [-kmax, kmax], zero skipped, f_k = exp(-k^2/(4 alpha^2)) / k^2; only the
 // first (2kx)(2ky)(2kz) are used.
+// k-space box length of axis d: the domain's, or slab_lz on the slab axis
+double klen(const cvr_ctx *c, int d) { return d == c->slab_axis ? c->slab_lz : c->L[d]; }
+double kvolume(const cvr_ctx *c) { return klen(c, 0) * klen(c, 1) * klen(c, 2); }
+
 int setup_kspace(cvr_ctx *c) {
   c->kint.clear();
   c->fk.clear();
@@ -412,7 +423,7 @@ int setup_kspace(cvr_ctx *c) {
     return CVR_OK;
   }
   const double two_pi = 6.28318530717958647692;
-  const double lx_inv = 1.0 / c->L[0], ly_inv = 1.0 / c->L[1], lz_inv = 1.0 / c->L[2];
+  const double lx_inv = 1.0 / klen(c, 0), ly_inv = 1.0 / klen(c, 1), lz_inv = 1.0 / klen(c, 2);
   const double alpha_sq = c->ewk_alpha * c->ewk_alpha;
   const double four_alpha2_inv = 1.0 / (4.0 * alpha_sq);
   const int64_t used = (int64_t)(2 * c->kmax[0]) * (2 * c->kmax[1]) * (2 * c->kmax[2]);
@@ -588,8 +599,8 @@ KArgs<real> kargs(cvr_ctx *c) {
   a.nruns = c->nruns;
   for (int d = 0; d < 3; ++d) {
     a.kmax[d] = c->kmax[d];
-    a.inv_L[d] = 1.0 / c->L[d];
-    a.two_pi_over_L[d] = (real)(6.28318530717958647692 / c->L[d]);
+    a.inv_L[d] = 1.0 / klen(c, d);
+    a.two_pi_over_L[d] = (real)(6.28318530717958647692 / klen(c, d));
   }
   a.kp = c->kp;
   a.kint = c->d_kint;
@@ -599,7 +610,7 @@ KArgs<real> kargs(cvr_ctx *c) {
   a.sk = c->d_sk;
   a.ak = (typename R2<real>::t *)c->d_ak;
   a.e_partials = c->ek_part;
-  a.four_pi_over_v = 12.56637061435917295384 / (c->L[0] * c->L[1] * c->L[2]);
+  a.four_pi_over_v = 12.56637061435917295384 / kvolume(c);
   a.charge = c->d_charge;
   a.k_e = c->ewk_ke;
   a.nchunks = c->nchunks;
@@ -649,7 +660,11 @@ void launch_thermo(cvr_ctx *c, double *out) {
   t.volume = c->L[0] * c->L[1] * c->L[2];
   t.k_b = c->k_b;
   t.n_atoms = (double)c->n;
-  t.ek_coef = 2.0 * 3.14159265358979323846 * c->ewk_ke / t.volume;  // (2 pi / V) k_e sum f_k |S_k|^2
+  t.ek_coef = 2.0 * 3.14159265358979323846 * c->ewk_ke / kvolume(c);  // (2 pi / V) k_e sum f_k |S_k|^2
+  if (c->ewk_on && c->dipole_mode && c->d_dipole) {
+    t.dipole = c->d_dipole;
+    t.dipole_coef = c->ewk_ke * 12.56637061435917295384 / kvolume(c) / (1.0 + 2.0 * c->eps_dipole);
+  }
   t.e_self = c->e_self;
   const int bcsum = c->bc[0] + c->bc[1] + c->bc[2];
   const int n_r_df = (bcsum == 0) ? 6 : (bcsum == 3 ? 3 : 6 - bcsum);  // atom_data.cpp:322-349
@@ -696,6 +711,23 @@ template <typename real>
 int forces_now(cvr_ctx *c, bool ev) {
   launch_pair<real>(c, ev);
   if (int r = launch_kspace<real>(c)) return r;
+  if (c->ewk_on && c->dipole_mode) {
+    const int nb = grid_for(c->n, 256);
+    if (!c->d_dipole) {
+      if (int r = dalloc(c, &c->d_dipole, 6)) return r;
+    }
+    if (!c->d_dip_part || c->dip_parts < nb) {
+      if (int r = dalloc(c, &c->d_dip_part, (size_t)nb * 3)) return r;
+      c->dip_parts = nb;
+    }
+    DevState<real> s = dev_state<real>(c);
+    const double coef = c->ewk_ke * 12.56637061435917295384 / kvolume(c) / (1.0 + 2.0 * c->eps_dipole);
+    k_dipole_partial<real><<<nb, 256, 0, c->stream>>>(s, c->d_charge, c->d_dip_part);
+    k_dipole_field<<<1, 256, 0, c->stream>>>(c->d_dip_part, nb, coef, c->d_dipole);
+    const double mult = c->dipole_mode == CVR_DIPOLE_ONCE ? 1.0 : (double)c->nk;
+    k_dipole_apply<real><<<nb, 256, 0, c->stream>>>(s, c->d_charge, c->d_dipole, mult);
+    c->launches += 3;
+  }
   return CVR_OK;
 }
 
@@ -1243,6 +1275,22 @@ int cvr_set_ewald_k(cvr_ctx *c, double alpha, int kx, int ky, int kz, double ke)
   c->kmax[1] = ky;
   c->kmax[2] = kz;
   c->ewk_ke = ke;
+  return refresh(c);
+}
+
+int cvr_set_ewald_k_geometry(cvr_ctx *c, int slab_axis, double slab_lz, int dipole_mode, double epsilon_dipole) {
+  if (!c) return CVR_ERR_INVALID;
+  if (slab_axis < -1 || slab_axis > 2) return fail(c, CVR_ERR_INVALID, "expected 'x' or 'y' or 'z' for axis.");
+  if (slab_axis >= 0 && !(slab_lz > 0)) return fail(c, CVR_ERR_INVALID, "slab_lz have to non-negative.");
+  if (dipole_mode != 0 && dipole_mode != CVR_DIPOLE_REFERENCE && dipole_mode != CVR_DIPOLE_ONCE)
+    return fail(c, CVR_ERR_INVALID, "unknown dipole mode");
+  if (dipole_mode && !(epsilon_dipole >= 0)) return fail(c, CVR_ERR_INVALID, "'epsilon_dipole' has to be non-negative.");
+  cudaSetDevice(c->device);
+  c->slab_axis = slab_axis;
+  c->slab_lz = slab_lz;
+  c->dipole_mode = dipole_mode;
+  c->eps_dipole = epsilon_dipole;
+  c->epoch++;
   return refresh(c);
 }
 

@@ -23,7 +23,8 @@
 //   force_field electrostatic_ewald_r <name>  cutoff, alpha, k_electrostatic, lambda i j v,
 //                              set_neighborlist, set_atom_data (electrostatic_ewald_r.cpp:38-107)
 //   force_field electrostatic_ewald_k <name>  alpha, k_max, kx_max, ky_max, kz_max,
-//                              k_electrostatic, set_atom_data, set_domain (electrostatic_ewald_k.cpp:48-143)
+//                              k_electrostatic, slab_normal_axis, slab_lz|slab_thickness,
+//                              epsilon_dipole, set_atom_data, set_domain (electrostatic_ewald_k.cpp:48-143)
 //   md_simulator basic <name>  set_atom_data, add_force_field|force_field,
 //                              add_neighborlist|neighborlist, add_writer|writer,
 //                              integrator_type velocity_verlet|velocity_verlet_langevin,
@@ -206,6 +207,10 @@ struct Ewald_r : Force_field {
 struct Ewald_k : Force_field {
   double alpha = 1.0, k_e = 1.0;
   int kmax[3] = {1, 1, 1};
+  int slab_axis = -1;  // slab_normal_axis (default z once slab_lz is given, electrostatic_ewald_k.cpp:44-45)
+  double slab_lz = 1.0;
+  bool slab = false, dipole = false, dipole_once = false;
+  double eps_dipole = 0.0;
 };
 
 struct Writer : Object {
@@ -622,7 +627,24 @@ struct Script {
       else if (t == "kx_max") f.kmax[0] = integer();
       else if (t == "ky_max") f.kmax[1] = integer();
       else if (t == "kz_max") f.kmax[2] = integer();
-      else err("force_field electrostatic_ewald_k: '" + t + "' is not supported on the B200 path");
+      else if (t == "slab_normal_axis") {
+        const std::string v = word();
+        f.slab = true;
+        if (v == "x") f.slab_axis = 0;
+        else if (v == "y") f.slab_axis = 1;
+        else if (v == "z") f.slab_axis = 2;
+        else err("expected 'x' or 'y' or 'z' for axis.");
+      } else if (t == "slab_lz" || t == "slab_thickness") {
+        f.slab = true;
+        f.slab_lz = real();
+        if (f.slab_lz < 0.0) err("slab_lz have to non-negative.");
+      } else if (t == "epsilon_dipole") {
+        f.eps_dipole = real();
+        if (f.eps_dipole < 0) err("'epsilon_dipole' has to be non-negative.");
+        f.dipole = true;
+      } else if (t == "dipole_once") {
+        f.dipole_once = true;  // extension: the textbook term once, not once per k-vector
+      } else err("force_field electrostatic_ewald_k: '" + t + "' is not supported on the B200 path");
     }
   }
 
@@ -869,6 +891,10 @@ struct Script {
         check(cvr_set_ewald_r(ctx, er->alpha, er->k_e, er->lambda_on ? lam.data() : nullptr, -1.0));
       } else if (auto *ek = dynamic_cast<Ewald_k *>(f)) {
         check(cvr_set_ewald_k(ctx, ek->alpha, ek->kmax[0], ek->kmax[1], ek->kmax[2], ek->k_e));
+        if (ek->slab || ek->dipole)
+          check(cvr_set_ewald_k_geometry(ctx, ek->slab ? (ek->slab_axis < 0 ? 2 : ek->slab_axis) : -1, ek->slab_lz,
+                                         ek->dipole ? (ek->dipole_once ? CVR_DIPOLE_ONCE : CVR_DIPOLE_REFERENCE) : 0,
+                                         ek->eps_dipole));
       }
     }
     check(cvr_set_integrator(ctx, m.dt, a->k_b > 0 ? a->k_b : 1.0));

@@ -768,6 +768,63 @@ __global__ void __launch_bounds__(256) k_thermostat_apply(DevState<real> s, int 
   if (KE && kind == 1) block_sum_store<4>(v, partials);
 }
 
+// ---------------------------------------------------- Ewald dipole term
+// The surrounding-medium term of Electrostatic_ewald_k (initialize.cpp:98-115,
+// electrostatic_ewald_k.cpp:219-223): M = sum_j q_j r_j over the wrapped
+// positions, E = -M k_e 4 pi / (V (1 + 2 eps')), F_i += mult q_i E.  The
+// reference adds the term inside its k-vector loop, once per k-vector
+// (mult = n_k); mult = 1 gives the textbook term.
+template <typename real>
+__global__ void __launch_bounds__(256) k_dipole_partial(DevState<real> s, const double *__restrict__ charge,
+                                                        double *__restrict__ partials) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double v[3] = {0, 0, 0};
+  if (i < s.n) {
+    const double q = charge[s.type[i]];
+    const double p[3] = {s.x[i], s.y[i], s.z[i]};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      double x = p[d];
+      if (s.box.bc[d] == 1) x -= s.box.L[d] * floor((x - s.box.lo[d]) / s.box.L[d]);
+      v[d] = q * x;
+    }
+  }
+  block_sum_store<3>(v, partials);
+}
+
+// One block: M from the partials, E = -coef M into dip[0..2], M into dip[3..5].
+__global__ void __launch_bounds__(256) k_dipole_field(const double *__restrict__ partials, int nparts, double coef,
+                                                      double *__restrict__ dip) {
+  __shared__ double acc[3][256];
+  double v[3] = {0, 0, 0};
+  for (int b = threadIdx.x; b < nparts; b += blockDim.x)
+    for (int q = 0; q < 3; ++q) v[q] += partials[(size_t)b * 3 + q];
+  for (int q = 0; q < 3; ++q) acc[q][threadIdx.x] = v[q];
+  __syncthreads();
+  for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+    if ((int)threadIdx.x < st)
+      for (int q = 0; q < 3; ++q) acc[q][threadIdx.x] += acc[q][threadIdx.x + st];
+    __syncthreads();
+  }
+  if (threadIdx.x < 3) {
+    dip[3 + threadIdx.x] = acc[threadIdx.x][0];
+    dip[threadIdx.x] = -acc[threadIdx.x][0] * coef;
+  }
+}
+
+template <typename real>
+__global__ void __launch_bounds__(256) k_dipole_apply(DevState<real> s, const double *__restrict__ charge,
+                                                      const double *__restrict__ dip, double mult) {
+  if (*s.err) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= s.n) return;
+  const int t = s.type[i];
+  const double f = mult * charge[t] * s.mass_inv[t];
+  s.ax[i] = (real)((double)s.ax[i] + f * dip[0]);
+  s.ay[i] = (real)((double)s.ay[i] + f * dip[1]);
+  s.az[i] = (real)((double)s.az[i] + f * dip[2]);
+}
+
 // Sets the step graph's IF condition from the device rebuild flag: the list
 // build nodes run only on steps that need them.
 __global__ void k_set_rebuild_condition(const int *__restrict__ flag, cudaGraphConditionalHandle h) {
@@ -827,6 +884,8 @@ struct ThermoArgs {
   const double *ek_part;
   int n_ek;
   double total_mass, dof, volume, k_b, n_atoms, ek_coef, e_self;
+  const double *dipole;  // E, M of the dipole term (nullable)
+  double dipole_coef;    // k_e 4 pi / (V (1 + 2 eps')): energy 0.5 coef |M|^2 (energy.cpp:52-56)
   int com_removed;
   const int *n_builds;
   long long *counters;  // [0] steps done, [1] next thermo record
@@ -865,6 +924,10 @@ __global__ void __launch_bounds__(256) k_thermo(ThermoArgs a) {
     out[3] = acc[4][0];
     out[4] = acc[5][0];
     out[5] = a.ek_coef * acc[7][0];
+    if (a.dipole) {
+      const double *M = a.dipole + 3;
+      out[5] += 0.5 * a.dipole_coef * (M[0] * M[0] + M[1] * M[1] + M[2] * M[2]);
+    }
     out[6] = a.e_self;
     out[7] = vir;
     out[8] = a.n_atoms * a.k_b * temp / a.volume + vir / (3.0 * a.volume);

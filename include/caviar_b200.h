@@ -90,6 +90,19 @@ int cvr_set_ewald_r(cvr_ctx *ctx, double alpha, double k_electrostatic, const do
  *           calculate_potential_k_coef_cmplx (:117-146), calculate_acceleration (:161-294). */
 int cvr_set_ewald_k(cvr_ctx *ctx, double alpha, int kx_max, int ky_max, int kz_max, double k_electrostatic);
 
+/* Electrostatic_ewald_k geometry keywords (electrostatic_ewald_k.cpp:87-126,
+ * initialize.cpp:49-115): slab_axis 0/1/2 (slab_normal_axis x/y/z, -1 off)
+ * replaces that axis' length by slab_lz in the k-vectors and the volume;
+ * dipole_mode != 0 (epsilon_dipole set) adds the surrounding-medium term
+ * F_i += q_i E, E = -(sum_j q_j r_j) k_e 4 pi / (V (1 + 2 epsilon_dipole)),
+ * and 0.5 (k_e 4 pi / (V (1 + 2 eps))) |M|^2 to the k-space energy.
+ * CVR_DIPOLE_REFERENCE adds the force term once per k-vector, as the
+ * reference does (inside its k loop, electrostatic_ewald_k.cpp:197-223);
+ * CVR_DIPOLE_ONCE adds it once. */
+#define CVR_DIPOLE_REFERENCE 1
+#define CVR_DIPOLE_ONCE 2
+int cvr_set_ewald_k_geometry(cvr_ctx *ctx, int slab_axis, double slab_lz, int dipole_mode, double epsilon_dipole);
+
 /* md_simulator basic: dt; atom_data k_b.
  * Replaces: Md_simulator::read dt / integrator_type velocity_verlet (md_simulator.cpp:58-233). */
 int cvr_set_integrator(cvr_ctx *ctx, double dt, double k_b);

@@ -37,6 +37,11 @@ GPU tests never need the reference at run time).
    coupling 0.1, dt 0.005, every 2 steps) or `constraint nose_hoover` (type 1,
    T0 1.2, mass 20, kb 1, dt 0.005), temperature_process on.
 
+7. ref_ewald_slab300.npz -- 300 ions (+-1) in a 10^3 box, LJ rc 2.5, Ewald
+   alpha 0.8, k_max 4, list cutoff 4 (coef 1.03): the reference's forces with
+   (a) z non-periodic, `slab_normal_axis z`, `slab_lz 30`, `epsilon_dipole 0`
+   and (b) all periodic with `epsilon_dipole 1`, and (c) a 10-step run of (a).
+
 Usage:  python tests/golden/make_golden.py [/path/to/reference]
 """
 import json
@@ -224,6 +229,34 @@ def thermostats(nsteps: int = 30) -> None:
                             ke=r["ke_trace"], nsteps=nsteps, script=extra)
 
 
+SLAB_SCRIPTS = {
+    "slab": "f_ek slab_normal_axis z\nf_ek slab_lz 30.0\nf_ek epsilon_dipole 0.0\n",
+    "dipole": "f_ek epsilon_dipole 1.0\n",
+}
+
+
+def slab_system(periodic_z: bool):
+    s = W.random_ions(300, 10.0, 21, rc=4.0, coef=1.03, kmax=4, alpha=0.8)
+    s.bc = (1, 1, 1 if periodic_z else 0)
+    return s
+
+
+def ewald_slab() -> None:
+    out = {}
+    for name, extra in SLAB_SCRIPTS.items():
+        s = slab_system(name != "slab")
+        r = O.run_reference(s, "forces", extra=extra)
+        order = np.argsort(r["id"].astype(np.int64))
+        out[f"{name}_acc"] = r["acc"].reshape(-1, 3)[order]
+        out[f"{name}_script"] = extra
+    s = slab_system(False)
+    r = O.run_reference(s, "run", 10, extra=SLAB_SCRIPTS["slab"])
+    order = np.argsort(r["id"].astype(np.int64))
+    out["slab_run_pos"] = r["pos"].reshape(-1, 3)[order]
+    out["slab_run_vel"] = r["vel"].reshape(-1, 3)[order]
+    np.savez_compressed(os.path.join(HERE, "ref_ewald_slab300.npz"), **out)
+
+
 def main():
     ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     g = ewald_n100(ref_root)
@@ -237,6 +270,7 @@ def main():
     writer_lj500()
     langevin500()
     thermostats()
+    ewald_slab()
     print("golden fixtures written to", HERE)
 
 
