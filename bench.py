@@ -180,6 +180,27 @@ def force_error(abi, s):
     return float(np.linalg.norm(d) / np.linalg.norm(nb)), float(d.max() / np.sqrt(np.mean(nb ** 2)))
 
 
+def ions_line(abi, W, torch, steps: int, warmup: int, device: int = 0):
+    """8000 ions (LJ + Ewald r + k), both precisions: K graph-launched steps
+    timed with CUDA events, then K more steps with per-kernel events (stream
+    launches) for the k-space / pair breakdown."""
+    s_ion = W.config_ions_8000(seed=2)
+    ion = {}
+    for nm, p in (("mixed", abi.PREC_MIXED), ("fp64", abi.PREC_FP64)):
+        si = abi.Simulation(s_ion, precision=p, device=device)
+        msi = time_run(si, torch, steps, warmup)
+        si.set_kernel_timing(True)
+        msk = time_run(si, torch, steps, 0)
+        kms, kn = si.kernel_time(abi.KT_KSPACE)
+        pms, pn = si.kernel_time(abi.KT_PAIR)
+        bms, _ = si.kernel_time(abi.KT_BUILD)
+        ion[nm] = {"value": s_ion.n * steps / (msi / 1e3), "ms_per_step": msi / steps,
+                   "kernel_window_ms_per_step": msk / steps, "kspace_ms_per_step": kms / max(kn, 1),
+                   "pair_ms_per_step": pms / max(pn, 1), "build_ms_per_step": bms / steps}
+        si.close()
+    return ion
+
+
 def replica_line(abi, W, torch, nsteps: int):
     """1024 replicas (64-2048 atoms, rho* 0.8, half charged +-1, alpha 0.35,
     k_max 6, T 0.7-1.5) advanced nsteps steps in one graph launch; device time
@@ -295,17 +316,7 @@ def gpu_arm(args):
         ms64 = time_run(sim64, torch, steps, warmup)
         sec["lj_1m_fp64"] = {"value": n * steps / (ms64 / 1e3), "ms_per_step": ms64 / steps}
         sim64.close()
-        s_ion = W.config_ions_8000(seed=2)
-        ion = {}
-        for nm, p in (("mixed", abi.PREC_MIXED), ("fp64", abi.PREC_FP64)):
-            si = abi.Simulation(s_ion, precision=p, device=local)
-            si.set_kernel_timing(True)
-            msi = time_run(si, torch, steps, warmup)
-            kms, kn = si.kernel_time(abi.KT_KSPACE)
-            pms, pn = si.kernel_time(abi.KT_PAIR)
-            ion[nm] = {"value": s_ion.n * steps / (msi / 1e3), "ms_per_step": msi / steps,
-                       "kspace_ms_per_step": kms / max(kn, 1), "pair_ms_per_step": pms / max(pn, 1)}
-            si.close()
+        ion = ions_line(abi, W, torch, steps, warmup, local)
         sec["ions_8k_mixed"] = ion["mixed"]
         sec["ions_8k_fp64"] = ion["fp64"]
         sec["mixed_over_fp64"] = {"lj_1m": value / world / sec["lj_1m_fp64"]["value"],
@@ -433,7 +444,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--replica-steps", type=int, default=1000)
     ap.add_argument("--adjoint-steps", type=int, default=500)
-    ap.add_argument("--only", default="all", choices=["all", "replicas", "adjoint"],
+    ap.add_argument("--only", default="all", choices=["all", "replicas", "adjoint", "ions"],
                     help="run one secondary workload alone and print its JSON (profiling runs)")
     args = ap.parse_args()
     if args.impl == "reference":
@@ -445,8 +456,12 @@ def main():
         B.build()
         from caviar_b200 import _abi as abi
         from caviar_b200 import workloads as W
-        res = replica_line(abi, W, torch, args.replica_steps) if args.only == "replicas" else adjoint_line(abi, W, torch,
-                                                                                                  args.adjoint_steps)
+        if args.only == "replicas":
+            res = replica_line(abi, W, torch, args.replica_steps)
+        elif args.only == "ions":
+            res = ions_line(abi, W, torch, args.steps, max(3, args.warmup))
+        else:
+            res = adjoint_line(abi, W, torch, args.adjoint_steps)
         print(json.dumps({"only": args.only, **res}), flush=True)
     else:
         gpu_arm(args)
