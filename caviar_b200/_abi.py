@@ -27,7 +27,8 @@ KT_PAIR, KT_KSPACE, KT_INTEGRATE, KT_BUILD = 0, 1, 2, 3
 # Every symbol declared in include/caviar_b200.h.
 EXPORTED = ["cvr_create", "cvr_destroy", "cvr_set_neighborlist", "cvr_set_lj", "cvr_set_ewald_r", "cvr_set_ewald_k",
             "cvr_set_integrator", "cvr_set_langevin", "cvr_set_berendsen", "cvr_set_nose_hoover",
-            "cvr_clear_thermostat", "cvr_set_ewald_k_geometry", "cvr_set_precision", "cvr_set_state", "cvr_build_neighbors", "cvr_compute_forces",
+            "cvr_clear_thermostat", "cvr_set_ewald_k_geometry",
+            "cvr_set_ewald_slab_correction", "cvr_set_precision", "cvr_set_state", "cvr_build_neighbors", "cvr_compute_forces",
             "cvr_run", "cvr_get_state", "cvr_get_pairs", "cvr_get_sk", "cvr_get_scalars", "cvr_last_error",
             "cvr_launch_count", "cvr_get_stream", "cvr_get_info", "cvr_set_kernel_timing", "cvr_kernel_time",
             "cvr_structure_factor_noalloc", "cvr_casl_run_file", "cvr_batch_create", "cvr_batch_destroy",
@@ -74,6 +75,8 @@ def load(path: str = LIB_PATH):
                                       ctypes.c_double, ctypes.c_double]
     L.cvr_clear_thermostat.argtypes = [vp]
     L.cvr_set_ewald_k_geometry.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_double]
+    L.cvr_set_ewald_slab_correction.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int,
+                                                ctypes.c_double]
     L.cvr_set_state.argtypes = [vp, ctypes.c_int64, vp, vp, vp, vp]
     L.cvr_build_neighbors.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     L.cvr_compute_forces.argtypes = [vp, vp, _dp]
@@ -185,6 +188,10 @@ class Simulation:
                              epsilon_dipole: float = 0.0):
         """Electrostatic_ewald_k slab_normal_axis / slab_lz / epsilon_dipole."""
         self._check(self.L.cvr_set_ewald_k_geometry(self.h, slab_axis, slab_lz, dipole_mode, epsilon_dipole))
+
+    def set_ewald_slab_correction(self, slab_axis: int, lz: float, kx_max: int, ky_max: int, k_e: float = 1.0):
+        """force_field electrostatic_ewald_slab_correction."""
+        self._check(self.L.cvr_set_ewald_slab_correction(self.h, slab_axis, lz, kx_max, ky_max, k_e))
 
     def set_berendsen(self, temperature: float, coupling: float, dt: float, step: int = 1, lambda_min: float = 0.8,
                       lambda_max: float = 1.25):

@@ -70,6 +70,12 @@ struct cvr_ctx {
   double slab_lz = 1.0;
   int dipole_mode = 0;    // 0 off, CVR_DIPOLE_REFERENCE (n_k times), CVR_DIPOLE_ONCE
   double eps_dipole = 0;
+  // force_field electrostatic_ewald_slab_correction
+  bool sc_on = false;
+  int sc_axis = 2, sc_kx = 1, sc_ky = 1;
+  double sc_lz = 1.0, sc_ke = 1.0;
+  double *d_sc_partial{}, *d_sc_chi{}, *d_sc_state{};
+  int sc_parts = 0;
   double *d_dipole{};     // E[3], M[3]
   double *d_dip_part{};
   int dip_parts = 0;
@@ -661,6 +667,7 @@ void launch_thermo(cvr_ctx *c, double *out) {
   t.k_b = c->k_b;
   t.n_atoms = (double)c->n;
   t.ek_coef = 2.0 * 3.14159265358979323846 * c->ewk_ke / kvolume(c);  // (2 pi / V) k_e sum f_k |S_k|^2
+  if (c->sc_on && c->d_sc_state) t.slab_e = c->d_sc_state + 1;
   if (c->ewk_on && c->dipole_mode && c->d_dipole) {
     t.dipole = c->d_dipole;
     t.dipole_coef = c->ewk_ke * 12.56637061435917295384 / kvolume(c) / (1.0 + 2.0 * c->eps_dipole);
@@ -707,10 +714,69 @@ int read_flags(cvr_ctx *c, int out[4]) {
   return CVR_OK;
 }
 
+SlabArgs slab_args(cvr_ctx *c) {
+  SlabArgs a{};
+  a.axis = c->sc_axis;
+  a.kx = c->sc_kx;
+  a.ky = c->sc_ky;
+  a.nv = 4 * c->sc_kx + 4 * c->sc_ky + 8 * c->sc_kx * c->sc_ky + 1;
+  a.nch = grid_for(c->n, SLAB_CH);
+  // initialize.cpp:33-76: in-plane lengths, slab_sum_e_coef, dipole coefficient
+  const int lxa = c->sc_axis == 0 ? 1 : (c->sc_axis == 1 ? 0 : 0);
+  const int lya = c->sc_axis == 0 ? 2 : (c->sc_axis == 1 ? 2 : 1);
+  a.lx = c->L[lxa];
+  a.ly = c->L[lya];
+  a.lz = c->sc_lz;
+  a.ke = c->sc_ke;
+  const double four_pi = 12.56637061435917295384, two_pi = 6.28318530717958647692;
+  a.sum_e_coef = -four_pi / (a.lx * a.ly);
+  a.dipole_coef = c->sc_ke * four_pi / (a.lx * a.ly * a.lz);
+  // make_slab_k_vectors (initialize.cpp:96-143)
+  for (int i = 0; i < a.kx; ++i) {
+    a.kxv[i] = two_pi * (i + 1) / a.lx;
+    a.kxc[i] = 1.0 / (a.kxv[i] * (std::exp(a.kxv[i] * a.lz) - 1.0));
+  }
+  for (int j = 0; j < a.ky; ++j) {
+    a.kyv[j] = two_pi * (j + 1) / a.ly;
+    a.kyc[j] = 1.0 / (a.kyv[j] * (std::exp(a.kyv[j] * a.lz) - 1.0));
+  }
+  for (int i = 0; i < a.kx; ++i)
+    for (int j = 0; j < a.ky; ++j) {
+      const double kp = std::sqrt(a.kxv[i] * a.kxv[i] + a.kyv[j] * a.kyv[j]);
+      a.kpv[i * a.ky + j] = kp;
+      a.kpc[i * a.ky + j] = 1.0 / (kp * (std::exp(kp * a.lz) - 1.0));
+    }
+  a.charge = c->d_charge;
+  a.partial = c->d_sc_partial;
+  a.chi = c->d_sc_chi;
+  a.state = c->d_sc_state;
+  return a;
+}
+
+template <typename real>
+int launch_slab(cvr_ctx *c) {
+  SlabArgs a = slab_args(c);
+  if (!c->d_sc_partial || c->sc_parts < a.nch * a.nv) {
+    if (int r = dalloc(c, &c->d_sc_partial, (size_t)a.nch * a.nv)) return r;
+    if (int r = dalloc(c, &c->d_sc_chi, (size_t)a.nv)) return r;
+    c->sc_parts = a.nch * a.nv;
+    a = slab_args(c);
+  }
+  DevState<real> s = dev_state<real>(c);
+  k_slab_chi_partial<real><<<a.nch, 128, 0, c->stream>>>(s, a);
+  k_slab_chi_reduce<<<1, 256, 0, c->stream>>>(a);
+  k_slab_field<real><<<grid_for(c->n, 128), 128, 0, c->stream>>>(s, a);
+  k_slab_store_moment<<<1, 1, 0, c->stream>>>(a);
+  c->launches += 4;
+  return CVR_OK;
+}
+
 template <typename real>
 int forces_now(cvr_ctx *c, bool ev) {
   launch_pair<real>(c, ev);
   if (int r = launch_kspace<real>(c)) return r;
+  if (c->sc_on)
+    if (int r = launch_slab<real>(c)) return r;
   if (c->ewk_on && c->dipole_mode) {
     const int nb = grid_for(c->n, 256);
     if (!c->d_dipole) {
@@ -993,7 +1059,8 @@ int run_impl(cvr_ctx *c, int64_t nsteps, int64_t every, double *thermo) {
     if (graphs) {
       // kernel nodes executed: per step kick_drift + condition + tail; 8 per rebuild
       const int tail = 1 + (c->lj_on || c->ewr_on ? 1 : 0) + ((c->ewk_on && c->nk > 0) ? (c->kf_slices > 1 ? 4 : 3) : 0) +
-                       ((c->tstat.kind && c->integrator == 0) ? 2 : 0);
+                       ((c->tstat.kind && c->integrator == 0) ? 2 : 0) + (c->sc_on ? 4 : 0) +
+                       ((c->ewk_on && c->dipole_mode) ? 3 : 0);
       c->launches = launches0 + nsteps * (2 + tail) + nrec + 8 * (int64_t)(f[3] - f0[3]);
     }
     if (f[1] & ERR_NAN) return fail(c, CVR_ERR_NAN, "NaN acceleration");
@@ -1292,6 +1359,34 @@ int cvr_set_ewald_k_geometry(cvr_ctx *c, int slab_axis, double slab_lz, int dipo
   c->eps_dipole = epsilon_dipole;
   c->epoch++;
   return refresh(c);
+}
+
+int cvr_set_ewald_slab_correction(cvr_ctx *c, int slab_axis, double lz, int kx_max, int ky_max, double k_e) {
+  if (!c) return CVR_ERR_INVALID;
+  if (slab_axis < 0) {
+    c->sc_on = false;
+    c->epoch++;
+    return CVR_OK;
+  }
+  if (slab_axis > 2) return fail(c, CVR_ERR_INVALID, "expected 'x', 'y' or 'z'.");
+  if (kx_max < 0 || ky_max < 0) return fail(c, CVR_ERR_INVALID, "'k_max' have to non-negative.");
+  if (kx_max < 1 || ky_max < 1 || kx_max > SLAB_KMAX || ky_max > SLAB_KMAX)
+    return fail(c, CVR_ERR_INVALID, "slab correction: kx_max and ky_max in [1, 8] on the B200 path");
+  if (!(lz >= 0)) return fail(c, CVR_ERR_INVALID, "'lz' has to be non-negative.");
+  if (!(k_e >= 0)) return fail(c, CVR_ERR_INVALID, "k_electrostatic has to be non-negative.");
+  if (c->L[slab_axis] > lz) return fail(c, CVR_ERR_GEOMETRY, "expected 'hz > lz' for slab geometry");
+  cudaSetDevice(c->device);
+  if (!c->d_sc_state) {
+    if (int r = dalloc(c, &c->d_sc_state, 2)) return r;  // zero: no moment before the first call
+  }
+  c->sc_on = true;
+  c->sc_axis = slab_axis;
+  c->sc_lz = lz;
+  c->sc_kx = kx_max;
+  c->sc_ky = ky_max;
+  c->sc_ke = k_e;
+  c->epoch++;
+  return CVR_OK;
 }
 
 int cvr_set_integrator(cvr_ctx *c, double dt, double k_b) {

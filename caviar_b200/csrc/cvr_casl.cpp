@@ -25,6 +25,9 @@
 //   force_field electrostatic_ewald_k <name>  alpha, k_max, kx_max, ky_max, kz_max,
 //                              k_electrostatic, slab_normal_axis, slab_lz|slab_thickness,
 //                              epsilon_dipole, set_atom_data, set_domain (electrostatic_ewald_k.cpp:48-143)
+//   force_field electrostatic_ewald_slab_correction <name>  slab_normal_axis, lz, k_max,
+//                              kx_max, ky_max, k_electrostatic, set_atom_data, set_domain
+//                              (electrostatic_ewald_slab_correction.cpp:44-111)
 //   md_simulator basic <name>  set_atom_data, add_force_field|force_field,
 //                              add_neighborlist|neighborlist, add_writer|writer,
 //                              integrator_type velocity_verlet|velocity_verlet_langevin,
@@ -240,6 +243,12 @@ struct Thermostat : Object {
   double mass = -1, tau = -1, kb = 1.0;
 };
 
+// force_field electrostatic_ewald_slab_correction (electrostatic_ewald_slab_correction.cpp:28-111)
+struct Slab_correction : Force_field {
+  int axis = 2, kx = 1, ky = 1;
+  double lz = 1.0, k_e = 1.0;
+};
+
 struct Md_simulator : Object {
   Atom_data *atom_data = nullptr;
   std::vector<Thermostat *> constraint;
@@ -306,6 +315,7 @@ struct Script {
     else if (cls == "force_field" && type == "lj") o.reset(new Lj);
     else if (cls == "force_field" && type == "electrostatic_ewald_r") o.reset(new Ewald_r);
     else if (cls == "force_field" && type == "electrostatic_ewald_k") o.reset(new Ewald_k);
+    else if (cls == "force_field" && type == "electrostatic_ewald_slab_correction") o.reset(new Slab_correction);
     else if (cls == "md_simulator" && type == "basic") o.reset(new Md_simulator);
     else if (cls == "writer" && type == "atom_data") o.reset(new Writer);
     else if (cls == "constraint" && (type == "berendsen" || type == "nose_hoover")) {
@@ -648,6 +658,34 @@ struct Script {
     }
   }
 
+  void read_slab(Slab_correction &f) {
+    while (!cur->done()) {
+      const std::string t = word();
+      bool h;
+      common_ff(f, t, h);
+      if (h) continue;
+      if (t == "k_max") {
+        const int k = integer();
+        if (k < 0) err("'k_max' have to non-negative.");
+        f.kx = f.ky = k;
+      } else if (t == "kx_max") f.kx = integer();
+      else if (t == "ky_max") f.ky = integer();
+      else if (t == "lz") {
+        f.lz = real();
+        if (f.lz < 0) err("'lz' has to be non-negative.");
+      } else if (t == "slab_normal_axis") {
+        const std::string v = word();
+        if (v == "x") f.axis = 0;
+        else if (v == "y") f.axis = 1;
+        else if (v == "z") f.axis = 2;
+        else err("expected 'x', 'y' or 'z'.");
+      } else if (t == "k_electrostatic") {
+        f.k_e = real();
+        if (f.k_e < 0) err("k_electrostatic has to be non-negative.");
+      } else err("force_field electrostatic_ewald_slab_correction: '" + t + "' is not supported on the B200 path");
+    }
+  }
+
   void read_md(Md_simulator &m) {
     while (!cur->done()) {
       const std::string t = word();
@@ -889,6 +927,8 @@ struct Script {
         for (int i = 0; i < T; ++i)
           for (int j = 0; j < T; ++j) lam[i * T + j] = elem(er->lambda, i, j, 1.0);
         check(cvr_set_ewald_r(ctx, er->alpha, er->k_e, er->lambda_on ? lam.data() : nullptr, -1.0));
+      } else if (auto *sc = dynamic_cast<Slab_correction *>(f)) {
+        check(cvr_set_ewald_slab_correction(ctx, sc->axis, sc->lz, sc->kx, sc->ky, sc->k_e));
       } else if (auto *ek = dynamic_cast<Ewald_k *>(f)) {
         check(cvr_set_ewald_k(ctx, ek->alpha, ek->kmax[0], ek->kmax[1], ek->kmax[2], ek->k_e));
         if (ek->slab || ek->dipole)
@@ -989,6 +1029,7 @@ struct Script {
       else if (auto *lj = dynamic_cast<Lj *>(o)) read_lj(*lj);
       else if (auto *er = dynamic_cast<Ewald_r *>(o)) read_ewald_r(*er);
       else if (auto *ek = dynamic_cast<Ewald_k *>(o)) read_ewald_k(*ek);
+      else if (auto *sc = dynamic_cast<Slab_correction *>(o)) read_slab(*sc);
       else if (auto *m = dynamic_cast<Md_simulator *>(o)) read_md(*m);
       else if (auto *w = dynamic_cast<Writer *>(o)) read_writer(*w);
       else if (auto *th = dynamic_cast<Thermostat *>(o)) read_thermostat(*th);

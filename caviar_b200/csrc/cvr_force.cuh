@@ -825,6 +825,187 @@ __global__ void __launch_bounds__(256) k_dipole_apply(DevState<real> s, const do
   s.az[i] = (real)((double)s.az[i] + f * dip[2]);
 }
 
+// ------------------------------------------- Ewald slab correction (ELC)
+// force_field electrostatic_ewald_slab_correction (electrostatic_ewald_slab_
+// correction/initialize.cpp:33-255, field.cpp:27-144, energy.cpp:33-111), FP64.
+// Slab-local coordinates (x, y in the periodic plane, z along the normal
+// axis); wave numbers kx_i = 2 pi (i+1)/lx, ky_j = 2 pi (j+1)/ly,
+// kp_ij = |(kx_i, ky_j)| with weights 1/(k (exp(k lz) - 1)); per k the charge
+// sums chi of sinh/cosh(k z) times sin/cos of the in-plane phases; the field
+// on atom i is their derivative combination, times 2 (-4 pi/(lx ly)) k_e,
+// plus the dipole term -M k_e 4 pi/(lx ly lz) along the normal axis, where M
+// is the normal dipole moment of the PREVIOUS force call (the reference
+// computes the field before it updates its stored moment).
+constexpr int SLAB_KMAX = 8;
+constexpr int SLAB_CH = 32;  // atoms per chunk of the chi sums
+
+struct SlabArgs {
+  int axis, kx, ky, nv, nch;
+  double lx, ly, lz, ke, sum_e_coef, dipole_coef;
+  double kxv[SLAB_KMAX], kyv[SLAB_KMAX], kxc[SLAB_KMAX], kyc[SLAB_KMAX];
+  double kpv[SLAB_KMAX * SLAB_KMAX], kpc[SLAB_KMAX * SLAB_KMAX];
+  const double *charge;
+  double *partial;  // [chunk][nv]
+  double *chi;      // [nv]: x-terms 4 kx, y-terms 4 ky, p-terms 8 kx ky, then M
+  double *state;    // [0] M of the previous call, [1] this call's slab energy
+};
+
+template <typename real>
+__device__ __forceinline__ void slab_local(const DevState<real> &s, int axis, int i, double p[3]) {
+  const double g[3] = {s.x[i], s.y[i], s.z[i]};
+  // give_slab_local_coordinates (electrostatic_ewald_slab_correction.h)
+  const int lx = axis == 0 ? 1 : (axis == 1 ? 2 : 0), ly = axis == 0 ? 2 : (axis == 1 ? 0 : 1);
+  p[0] = g[lx];
+  p[1] = g[ly];
+  p[2] = g[axis];
+}
+
+// chi partial sums of one chunk: block = chunk, threads over the nv values.
+template <typename real>
+__global__ void __launch_bounds__(128) k_slab_chi_partial(DevState<real> s, SlabArgs a) {
+  const int a0 = blockIdx.x * SLAB_CH, a1 = min(s.n, a0 + SLAB_CH);
+  const int KX = a.kx, KY = a.ky;
+  for (int v = threadIdx.x; v < a.nv; v += blockDim.x) {
+    double acc = 0.0;
+    for (int i = a0; i < a1; ++i) {
+      const double q = a.charge[s.type[i]];
+      double p[3];
+      slab_local(s, a.axis, i, p);
+      double t;
+      if (v < 4 * KX) {
+        const int ix = v >> 2, c = v & 3;
+        const double kx = a.kxv[ix];
+        const double h = (c >> 1) ? cosh(kx * p[2]) : sinh(kx * p[2]);
+        const double f = (c & 1) ? cos(kx * p[0]) : sin(kx * p[0]);
+        t = q * h * f;
+      } else if (v < 4 * KX + 4 * KY) {
+        const int iy = (v - 4 * KX) >> 2, c = (v - 4 * KX) & 3;
+        const double ky = a.kyv[iy];
+        const double h = (c >> 1) ? cosh(ky * p[2]) : sinh(ky * p[2]);
+        const double f = (c & 1) ? cos(ky * p[1]) : sin(ky * p[1]);
+        t = q * h * f;
+      } else if (v < 4 * KX + 4 * KY + 8 * KX * KY) {
+        const int w = v - 4 * KX - 4 * KY, ip = w >> 3, c = w & 7;  // c = 4 h + 2 a + b
+        const int ix = ip / KY, iy = ip % KY;
+        const double kp = a.kpv[ip];
+        const double h = (c >> 2) ? cosh(kp * p[2]) : sinh(kp * p[2]);
+        const double fx = ((c >> 1) & 1) ? cos(a.kxv[ix] * p[0]) : sin(a.kxv[ix] * p[0]);
+        const double fy = (c & 1) ? cos(a.kyv[iy] * p[1]) : sin(a.kyv[iy] * p[1]);
+        t = q * h * fx * fy;
+      } else {
+        t = q * p[2];  // normal dipole moment
+      }
+      acc += t;
+    }
+    a.partial[(size_t)blockIdx.x * a.nv + v] = acc;
+  }
+}
+
+// chi = sum of the chunk partials (fixed order); slab energy (energy.cpp:33-111).
+__global__ void __launch_bounds__(256) k_slab_chi_reduce(SlabArgs a) {
+  __shared__ double red[256];
+  double e = 0.0;
+  const int KX = a.kx, KY = a.ky;
+  for (int v = threadIdx.x; v < a.nv; v += blockDim.x) {
+    double c = 0.0;
+    for (int ch = 0; ch < a.nch; ++ch) c += a.partial[(size_t)ch * a.nv + v];
+    a.chi[v] = c;
+    // sign of c^2 in the energy: + for the cosh terms, - for the sinh terms
+    if (v < 4 * KX) {
+      e += ((v & 3) >> 1 ? 1.0 : -1.0) * c * c * a.kxc[v >> 2];
+    } else if (v < 4 * KX + 4 * KY) {
+      const int w = v - 4 * KX;
+      e += ((w & 3) >> 1 ? 1.0 : -1.0) * c * c * a.kyc[w >> 2];
+    } else if (v < 4 * KX + 4 * KY + 8 * KX * KY) {
+      const int w = v - 4 * KX - 4 * KY;
+      e += ((w & 7) >> 2 ? 1.0 : -1.0) * c * c * 2.0 * a.kpc[w >> 3];
+    }
+  }
+  red[threadIdx.x] = e;
+  __syncthreads();
+  for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+    if ((int)threadIdx.x < st) red[threadIdx.x] += red[threadIdx.x + st];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const double M = a.chi[a.nv - 1];
+    a.state[1] = red[0] * a.ke * a.sum_e_coef + 0.5 * a.dipole_coef * M * M;
+  }
+}
+
+// Field on each atom and its acceleration (field.cpp:27-144).
+template <typename real>
+__global__ void __launch_bounds__(128) k_slab_field(DevState<real> s, SlabArgs a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= s.n || *s.err) return;
+  const int KX = a.kx, KY = a.ky;
+  const double *cx_ = a.chi, *cy_ = a.chi + 4 * KX, *cp_ = a.chi + 4 * KX + 4 * KY;
+  double p[3];
+  slab_local(s, a.axis, i, p);
+  double f[3] = {0, 0, 0};
+  for (int ix = 0; ix < KX; ++ix) {
+    const double kx = a.kxv[ix];
+    const double sh = sinh(kx * p[2]), chh = cosh(kx * p[2]);
+    double sxx, cxx;
+    sincos(kx * p[0], &sxx, &cxx);
+    const double *c = cx_ + 4 * ix;  // [h][f]: sinh-sin, sinh-cos, cosh-sin, cosh-cos
+    f[0] += a.kxc[ix] * -kx * (-c[0] * cxx * sh + c[1] * sxx * sh + c[2] * cxx * chh - c[3] * sxx * chh);
+    f[2] += a.kxc[ix] * -kx * (-c[0] * chh * sxx - c[1] * chh * cxx + c[2] * sh * sxx + c[3] * sh * cxx);
+    for (int iy = 0; iy < KY; ++iy) {
+      const int ip = ix * KY + iy;
+      const double kp = a.kpv[ip], ky = a.kyv[iy];
+      const double sp = sinh(kp * p[2]), cp = cosh(kp * p[2]);
+      double syy, cyy;
+      sincos(ky * p[1], &syy, &cyy);
+      const double *q = cp_ + 8 * ip;  // [h][a][b]: h sinh/cosh, a sin/cos x, b sin/cos y
+      const double gx = -kx * (-q[0] * cxx * sp * syy - q[1] * cxx * sp * cyy + q[2] * sxx * sp * syy +
+                               q[4] * cxx * cp * syy + q[3] * sxx * sp * cyy + q[5] * cxx * cp * cyy -
+                               q[6] * sxx * cp * syy - q[7] * sxx * cp * cyy);
+      const double gy = -ky * (-q[0] * cyy * sp * sxx + q[1] * syy * sp * sxx - q[2] * cyy * sp * cxx +
+                               q[4] * cyy * cp * sxx + q[3] * syy * sp * cxx - q[5] * syy * cp * sxx +
+                               q[6] * cyy * cp * cxx - q[7] * syy * cp * cxx);
+      const double gz = -kp * (-q[0] * cp * sxx * syy - q[1] * cp * sxx * cyy - q[2] * cp * cxx * syy +
+                               q[4] * sp * sxx * syy - q[3] * cp * cxx * cyy + q[5] * sp * sxx * cyy +
+                               q[6] * sp * cxx * syy + q[7] * sp * cxx * cyy);
+      f[0] += 2.0 * a.kpc[ip] * gx;
+      f[1] += 2.0 * a.kpc[ip] * gy;
+      f[2] += 2.0 * a.kpc[ip] * gz;
+      if (ix == 0) {
+        const double shy = sinh(ky * p[2]), chy = cosh(ky * p[2]);
+        const double *y = cy_ + 4 * iy;
+        f[1] += a.kyc[iy] * -ky * (-y[0] * cyy * shy + y[1] * syy * shy + y[2] * cyy * chy - y[3] * syy * chy);
+        f[2] += a.kyc[iy] * -ky * (-y[0] * syy * chy - y[1] * cyy * chy + y[2] * syy * shy + y[3] * cyy * shy);
+      }
+    }
+  }
+  const double sc = 2.0 * a.sum_e_coef * a.ke;
+  // back to global axes as give_slab_global_coordinates does (for normal axes x
+  // and y its rotation is not the inverse of the local one; kept for parity),
+  // plus the lagged dipole field along the normal axis
+  double g[3];
+  if (a.axis == 0) {
+    g[0] = sc * f[1];
+    g[1] = sc * f[2];
+    g[2] = sc * f[0];
+  } else if (a.axis == 1) {
+    g[0] = sc * f[2];
+    g[1] = sc * f[0];
+    g[2] = sc * f[1];
+  } else {
+    g[0] = sc * f[0];
+    g[1] = sc * f[1];
+    g[2] = sc * f[2];
+  }
+  g[a.axis] -= a.state[0] * a.dipole_coef;
+  const int t = s.type[i];
+  const double qm = a.charge[t] * s.mass_inv[t];
+  s.ax[i] = (real)((double)s.ax[i] + qm * g[0]);
+  s.ay[i] = (real)((double)s.ay[i] + qm * g[1]);
+  s.az[i] = (real)((double)s.az[i] + qm * g[2]);
+}
+
+__global__ void k_slab_store_moment(SlabArgs a) { a.state[0] = a.chi[a.nv - 1]; }
+
 // Sets the step graph's IF condition from the device rebuild flag: the list
 // build nodes run only on steps that need them.
 __global__ void k_set_rebuild_condition(const int *__restrict__ flag, cudaGraphConditionalHandle h) {
@@ -885,6 +1066,7 @@ struct ThermoArgs {
   int n_ek;
   double total_mass, dof, volume, k_b, n_atoms, ek_coef, e_self;
   const double *dipole;  // E, M of the dipole term (nullable)
+  const double *slab_e;  // slab-correction energy of the last force call (nullable)
   double dipole_coef;    // k_e 4 pi / (V (1 + 2 eps')): energy 0.5 coef |M|^2 (energy.cpp:52-56)
   int com_removed;
   const int *n_builds;
@@ -928,6 +1110,7 @@ __global__ void __launch_bounds__(256) k_thermo(ThermoArgs a) {
       const double *M = a.dipole + 3;
       out[5] += 0.5 * a.dipole_coef * (M[0] * M[0] + M[1] * M[1] + M[2] * M[2]);
     }
+    if (a.slab_e) out[5] += *a.slab_e;
     out[6] = a.e_self;
     out[7] = vir;
     out[8] = a.n_atoms * a.k_b * temp / a.volume + vir / (3.0 * a.volume);

@@ -103,6 +103,16 @@ int cvr_set_ewald_k(cvr_ctx *ctx, double alpha, int kx_max, int ky_max, int kz_m
 #define CVR_DIPOLE_ONCE 2
 int cvr_set_ewald_k_geometry(cvr_ctx *ctx, int slab_axis, double slab_lz, int dipole_mode, double epsilon_dipole);
 
+/* force_field electrostatic_ewald_slab_correction (electrostatic_ewald_slab_correction.cpp:44-181
+ * and its initialize/field/energy files): the slab correction term for a
+ * system periodic in two directions, with the reference's keywords
+ * slab_normal_axis (0/1/2; -1 turns it off), lz (>= the box along that axis),
+ * kx_max, ky_max (1..8 here) and k_electrostatic.  Its field includes the
+ * reference's dipole term, which uses the normal dipole moment of the previous
+ * force call (the first call has none); its energy is added to
+ * thermo[CVR_TH_E_K]. */
+int cvr_set_ewald_slab_correction(cvr_ctx *ctx, int slab_axis, double lz, int kx_max, int ky_max, double k_e);
+
 /* md_simulator basic: dt; atom_data k_b.
  * Replaces: Md_simulator::read dt / integrator_type velocity_verlet (md_simulator.cpp:58-233). */
 int cvr_set_integrator(cvr_ctx *ctx, double dt, double k_b);

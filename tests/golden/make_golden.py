@@ -42,6 +42,11 @@ GPU tests never need the reference at run time).
    (a) z non-periodic, `slab_normal_axis z`, `slab_lz 30`, `epsilon_dipole 0`
    and (b) all periodic with `epsilon_dipole 1`, and (c) a 10-step run of (a).
 
+8. ref_slab_correction300.npz -- the same ions with the reference's
+   `force_field electrostatic_ewald_slab_correction` (lz 30, k_max 4) next to
+   the slab Ewald sum: forces and a 10-step run with the normal axis z, and
+   forces with the normal axis x.
+
 Usage:  python tests/golden/make_golden.py [/path/to/reference]
 """
 import json
@@ -257,6 +262,27 @@ def ewald_slab() -> None:
     np.savez_compressed(os.path.join(HERE, "ref_ewald_slab300.npz"), **out)
 
 
+def slab_correction() -> None:
+    out = {}
+    for ax, name in ((2, "z"), (0, "x")):
+        s = W.random_ions(300, 10.0, 21, rc=4.0, coef=1.03, kmax=4, alpha=0.8)
+        s.bc = (0, 1, 1) if ax == 0 else (1, 1, 0)
+        extra = (f"f_ek slab_normal_axis {name}\nf_ek slab_lz 30.0\n"
+                 "force_field electrostatic_ewald_slab_correction f_sc\nf_sc set_atom_data adata\n"
+                 f"f_sc set_domain dom\nf_sc slab_normal_axis {name}\nf_sc lz 30.0\nf_sc k_max 4\n"
+                 "sim add_force_field f_sc\n")
+        r = O.run_reference(s, "forces", extra=extra)
+        order = np.argsort(r["id"].astype(np.int64))
+        out[f"{name}_acc"] = r["acc"].reshape(-1, 3)[order]
+        out[f"{name}_script"] = extra
+        if name == "z":
+            r = O.run_reference(s, "run", 10, extra=extra)
+            order = np.argsort(r["id"].astype(np.int64))
+            out["z_run_pos"] = r["pos"].reshape(-1, 3)[order]
+            out["z_run_vel"] = r["vel"].reshape(-1, 3)[order]
+    np.savez_compressed(os.path.join(HERE, "ref_slab_correction300.npz"), **out)
+
+
 def main():
     ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     g = ewald_n100(ref_root)
@@ -271,6 +297,7 @@ def main():
     langevin500()
     thermostats()
     ewald_slab()
+    slab_correction()
     print("golden fixtures written to", HERE)
 
 
