@@ -10,6 +10,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <string>
 #include <array>
 #include <random>
@@ -25,7 +26,15 @@ using namespace cvr;
 
 namespace {
 
-constexpr int KCH = 64;  // atoms per S(k) chunk
+constexpr int KCH = 64;    // atoms per S(k) chunk
+constexpr int KMG = 3;     // m-values per S(k) thread
+constexpr int KMZ = 16;    // k-force: Z[m] held in registers up to this many m-values (kmax_z < 16)
+#ifndef CVR_KF_WMAX
+#define CVR_KF_WMAX 8
+#endif
+constexpr int KF_WMAX = CVR_KF_WMAX;  // k-force: most warps per block of 32 atoms
+constexpr int KRW = 16;    // warps of the S(k) chunk reduction
+constexpr size_t KF_COEF_SMEM = 72 * 1024;  // k-force: shared memory for staged column coefficients
 
 struct DBuf {
   void *p = nullptr;
@@ -90,10 +99,10 @@ struct cvr_ctx {
   double w[3] = {1, 1, 1};
   int tpa = 1, log2_tpa = 0, cap = 0, n_pad = 0;
   // k space
-  int nk = 0, nruns = 0, kp = 2;
+  int nk = 0, nxy = 0, kM = 1, kp = 2;
   std::vector<int4> kint;
   std::vector<double> fk;
-  std::vector<KRun> runs;
+  std::vector<int2> kxy, kpm;
   double e_self = 0, total_mass = 0;
   // device memory
   std::vector<std::pair<void **, size_t>> atom_bufs;
@@ -126,13 +135,13 @@ struct cvr_ctx {
   double *d_thermo{};
   size_t thermo_cap = 0;
   // k space device
-  int4 *d_kint{};
   double *d_fk{};
-  KRun *d_runs{};
+  int2 *d_kxy{}, *d_kpm{};
   double2 *d_kpartial{}, *d_sk{};
-  void *d_ak{}, *d_fpart{};
+  void *d_ptab{}, *d_kcoef{};
   int nchunks = 0;
-  int kf_threads = 128, kf_slices = 1, kf_runs_per_slice = 1;
+  int kf_warps = 1;  // k-force warps per block of 32 atoms
+  int kf_tc = 1;     // k-force columns per staged tile of one warp
   // diagnostics
   std::string err;
   int64_t launches = 0;
@@ -423,7 +432,8 @@ double kvolume(const cvr_ctx *c) { return klen(c, 0) * klen(c, 1) * klen(c, 2); 
 int setup_kspace(cvr_ctx *c) {
   c->kint.clear();
   c->fk.clear();
-  c->runs.clear();
+  c->kxy.clear();
+  c->kpm.clear();
   if (!c->ewk_on) {
     c->nk = 0;
     return CVR_OK;
@@ -444,32 +454,41 @@ int setup_kspace(cvr_ctx *c) {
         c->fk.push_back((1.0 / ksq) * std::exp(-ksq * four_alpha2_inv));
       }
   c->nk = (int)c->kint.size();
-  for (int k = 0; k < c->nk; ++k) {
-    const int4 v = c->kint[k];
-    if (!c->runs.empty()) {
-      KRun &r = c->runs.back();
-      if (r.nx == v.x && r.ny == v.y && r.nz0 + r.len == v.z) {
-        r.len++;
-        continue;
+  // (nx, ny) columns in order of first use; per column and m = 0..kmax_z the
+  // k indices of (nx, ny, +m) and (nx, ny, -m) (-1: not in the set)
+  c->kxy.clear();
+  std::vector<int> col_of(c->nk);
+  {
+    std::map<std::pair<int, int>, int> col;
+    for (int k = 0; k < c->nk; ++k) {
+      const int4 v = c->kint[k];
+      auto it = col.find({v.x, v.y});
+      if (it == col.end()) {
+        it = col.emplace(std::make_pair(v.x, v.y), (int)c->kxy.size()).first;
+        c->kxy.push_back(make_int2(v.x, v.y));
       }
+      col_of[k] = it->second;
     }
-    c->runs.push_back(KRun{v.x, v.y, v.z, 1, k});
   }
-  c->nruns = (int)c->runs.size();
+  c->nxy = (int)c->kxy.size();
+  c->kM = c->kmax[2] + 1;
+  c->kpm.assign((size_t)c->kM * c->nxy, make_int2(-1, -1));
+  for (int k = 0; k < c->nk; ++k) {
+    const int z = c->kint[k].z;
+    int2 &e = c->kpm[(size_t)std::abs(z) * c->nxy + col_of[k]];
+    (z >= 0 ? e.x : e.y) = k;
+  }
   c->kp = std::max(c->kmax[0], std::max(c->kmax[1], c->kmax[2])) + 1;
-  if (int r = dalloc(c, &c->d_kint, c->nk)) return r;
   if (int r = dalloc(c, &c->d_fk, c->nk)) return r;
-  if (int r = dalloc(c, &c->d_runs, c->nruns)) return r;
+  if (int r = dalloc(c, &c->d_kxy, c->nxy)) return r;
+  if (int r = dalloc(c, &c->d_kpm, c->kpm.size())) return r;
   if (int r = dalloc(c, &c->d_sk, c->nk)) return r;
-  if (c->precision == CVR_PREC_FP64) {
-    if (int r = dalloc(c, (double2 **)&c->d_ak, c->nk)) return r;
-  } else {
-    if (int r = dalloc(c, (float2 **)&c->d_ak, c->nk)) return r;
-  }
-  CVR_CUDA(c, cudaMemcpyAsync(c->d_kint, c->kint.data(), c->nk * sizeof(int4), cudaMemcpyHostToDevice, c->stream));
+  const size_t rb = (c->precision == CVR_PREC_FP64) ? 8 : 4;
+  if (int r = dalloc(c, (unsigned char **)&c->d_kcoef, (size_t)c->nxy * c->kM * 8 * rb)) return r;
   CVR_CUDA(c, cudaMemcpyAsync(c->d_fk, c->fk.data(), c->nk * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-  CVR_CUDA(c, cudaMemcpyAsync(c->d_runs, c->runs.data(), c->nruns * sizeof(KRun), cudaMemcpyHostToDevice, c->stream));
-  c->n_ek_blocks = grid_for(c->nk, 256);
+  CVR_CUDA(c, cudaMemcpyAsync(c->d_kxy, c->kxy.data(), c->nxy * sizeof(int2), cudaMemcpyHostToDevice, c->stream));
+  CVR_CUDA(c, cudaMemcpyAsync(c->d_kpm, c->kpm.data(), c->kpm.size() * sizeof(int2), cudaMemcpyHostToDevice, c->stream));
+  c->n_ek_blocks = grid_for(c->kM * c->nxy, 32);
   if (int r = dalloc(c, &c->ek_part, c->n_ek_blocks)) return r;
   return CVR_OK;
 }
@@ -602,19 +621,21 @@ template <typename real>
 KArgs<real> kargs(cvr_ctx *c) {
   KArgs<real> a{};
   a.nk = c->nk;
-  a.nruns = c->nruns;
+  a.nxy = c->nxy;
+  a.M = c->kM;
   for (int d = 0; d < 3; ++d) {
     a.kmax[d] = c->kmax[d];
     a.inv_L[d] = 1.0 / klen(c, d);
     a.two_pi_over_L[d] = (real)(6.28318530717958647692 / klen(c, d));
   }
   a.kp = c->kp;
-  a.kint = c->d_kint;
+  a.xy = c->d_kxy;
+  a.kpm = c->d_kpm;
   a.fk = c->d_fk;
-  a.runs = c->d_runs;
+  a.ptab = (typename R2<real>::t *)c->d_ptab;
   a.partial = c->d_kpartial;
   a.sk = c->d_sk;
-  a.ak = (typename R2<real>::t *)c->d_ak;
+  a.kcoef = (real *)c->d_kcoef;
   a.e_partials = c->ek_part;
   a.four_pi_over_v = 12.56637061435917295384 / kvolume(c);
   a.charge = c->d_charge;
@@ -623,35 +644,72 @@ KArgs<real> kargs(cvr_ctx *c) {
   return a;
 }
 
+// dynamic shared memory of the S(k) kernel (a chunk's phase tables and
+// charges) and of the k-force kernel (the warps' coefficient tiles and
+// column indices, 32 atoms' phase tables, the warps' partial forces)
+template <typename real>
+size_t sk_smem(const cvr_ctx *c) {
+  const int rw = 2 * c->kp + ((c->kM + KMG - 1) / KMG) * KMG;
+  return (size_t)KCH * rw * sizeof(typename R2<real>::t) + KCH * sizeof(real);
+}
+template <typename real>
+size_t kf_smem(const cvr_ctx *c) {
+  const size_t tiles = (size_t)c->kf_warps * c->kf_tc;
+  return tiles * c->kM * 8 * sizeof(real) + ((tiles + 1) & ~(size_t)1) * sizeof(int2) +
+         (size_t)32 * 3 * c->kp * sizeof(typename R2<real>::t) + (size_t)c->kf_warps * 96 * sizeof(real);
+}
+
+// k-force kernel instance for the context's m-count: Z in registers for
+// M = 1..KMZ (one instance per M), else from shared memory.
+template <typename real, int MZ>
+struct KForceTable {
+  static void launch(cvr_ctx *c, const DevState<real> &s, const KArgs<real> &a) {
+    if (c->kM == MZ)
+      k_kforce<real, MZ><<<grid_for(c->n, 32), dim3(32, c->kf_warps), kf_smem<real>(c), c->stream>>>(s, a, c->kf_tc);
+    else
+      KForceTable<real, MZ - 1>::launch(c, s, a);
+  }
+  static void attrs(cvr_ctx *c) {
+    cudaFuncSetAttribute(k_kforce<real, MZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)std::max<size_t>(kf_smem<real>(c), 48 * 1024));
+    KForceTable<real, MZ - 1>::attrs(c);
+  }
+};
+template <typename real>
+struct KForceTable<real, 0> {
+  static void launch(cvr_ctx *c, const DevState<real> &s, const KArgs<real> &a) {
+    k_kforce<real, 0><<<grid_for(c->n, 32), dim3(32, c->kf_warps), kf_smem<real>(c), c->stream>>>(s, a, c->kf_tc);
+  }
+  static void attrs(cvr_ctx *c) {
+    cudaFuncSetAttribute(k_kforce<real, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)std::max<size_t>(kf_smem<real>(c), 48 * 1024));
+  }
+};
+template <typename real>
+void launch_kforce(cvr_ctx *c, const DevState<real> &s, const KArgs<real> &a) {
+  KForceTable<real, KMZ>::launch(c, s, a);
+}
+
 template <typename real>
 int launch_kspace(cvr_ctx *c) {
   if (!c->ewk_on || c->nk == 0) return CVR_OK;
   Bracket br(c, CVR_KT_KSPACE);
-  using c2 = typename R2<real>::t;
   DevState<real> s = dev_state<real>(c);
   KArgs<real> a = kargs<real>(c);
-  const size_t sm1 = (size_t)KCH * 3 * c->kp * sizeof(c2) + KCH * sizeof(real);
-  dim3 g1(grid_for(c->nk, 256), c->nchunks);
-  k_sk_partial<real, KCH><<<g1, 256, sm1, c->stream>>>(s, a);
-  k_sk_reduce<real><<<c->n_ek_blocks, 256, 0, c->stream>>>(s, a);
-  const int tb = c->kf_threads;
-  const size_t sm3 = (size_t)tb * 3 * c->kp * sizeof(c2);
-  dim3 g3(grid_for(c->n, tb), c->kf_slices);
-  k_kforce<real><<<g3, tb, sm3, c->stream>>>(s, a, c->kf_runs_per_slice, (real *)c->d_fpart);
-  c->launches += 3;
-  if (c->kf_slices > 1) {
-    k_kforce_reduce<real><<<grid_for(c->n, 256), 256, 0, c->stream>>>(s, a, c->kf_slices, (const real *)c->d_fpart);
-    c->launches++;
-  }
+  k_phase<real><<<grid_for(3 * c->n, 256), 256, 0, c->stream>>>(s, a);
+  dim3 g1(grid_for(((c->kM + KMG - 1) / KMG) * c->nxy, 128), c->nchunks);
+  k_sk_partial<real, KMG, KCH><<<g1, 128, sk_smem<real>(c), c->stream>>>(s, a);
+  k_sk_reduce<real, KRW><<<c->n_ek_blocks, KRW * 32, 0, c->stream>>>(s, a);
+  launch_kforce<real>(c, s, a);
+  c->launches += 4;
   return CVR_OK;
 }
 
 template <typename real>
 void set_smem_attrs(cvr_ctx *c) {
-  using c2 = typename R2<real>::t;
-  const size_t sm1 = (size_t)KCH * 3 * c->kp * sizeof(c2) + KCH * sizeof(real);
-  cudaFuncSetAttribute(k_sk_partial<real, KCH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(sm1, 48 * 1024));
-  cudaFuncSetAttribute(k_kforce<real>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024 + 1024);
+  cudaFuncSetAttribute(k_sk_partial<real, KMG, KCH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)std::max<size_t>(sk_smem<real>(c), 48 * 1024));
+  KForceTable<real, KMZ>::attrs(c);
 }
 
 template <typename real>
@@ -1058,7 +1116,7 @@ int run_impl(cvr_ctx *c, int64_t nsteps, int64_t every, double *thermo) {
     collect_timing(c);
     if (graphs) {
       // kernel nodes executed: per step kick_drift + condition + tail; 8 per rebuild
-      const int tail = 1 + (c->lj_on || c->ewr_on ? 1 : 0) + ((c->ewk_on && c->nk > 0) ? (c->kf_slices > 1 ? 4 : 3) : 0) +
+      const int tail = 1 + (c->lj_on || c->ewr_on ? 1 : 0) + ((c->ewk_on && c->nk > 0) ? 4 : 0) +
                        ((c->tstat.kind && c->integrator == 0) ? 2 : 0) + (c->sc_on ? 4 : 0) +
                        ((c->ewk_on && c->dipole_mode) ? 3 : 0);
       c->launches = launches0 + nsteps * (2 + tail) + nrec + 8 * (int64_t)(f[3] - f0[3]);
@@ -1157,20 +1215,19 @@ int refresh(cvr_ctx *c) {
   if (int r = setup_kspace(c)) return r;
   if (c->ewk_on && c->nk > 0) {
     c->nchunks = grid_for(c->n, KCH);
-    if (int r = dalloc(c, &c->d_kpartial, (size_t)c->nchunks * c->nk)) return r;
-    // k-force launch shape: threads per block bounded by the phase tables'
-    // shared memory, k-runs split into slices until ~8 blocks per SM exist
+    if (int r = dalloc(c, &c->d_kpartial, (size_t)c->nchunks * c->kM * c->nxy * 2)) return r;
     const size_t c2b = (c->precision == CVR_PREC_FP64) ? 16 : 8;
-    int tb = 128;
-    while (tb > 32 && (size_t)tb * 3 * c->kp * c2b > 96 * 1024) tb /= 2;
-    c->kf_threads = tb;
-    const int atom_blocks = grid_for(c->n, tb);
-    int slices = std::max(1, std::min(c->nruns, (8 * 148 + atom_blocks - 1) / atom_blocks));
-    c->kf_runs_per_slice = (c->nruns + slices - 1) / slices;
-    c->kf_slices = (c->nruns + c->kf_runs_per_slice - 1) / c->kf_runs_per_slice;
-    if (c->kf_slices > 1) {
-      const size_t bytes = (size_t)c->kf_slices * 3 * c->n * ((c->precision == CVR_PREC_FP64) ? 8 : 4);
-      if (int r = dalloc(c, (unsigned char **)&c->d_fpart, bytes)) return r;
+    if (int r = dalloc(c, (unsigned char **)&c->d_ptab, (size_t)3 * c->kp * c->n * c2b)) return r;
+    // k-force launch shape: warps per block of 32 atoms until ~24 warps per
+    // SM exist (at most 16, at most one per column)
+    const int atom_blocks = grid_for(c->n, 32);
+    c->kf_warps = std::max(1, std::min(std::min(KF_WMAX, c->nxy), (24 * 148 + atom_blocks - 1) / atom_blocks));
+    // columns per warp staged in tiles of equal size within KF_COEF_SMEM
+    {
+      const int per_warp = (c->nxy + c->kf_warps - 1) / c->kf_warps;
+      const int tc_max = std::max<int>(1, (int)(KF_COEF_SMEM / ((size_t)c->kf_warps * c->kM * 8 * (c2b / 2))));
+      const int ntiles = (per_warp + tc_max - 1) / tc_max;
+      c->kf_tc = (per_warp + ntiles - 1) / ntiles;
     }
     if (c->precision == CVR_PREC_FP64)
       set_smem_attrs<double>(c);

@@ -26,6 +26,14 @@
 #ifndef CVR_PAIR_MINB
 #define CVR_PAIR_MINB 1
 #endif
+// k-force kernel: minimum resident blocks (FP32) and 16-byte coefficient
+// loads in flight per lane while staging.
+#ifndef CVR_KF_MINB
+#define CVR_KF_MINB 1
+#endif
+#ifndef CVR_KF_SB
+#define CVR_KF_SB 4
+#endif
 
 namespace cvr {
 
@@ -263,32 +271,32 @@ __global__ void __launch_bounds__(128, CVR_PAIR_MINB) k_pair(DevState<real> s, c
 }
 
 // ------------------------------------------------------------------ k space
-// k-vectors of the used set in the reference's enumeration order, grouped in
-// runs of consecutive nz at fixed (nx, ny).
-struct KRun {
-  int nx, ny, nz0, len, k0;
-};
-
+// The reference's k-set (initialize.cpp:184-222) is regrouped by (nx, ny)
+// column: for column c and m = 0..kmax_z, kpm[m * nxy + c] holds the indices
+// of (nx, ny, +m) and (nx, ny, -m) in the k-set (-1 where the set lacks
+// it).  e^{i k.r} = X[nx] Y[ny] Z[+-m] with Z[-m] = conj(Z[m]), so one
+// complex product P = X Y serves a whole column and each +-m pair costs
+// eight FMAs in both the S(k) and the force kernel.
 template <typename real> struct KArgs {
-  int nk, nruns, kmax[3], kp;  // kp = max kmax + 1 (table row length)
-  const int4 *kint;            // (nx, ny, nz, -) per used k
-  const double *fk;            // exp(-k^2/4a^2)/k^2 per used k
-  const KRun *runs;
-  double2 *partial;            // [nchunks][nk]
-  double2 *sk;                 // S(k)
-  typename R2<real>::t *ak;    // (4 pi / V) f_k conj(S_k)
-  double *e_partials;          // per block of k_sk_reduce
+  int nk, nxy, M, kmax[3], kp;  // M = kmax_z + 1 m-values; kp = max kmax + 1
+  const int2 *xy;               // (nx, ny) per column
+  const int2 *kpm;              // [M][nxy] k indices of (nx, ny, +m), (nx, ny, -m)
+  const double *fk;             // exp(-k^2/4a^2)/k^2 per used k
+  typename R2<real>::t *ptab;   // phase tables [3 * kp][n]
+  double2 *partial;             // [nchunks][M][nxy][2]: S(+m), S(-m) of one atom chunk
+  double2 *sk;                  // S(k)
+  real *kcoef;                  // [nxy][M][8] force coefficients (see k_sk_reduce)
+  double *e_partials;           // per block of k_sk_reduce
   double inv_L[3];
   real two_pi_over_L[3];
   double four_pi_over_v;
-  double *charge;              // per type
+  double *charge;               // per type
   double k_e;
   int nchunks;
 };
 
-// Phase table of one atom: e^{i 2 pi m x_d / L_d}, m = 0..kmax_d, from the
-// fractional part of m x_d / L_d in FP64 (so |x| up to the box size costs no
-// phase accuracy), then sincospi in `real`.
+// Phase e^{i 2 pi m x / L} from the fractional part of m x / L in FP64 (so
+// |x| up to the box size costs no phase accuracy), then sincospi in `real`.
 template <typename real>
 __device__ __forceinline__ typename R2<real>::t phase(double x_over_L, int m) {
   const double u = (double)m * x_over_L;
@@ -314,153 +322,335 @@ __device__ __forceinline__ T conj_if(T a, bool c) {
   return a;
 }
 
-// S(k) partial sums: one thread per k-vector, one block row per chunk of
-// KCH atoms whose phase tables sit in shared memory.  Products are summed in
-// `real` over groups of 16 atoms; groups and chunks accumulate in FP64.
-template <typename real, int KCH>
-__global__ void __launch_bounds__(256) k_sk_partial(DevState<real> s, KArgs<real> a) {
+// Phase tables of every atom, once per force evaluation:
+// ptab[(d * kp + m) * n + i] = e^{i 2 pi m x_d / L_d}, m = 0..kmax_d
+// (row-major by (d, m), so 32 consecutive atoms are 32 consecutive words).
+template <typename real>
+__global__ void __launch_bounds__(256) k_phase(DevState<real> s, KArgs<real> a) {
+  if (*s.err) return;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 3 * s.n) return;
+  const int d = t / s.n, i = t - d * s.n;
+  const double x = ((d == 0) ? s.x[i] : ((d == 1) ? s.y[i] : s.z[i])) * a.inv_L[d];
+  for (int m = 0; m <= a.kmax[d]; ++m) a.ptab[(size_t)(d * a.kp + m) * s.n + i] = phase<real>(x, m);
+}
+
+// S(k) partial sums (electrostatic_ewald_k/initialize.cpp:117-146): one thread per
+// (column, group of MG m-values), one block row per chunk of CH atoms whose
+// phase tables and charges sit in shared memory.  Table rows per atom
+// (atom-major, so the lanes' X and Y rows of one atom are distinct words,
+// conflict-free): X[0..kp), Y[0..kp), Z[0..MG * groups), zero past kmax and
+// past the chunk's last atom, so the inner loops need no guards.
+// Consecutive threads take consecutive columns of one m-group: the Z loads
+// are warp broadcasts.  Products are summed in `real` over groups of 16
+// atoms; groups accumulate in FP64; chunks are summed by k_sk_reduce in a
+// fixed order.
+template <typename real, int MG, int CH>
+__global__ void __launch_bounds__(128) k_sk_partial(DevState<real> s, KArgs<real> a) {
+  static_assert(CH % 16 == 0, "atom chunk in whole groups of 16");
   using c2 = typename R2<real>::t;
   extern __shared__ unsigned char smem_raw[];
-  c2 *tab = reinterpret_cast<c2 *>(smem_raw);  // [KCH][3][kp]
-  real *q = reinterpret_cast<real *>(tab + KCH * 3 * a.kp);
+  const int ngroups = (a.M + MG - 1) / MG;
+  const int rw = 2 * a.kp + ngroups * MG;
+  c2 *tab = reinterpret_cast<c2 *>(smem_raw);          // [CH][rw]
+  real *q = reinterpret_cast<real *>(tab + rw * CH);  // [CH]
   if (*s.err) return;
-  const int chunk = blockIdx.y;
-  const int a0 = chunk * KCH;
-  const int kp = a.kp;
-  for (int t = threadIdx.x; t < KCH * 3 * kp; t += blockDim.x) {
-    const int at = t / (3 * kp), rem = t % (3 * kp), d = rem / kp, m = rem % kp;
-    const int idx = a0 + at;
+  const int a0 = blockIdx.y * CH;
+  const int na = min(CH, s.n - a0);
+  // staging: SB loads in flight per thread before their stores
+  constexpr int SB = 8;
+  for (int e0 = threadIdx.x; e0 < rw * CH; e0 += SB * blockDim.x) {
+    c2 v[SB];
+#pragma unroll
+    for (int u = 0; u < SB; ++u) {
+      const int e = e0 + u * blockDim.x;
+      const int row = e / CH, at = e - row * CH;
+      const int d = min(row / a.kp, 2), m = row - d * a.kp;
+      v[u].x = 0;
+      v[u].y = 0;
+      if (e < rw * CH && at < na && m <= a.kmax[d]) v[u] = a.ptab[(size_t)(d * a.kp + m) * s.n + a0 + at];
+    }
+#pragma unroll
+    for (int u = 0; u < SB; ++u) {
+      const int e = e0 + u * blockDim.x;
+      const int row = e / CH, at = e - row * CH;
+      if (e < rw * CH) tab[at * rw + row] = v[u];
+    }
+  }
+  for (int t = threadIdx.x; t < CH; t += blockDim.x) q[t] = (t < na) ? (real)a.charge[s.type[a0 + t]] : (real)0;
+  __syncthreads();
+  const int task = blockIdx.x * blockDim.x + threadIdx.x;
+  if (task >= ngroups * a.nxy) return;
+  const int g = task / a.nxy, col = task - g * a.nxy;
+  const int2 nn = a.xy[col];
+  const int ox = abs(nn.x), oy = a.kp + abs(nn.y), oz = 2 * a.kp + g * MG;
+  const bool cx = nn.x < 0, cy = nn.y < 0;
+  double tot[MG][4];
+#pragma unroll
+  for (int u = 0; u < MG; ++u) tot[u][0] = tot[u][1] = tot[u][2] = tot[u][3] = 0.0;
+  for (int t0 = 0; t0 < na; t0 += 16) {
+    real acc[MG][4];
+#pragma unroll
+    for (int u = 0; u < MG; ++u) acc[u][0] = acc[u][1] = acc[u][2] = acc[u][3] = (real)0;
+    const c2 *ta = tab + t0 * rw;
+#pragma unroll 4
+    for (int t = 0; t < 16; ++t, ta += rw) {
+      c2 w = cmul(conj_if(ta[ox], cx), conj_if(ta[oy], cy));
+      const real qt = q[t0 + t];
+      w.x *= qt;
+      w.y *= qt;
+#pragma unroll
+      for (int u = 0; u < MG; ++u) {
+        const c2 z = ta[oz + u];
+        // S(+m) += w z, S(-m) += w conj(z)
+        acc[u][0] += w.x * z.x;
+        acc[u][0] -= w.y * z.y;
+        acc[u][1] += w.x * z.y;
+        acc[u][1] += w.y * z.x;
+        acc[u][2] += w.x * z.x;
+        acc[u][2] += w.y * z.y;
+        acc[u][3] += w.y * z.x;
+        acc[u][3] -= w.x * z.y;
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < MG; ++u)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) tot[u][c] += (double)acc[u][c];
+  }
+#pragma unroll
+  for (int u = 0; u < MG; ++u) {
+    if (g * MG + u < a.M) {
+      const size_t idx = ((size_t)blockIdx.y * a.M + g * MG + u) * a.nxy + col;
+      a.partial[2 * idx] = make_double2(tot[u][0], tot[u][1]);
+      a.partial[2 * idx + 1] = make_double2(tot[u][2], tot[u][3]);
+    }
+  }
+}
+
+// S(k) = sum of the chunk partials (RW warps: warp w adds chunks w, w + RW,
+// ... in order, four loads in flight; then warp 0 adds the RW sums in warp
+// order: a fixed order, deterministic), one lane per (column, m) pair.
+// Writes S(k), the FP64 k-space energy partials sum_k f_k |S_k|^2, and the
+// force coefficients of the pair: with A_k = (4 pi / V) f_k conj(S_k) =
+// a + ib at +m and c + id at -m, kcoef = (a+c, d-b, b+d, a-c) and the same
+// times m.
+template <typename real, int RW>
+__global__ void __launch_bounds__(RW * 32) k_sk_reduce(DevState<real> s, KArgs<real> a) {
+  __shared__ double part[RW][4][32];
+  if (*s.err) return;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int np = a.M * a.nxy;
+  const int p = blockIdx.x * 32 + lane;
+  double v[4] = {0.0, 0.0, 0.0, 0.0};
+  if (p < np) {
+    for (int c0 = w; c0 < a.nchunks; c0 += 4 * RW) {
+      double2 u[4][2];
+#pragma unroll
+      for (int h = 0; h < 4; ++h) {
+        const int c = c0 + h * RW;
+        const size_t idx = (size_t)min(c, a.nchunks - 1) * np + p;
+        u[h][0] = a.partial[2 * idx];
+        u[h][1] = a.partial[2 * idx + 1];
+      }
+#pragma unroll
+      for (int h = 0; h < 4; ++h) {
+        if (c0 + h * RW < a.nchunks) {
+          v[0] += u[h][0].x;
+          v[1] += u[h][0].y;
+          v[2] += u[h][1].x;
+          v[3] += u[h][1].y;
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 4; ++c) part[w][c][lane] = v[c];
+  __syncthreads();
+  double e = 0;
+  if (w == 0 && p < np) {
+    double S[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int ww = 0; ww < RW; ++ww)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) S[c] += part[ww][c][lane];
+    const int2 kk = a.kpm[p];
+    double A[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int k = h ? kk.y : kk.x;
+      if (k >= 0) {
+        const double sr = S[2 * h], si = S[2 * h + 1];
+        a.sk[k] = make_double2(sr, si);
+        const double f = a.fk[k];
+        const double cf = a.four_pi_over_v * f;
+        A[2 * h] = cf * sr;
+        A[2 * h + 1] = -cf * si;
+        e += f * (sr * sr + si * si);
+      }
+    }
+    const int m = p / a.nxy, col = p - m * a.nxy;
+    const double c4[4] = {A[0] + A[2], A[3] - A[1], A[1] + A[3], A[0] - A[2]};
+    real *o = a.kcoef + ((size_t)col * a.M + m) * 8;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      o[c] = (real)c4[c];
+      o[4 + c] = (real)(m * c4[c]);
+    }
+  }
+  double ev[1] = {e};
+  block_sum_store<1>(ev, a.e_partials);
+}
+
+// Eight force coefficients of one (column, m) pair: two 16-byte loads (float)
+// or four (double), uniform across the warp.
+__device__ __forceinline__ void load8(const float *p, float (&r)[8]) {
+  const float4 u = __ldg(reinterpret_cast<const float4 *>(p)), v = __ldg(reinterpret_cast<const float4 *>(p) + 1);
+  r[0] = u.x; r[1] = u.y; r[2] = u.z; r[3] = u.w; r[4] = v.x; r[5] = v.y; r[6] = v.z; r[7] = v.w;
+}
+__device__ __forceinline__ void load8(const double *p, double (&r)[8]) {
+  const double2 *q = reinterpret_cast<const double2 *>(p);
+#pragma unroll
+  for (int h = 0; h < 4; ++h) {
+    const double2 u = __ldg(q + h);
+    r[2 * h] = u.x;
+    r[2 * h + 1] = u.y;
+  }
+}
+
+__device__ __forceinline__ void load8s(const float *p, float (&r)[8]) {
+  const float4 u = reinterpret_cast<const float4 *>(p)[0], v = reinterpret_cast<const float4 *>(p)[1];
+  r[0] = u.x; r[1] = u.y; r[2] = u.z; r[3] = u.w; r[4] = v.x; r[5] = v.y; r[6] = v.z; r[7] = v.w;
+}
+__device__ __forceinline__ void load8s(const double *p, double (&r)[8]) {
+#pragma unroll
+  for (int h = 0; h < 4; ++h) {
+    const double2 u = reinterpret_cast<const double2 *>(p)[h];
+    r[2 * h] = u.x;
+    r[2 * h + 1] = u.y;
+  }
+}
+
+// One (column, m) term of the k-force sums C and D (see k_kforce).
+template <typename real>
+__device__ __forceinline__ void kf_term(const real (&q)[8], real zx, real zy, real &Cx, real &Cy, real &Dx, real &Dy) {
+  Cx += q[0] * zx;
+  Cx += q[1] * zy;
+  Cy += q[2] * zx;
+  Cy += q[3] * zy;
+  Dx += q[7] * zx;
+  Dx -= q[6] * zy;
+  Dy += q[4] * zy;
+  Dy -= q[5] * zx;
+}
+
+// k-space force (electrostatic_ewald_k.cpp:215-218):
+// F_i = k_e q_i sum_k k Im(A_k e^{i k.r_i}).  A block holds 32 atoms (one per
+// lane) and W warps; warp w takes the w-th of W equal ranges of (nx, ny)
+// columns, so a few thousand atoms still fill the GPU.  Each warp stages its
+// columns' coefficients in shared memory, TC columns at a time, with
+// 16-byte loads all in flight (one L2 round trip per tile), then reads them
+// as broadcasts.  The 32 atoms' phase tables sit in shared memory
+// (atom-major).  MZ = M (the number of m-values, exact, so the m-loop
+// unrolls without guards) keeps Z[m] in registers; MZ = 0 reads it from
+// shared memory for any M.  Per column: C = sum_m (A+ z + A- conj z),
+// D = sum_m m (A+ z - A- conj z), then Im(P C) feeds F_x, F_y and Im(P D)
+// feeds F_z, P = X[nx] Y[ny].  The W partial forces of an atom are added in
+// warp order (deterministic).
+template <typename real, int MZ>
+__global__ void __launch_bounds__(512, sizeof(real) == 4 ? CVR_KF_MINB : 1) k_kforce(DevState<real> s, KArgs<real> a,
+                                                                                  int TC) {
+  using c2 = typename R2<real>::t;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x, w = threadIdx.y, W = blockDim.y;
+  const int M = a.M, rw = 3 * a.kp;
+  const int cw = M * 8;  // reals per column
+  real *cfw = reinterpret_cast<real *>(smem_raw) + (size_t)w * TC * cw;                  // [W][TC][M][8]
+  int2 *xyw = reinterpret_cast<int2 *>(reinterpret_cast<real *>(smem_raw) + (size_t)W * TC * cw) + w * TC;
+  c2 *tab = reinterpret_cast<c2 *>(reinterpret_cast<int2 *>(reinterpret_cast<real *>(smem_raw) + (size_t)W * TC * cw) +
+                                   ((W * TC + 1) & ~1));                                  // [32][3 * kp]
+  real *red = reinterpret_cast<real *>(tab + 32 * rw);                                     // [W][3][32]
+  if (*s.err) return;
+  const int i = blockIdx.x * 32 + lane;
+  const bool valid = i < s.n;
+  for (int row = w; row < rw; row += W) {
+    const int d = row / a.kp, m = row - d * a.kp;
     c2 v;
     v.x = 0;
     v.y = 0;
-    if (idx < s.n && m <= a.kmax[d]) {
-      const double x = (d == 0) ? s.x[idx] : ((d == 1) ? s.y[idx] : s.z[idx]);
-      v = phase<real>(x * a.inv_L[d], m);
-    }
-    tab[t] = v;
-  }
-  for (int t = threadIdx.x; t < KCH; t += blockDim.x) {
-    const int idx = a0 + t;
-    q[t] = (idx < s.n) ? (real)a.charge[s.type[idx]] : (real)0;
+    if (valid && m <= a.kmax[d]) v = a.ptab[(size_t)row * s.n + i];
+    tab[lane * rw + row] = v;
   }
   __syncthreads();
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= a.nk) return;
-  const int4 kn = a.kint[k];
-  const int mx = abs(kn.x), my = abs(kn.y), mz = abs(kn.z);
-  double sr = 0, si = 0;
-  const int na = min(KCH, s.n - a0);
-  for (int t0 = 0; t0 < na; t0 += 16) {
-    // products in `real`, summed over 16 atoms, then accumulated in FP64
-    real pr = 0, pim = 0;
-    const int t1 = min(na, t0 + 16);
-    for (int t = t0; t < t1; ++t) {
-      const c2 *tb = tab + t * 3 * kp;
-      const c2 px = conj_if(tb[mx], kn.x < 0);
-      const c2 py = conj_if(tb[kp + my], kn.y < 0);
-      const c2 pz = conj_if(tb[2 * kp + mz], kn.z < 0);
-      const c2 p = cmul(cmul(px, py), pz);
-      pr += q[t] * p.x;
-      pim += q[t] * p.y;
+  const c2 *ta = tab + lane * rw;
+  real zx[MZ > 0 ? MZ : 1], zy[MZ > 0 ? MZ : 1];
+  if (MZ > 0) {
+#pragma unroll
+    for (int m = 0; m < (MZ > 0 ? MZ : 1); ++m) {
+      const c2 z = ta[2 * a.kp + m];
+      zx[m] = z.x;
+      zy[m] = z.y;
     }
-    sr += (double)pr;
-    si += (double)pim;
   }
-  a.partial[(size_t)chunk * a.nk + k] = make_double2(sr, si);
-}
-
-// S(k) = sum of the chunk partials in chunk order; A_k for the force; FP64
-// k-space energy partials sum_k f_k |S_k|^2.
-template <typename real>
-__global__ void __launch_bounds__(256) k_sk_reduce(DevState<real> s, KArgs<real> a) {
-  if (*s.err) return;
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  double e = 0;
-  if (k < a.nk) {
-    double sr = 0, si = 0;
-    for (int c = 0; c < a.nchunks; ++c) {
-      const double2 p = a.partial[(size_t)c * a.nk + k];
-      sr += p.x;
-      si += p.y;
-    }
-    a.sk[k] = make_double2(sr, si);
-    const double f = a.fk[k];
-    const double cf = a.four_pi_over_v * f;
-    typename R2<real>::t A;
-    A.x = (real)(cf * sr);
-    A.y = (real)(-cf * si);
-    a.ak[k] = A;
-    e = f * (sr * sr + si * si);
-  }
-  double v[1] = {e};
-  block_sum_store<1>(v, a.e_partials);
-}
-
-// k-space force: one thread per atom, one block column per slice of the
-// k-runs (so a few thousand atoms still fill the GPU), the atom's phase
-// table in shared memory, runs of nz at fixed (nx, ny) so each k costs one
-// complex multiply.  F_i = k_e q_i sum_k k Im(A_k e^{i k.r_i})
-// (electrostatic_ewald_k.cpp:215-218).  With one slice the kernel adds into
-// the accelerations; with several it writes per-slice sums that
-// k_kforce_reduce adds in slice order (deterministic).
-template <typename real>
-__global__ void __launch_bounds__(128) k_kforce(DevState<real> s, KArgs<real> a, int runs_per_slice,
-                                                real *__restrict__ fpart) {
-  using c2 = typename R2<real>::t;
-  extern __shared__ unsigned char smem_raw[];
-  const int kp = a.kp;
-  c2 *tab = reinterpret_cast<c2 *>(smem_raw) + (size_t)threadIdx.x * 3 * kp;
-  if (*s.err) return;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= s.n) return;
-  const double pd[3] = {s.x[i], s.y[i], s.z[i]};
-  for (int d = 0; d < 3; ++d)
-    for (int m = 0; m <= a.kmax[d]; ++m) tab[d * kp + m] = phase<real>(pd[d] * a.inv_L[d], m);
-  const int r0 = blockIdx.y * runs_per_slice;
-  const int r1 = min(a.nruns, r0 + runs_per_slice);
+  const int c0 = (int)(((long)w * a.nxy) / W), c1 = (int)(((long)(w + 1) * a.nxy) / W);
   real fx = 0, fy = 0, fz = 0;
-  for (int r = r0; r < r1; ++r) {
-    const KRun run = a.runs[r];
-    const c2 pxy = cmul(conj_if(tab[abs(run.nx)], run.nx < 0), conj_if(tab[kp + abs(run.ny)], run.ny < 0));
-    real tsum = 0;
-    for (int u = 0; u < run.len; ++u) {
-      const int nz = run.nz0 + u;
-      const c2 p = cmul(pxy, conj_if(tab[2 * kp + abs(nz)], nz < 0));
-      const c2 A = a.ak[run.k0 + u];
-      const real t = A.x * p.y + A.y * p.x;
-      tsum += t;
-      fz += (real)nz * t;
+  for (int cb = c0; cb < c1; cb += TC) {
+    const int nt = min(TC, c1 - cb);
+    __syncwarp();
+    {
+      constexpr int SB = CVR_KF_SB;
+      const int nv = nt * cw * (int)sizeof(real) / 16;
+      const uint4 *src = reinterpret_cast<const uint4 *>(a.kcoef + (size_t)cb * cw);
+      uint4 *dst = reinterpret_cast<uint4 *>(cfw);
+      for (int v0 = lane; v0 < nv; v0 += SB * 32) {
+        uint4 r[SB];
+#pragma unroll
+        for (int u = 0; u < SB; ++u)
+          if (v0 + u * 32 < nv) r[u] = __ldg(src + v0 + u * 32);
+#pragma unroll
+        for (int u = 0; u < SB; ++u)
+          if (v0 + u * 32 < nv) dst[v0 + u * 32] = r[u];
+      }
+      for (int c = lane; c < nt; c += 32) xyw[c] = a.xy[cb + c];
     }
-    fx += (real)run.nx * tsum;
-    fy += (real)run.ny * tsum;
+    __syncwarp();
+    for (int c = 0; c < nt; ++c) {
+      const int2 nn = xyw[c];
+      const c2 P = cmul(conj_if(ta[abs(nn.x)], nn.x < 0), conj_if(ta[a.kp + abs(nn.y)], nn.y < 0));
+      const real *qc = cfw + (size_t)c * cw;
+      real Cx = 0, Cy = 0, Dx = 0, Dy = 0;
+      if (MZ > 0) {
+#pragma unroll
+        for (int m = 0; m < (MZ > 0 ? MZ : 1); ++m) {
+          real q[8];
+          load8s(qc + m * 8, q);
+          kf_term(q, zx[m], zy[m], Cx, Cy, Dx, Dy);
+        }
+      } else {
+#pragma unroll 3
+        for (int m = 0; m < M; ++m) {
+          real q[8];
+          load8s(qc + m * 8, q);
+          const c2 z = ta[2 * a.kp + m];
+          kf_term(q, z.x, z.y, Cx, Cy, Dx, Dy);
+        }
+      }
+      const real t = P.x * Cy + P.y * Cx;
+      fx += (real)nn.x * t;
+      fy += (real)nn.y * t;
+      fz += P.x * Dy + P.y * Dx;
+    }
   }
-  if (gridDim.y == 1) {
-    const int ti = s.type[i];
-    const real qm = (real)(a.k_e * a.charge[ti] * s.mass_inv[ti]);
-    s.ax[i] += qm * a.two_pi_over_L[0] * fx;
-    s.ay[i] += qm * a.two_pi_over_L[1] * fy;
-    s.az[i] += qm * a.two_pi_over_L[2] * fz;
-  } else {
-    const size_t n = (size_t)s.n, b = (size_t)blockIdx.y * 3 * n;
-    fpart[b + i] = fx;
-    fpart[b + n + i] = fy;
-    fpart[b + 2 * n + i] = fz;
-  }
-}
-
-template <typename real>
-__global__ void __launch_bounds__(256) k_kforce_reduce(DevState<real> s, KArgs<real> a, int nslices,
-                                                       const real *__restrict__ fpart) {
-  if (*s.err) return;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= s.n) return;
-  const size_t n = (size_t)s.n;
-  real fx = 0, fy = 0, fz = 0;
-  for (int sl = 0; sl < nslices; ++sl) {
-    const size_t b = (size_t)sl * 3 * n;
-    fx += fpart[b + i];
-    fy += fpart[b + n + i];
-    fz += fpart[b + 2 * n + i];
+  real *r = red + w * 3 * 32 + lane;
+  r[0] = fx;
+  r[32] = fy;
+  r[64] = fz;
+  __syncthreads();
+  if (w != 0 || !valid) return;
+  fx = fy = fz = 0;
+  for (int ww = 0; ww < W; ++ww) {
+    fx += red[ww * 96 + lane];
+    fy += red[ww * 96 + 32 + lane];
+    fz += red[ww * 96 + 64 + lane];
   }
   const int ti = s.type[i];
   const real qm = (real)(a.k_e * a.charge[ti] * s.mass_inv[ti]);
