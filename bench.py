@@ -324,7 +324,7 @@ def gpu_arm(args):
         sec["replicas_1024"] = replica_line(abi, W, torch, args.replica_steps)
         sec["adjoint_4000"] = adjoint_line(abi, W, torch)
         g1, m1 = force_error(abi, W.fcc_lattice(64, 0.8442, 0.72, seed=3, jitter=0.1))
-        g2, m2 = force_error(abi, s_ion)
+        g2, m2 = force_error(abi, W.config_ions_8000(seed=2))
         sec["force_rel_err_mixed_vs_fp64"] = {"lj_1m": {"global": g1, "max_over_rms": m1},
                                               "ions_8k": {"global": g2, "max_over_rms": m2}}
 
