@@ -276,10 +276,10 @@ class Simulation:
         return dict(zip(TH_KEYS, th.tolist()))
 
     def info(self) -> dict:
-        v = (ctypes.c_int64 * 13)()
-        self._check(self.L.cvr_get_info(self.h, v, 13))
+        v = (ctypes.c_int64 * 14)()
+        self._check(self.L.cvr_get_info(self.h, v, 14))
         keys = ["n", "ncx", "ncy", "ncz", "cap", "builds", "tpa", "nk", "R", "max_count", "err", "step",
-                "list_entries"]
+                "list_entries", "fixed_point"]
         return dict(zip(keys, list(v)))
 
     @property

@@ -98,6 +98,7 @@ struct cvr_ctx {
   int R = 2, nc[3] = {1, 1, 1}, ncells = 1;
   double w[3] = {1, 1, 1};
   int tpa = 1, log2_tpa = 0, cap = 0, n_pad = 0;
+  int fixed = 0;  // mixed form: fixed-point pair displacements (choose_fixed)
   // k space
   int nk = 0, nxy = 0, kM = 1, kp = 2;
   std::vector<int4> kint;
@@ -250,6 +251,8 @@ DevState<real> dev_state(cvr_ctx *c) {
     if (c->bc[d] == 1 && !(c->gc >= rl && c->gc <= 0.5 * c->L[d])) s.regular_images = 0;
   const double half_skin = 0.5 * (rl - c->cutoff);  // threshold_distance_sq = 0.25 (rl - rc)^2
   s.thr_sq = (float)(half_skin * half_skin);
+  s.fixed = c->fixed;
+  s.fx_scale = c->fixed ? std::ldexp(1.0, 32) / c->L[0] : 0.0;
   s.x = c->x;
   s.y = c->y;
   s.z = c->z;
@@ -347,6 +350,29 @@ int setup_cells(cvr_ctx *c) {
   return CVR_OK;
 }
 
+// Fixed-point pair displacements (mixed form): positions as u = r 2^32 / L
+// mod 2^32, the displacement of a listed pair as the wrapping int32
+// difference.  Taken when
+//  * the box is cubic (one scale for all axes, folded into the coefficients);
+//  * every listed pair stays below L/2 apart until the next build: at most
+//    rl + 2 (skin/2) = 2 rl - rc, since each atom moves at most skin/2 before
+//    the displacement trigger rebuilds the list (so the integer wrap is the
+//    image the list entry names; a non-periodic axis never wraps a listed pair);
+//  * the fixed-point step L / 2^32 is no coarser than the FP32 spacing of the
+//    cell-local coordinates it replaces (|r| < w/2 with w = L / nc: 2^-24 w),
+//    i.e. at most 256 cells per axis.
+// Otherwise the cell-local FP32 form is used.
+void choose_fixed(cvr_ctx *c) {
+  c->fixed = 0;
+  if (c->precision == CVR_PREC_FP64) return;
+  const double rl = c->cutoff * c->coef;
+  if (!(c->L[0] == c->L[1] && c->L[1] == c->L[2])) return;
+  if (!(0.5 * c->L[0] > (2.0 * rl - c->cutoff) * (1.0 + 1e-6))) return;
+  for (int d = 0; d < 3; ++d)
+    if (c->nc[d] > 256) return;
+  c->fixed = 1;
+}
+
 int upload_tables(cvr_ctx *c) {
   const int T = c->n_types;
   const bool dbl = c->precision == CVR_PREC_FP64;
@@ -392,11 +418,15 @@ int upload_tables(cvr_ctx *c) {
     if (int r = dalloc(c, (double4 **)&c->d_offs, S * S * S)) return r;
     CVR_CUDA(c, cudaMemcpyAsync(c->d_offs, od.data(), od.size() * sizeof(double4), cudaMemcpyHostToDevice, c->stream));
   } else {
+    // fixed-point form: lengths in units of h = L / 2^32 (r2 -> r2 / h^2; the
+    // force coefficient c -> c h^2, so c * du summed and times 1/h is the force)
+    const double h = c->fixed ? c->L[0] / std::ldexp(1.0, 32) : 1.0, h2 = h * h;
     std::vector<PairCoef<float>> cf(T * T);
     for (int t = 0; t < T * T; ++t) {
       const auto &p = cd[t];
-      cf[t] = PairCoef<float>{(float)p.sig2, (float)p.eps24, (float)p.eps48, (float)p.K, (float)p.rc2,
-                              (float)p.qq,   (float)p.e4,    (float)p.C0,    (float)p.C1, (float)p.lam};
+      cf[t] = PairCoef<float>{(float)(p.sig2 / h2), (float)p.eps24, (float)p.eps48, (float)(p.K * h2),
+                              (float)(p.rc2 > 0 ? p.rc2 / h2 : p.rc2),
+                              (float)(p.qq / h), (float)p.e4, (float)p.C0, (float)(p.C1 * h2), (float)p.lam};
     }
     std::vector<float4> of(S * S * S);
     for (int code = 0; code < S * S * S; ++code) {
@@ -572,30 +602,46 @@ void launch_build(cvr_ctx *c, int count_only) {
   c->launches += 8;
 }
 
-template <typename real, int TPA, bool LJ, bool EWR, bool EV, bool ONE_TYPE>
+template <typename real, int TPA, bool LJ, bool EWR, bool EV, bool ONE_TYPE, bool FIXED>
 void launch_pair_t(cvr_ctx *c) {
   DevState<real> s = dev_state<real>(c);
+  // fixed-point form: lengths in units of h = L / 2^32 (see upload_tables)
+  const double h = FIXED ? c->L[0] / std::ldexp(1.0, 32) : 1.0;
   EwrArgs<real> ew;
-  ew.alpha = (real)c->ewr_alpha;
-  ew.alpha2 = (real)(c->ewr_alpha * c->ewr_alpha);
-  ew.two_alpha_spi = (real)(2.0 * c->ewr_alpha * 0.56418958354775628695);  // 2 alpha / sqrt(pi)
-  ew.cut2 = (real)(c->ewr_cut >= 0 ? c->ewr_cut * c->ewr_cut : -1.0);
+  ew.alpha = (real)(c->ewr_alpha * h);
+  ew.alpha2 = (real)(c->ewr_alpha * c->ewr_alpha * h * h);
+  ew.two_alpha_spi = (real)(2.0 * c->ewr_alpha * 0.56418958354775628695 * h);  // 2 alpha / sqrt(pi)
+  ew.cut2 = (real)(c->ewr_cut >= 0 ? c->ewr_cut * c->ewr_cut / (h * h) : -1.0);
   const int blocks = grid_for(c->n * TPA, 128);
-  k_pair<real, TPA, LJ, EWR, EV, ONE_TYPE><<<blocks, 128, 0, c->stream>>>(
-      s, (const PairCoef<real> *)c->d_coef, (const typename V4<real>::t *)c->d_offs, ew, c->ignore_intra,
-      c->use_mol ? 1 : 0, c->ev_part);
+  k_pair<real, TPA, LJ, EWR, EV, ONE_TYPE, FIXED><<<blocks, 128, 0, c->stream>>>(
+      s, (const PairCoef<real> *)c->d_coef, (real)(1.0 / h), ew, c->ignore_intra, c->use_mol ? 1 : 0, c->ev_part);
   c->launches++;
+}
+
+template <typename real, bool LJ, bool EWR, bool EV, bool FIXED>
+void launch_pair_tpa_f(cvr_ctx *c) {
+  // one type pair, no molecule tests: LJ constants in registers
+  const bool one = LJ && !EWR && c->n_types == 1 && !c->use_mol;
+  switch (c->tpa) {
+    case 1:
+      one ? launch_pair_t<real, 1, LJ, EWR, EV, true, FIXED>(c) : launch_pair_t<real, 1, LJ, EWR, EV, false, FIXED>(c);
+      break;
+    case 8:
+      one ? launch_pair_t<real, 8, LJ, EWR, EV, true, FIXED>(c) : launch_pair_t<real, 8, LJ, EWR, EV, false, FIXED>(c);
+      break;
+    default:
+      one ? launch_pair_t<real, 32, LJ, EWR, EV, true, FIXED>(c)
+          : launch_pair_t<real, 32, LJ, EWR, EV, false, FIXED>(c);
+      break;
+  }
 }
 
 template <typename real, bool LJ, bool EWR, bool EV>
 void launch_pair_tpa(cvr_ctx *c) {
-  // one type pair, no molecule tests: LJ constants in registers
-  const bool one = LJ && !EWR && c->n_types == 1 && !c->use_mol;
-  switch (c->tpa) {
-    case 1: one ? launch_pair_t<real, 1, LJ, EWR, EV, true>(c) : launch_pair_t<real, 1, LJ, EWR, EV, false>(c); break;
-    case 8: one ? launch_pair_t<real, 8, LJ, EWR, EV, true>(c) : launch_pair_t<real, 8, LJ, EWR, EV, false>(c); break;
-    default: one ? launch_pair_t<real, 32, LJ, EWR, EV, true>(c) : launch_pair_t<real, 32, LJ, EWR, EV, false>(c); break;
+  if constexpr (sizeof(real) == 4) {
+    if (c->fixed) return launch_pair_tpa_f<real, LJ, EWR, EV, true>(c);
   }
+  launch_pair_tpa_f<real, LJ, EWR, EV, false>(c);
 }
 
 template <typename real>
@@ -1211,6 +1257,7 @@ int refresh(cvr_ctx *c) {
   if (!c->have_state || !c->nl_set) return CVR_OK;
   if (int r = setup_cells(c)) return r;
   if (int r = alloc_cells(c)) return r;
+  choose_fixed(c);
   if (int r = upload_tables(c)) return r;
   if (int r = setup_kspace(c)) return r;
   if (c->ewk_on && c->nk > 0) {
@@ -1714,9 +1761,9 @@ int cvr_get_info(const cvr_ctx *c, int64_t *out, int len) {
     cudaStreamSynchronize(c->stream);
     for (int v : cnt) entries += v;
   }
-  const int64_t v[13] = {c->n, c->nc[0], c->nc[1], c->nc[2], c->cap, flags[3], c->tpa, c->nk, c->R, flags[2],
-                         flags[1], c->step, entries};
-  for (int k = 0; k < len && k < 13; ++k) out[k] = v[k];
+  const int64_t v[14] = {c->n, c->nc[0], c->nc[1], c->nc[2], c->cap, flags[3], c->tpa, c->nk, c->R, flags[2],
+                         flags[1], c->step, entries, c->fixed};
+  for (int k = 0; k < len && k < 14; ++k) out[k] = v[k];
   return CVR_OK;
 }
 

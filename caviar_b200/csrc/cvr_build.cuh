@@ -228,10 +228,16 @@ __global__ void k_permute(DevState<real> s) {
   q.x = (real)loc[0];
   q.y = (real)loc[1];
   q.z = (real)loc[2];
-  if constexpr (sizeof(real) == 4)
+  if constexpr (sizeof(real) == 4) {
     q.w = __int_as_float(ty);
-  else
+    if (s.fixed) {
+      q.x = fixed_coord(p[0], s.fx_scale);
+      q.y = fixed_coord(p[1], s.fx_scale);
+      q.z = fixed_coord(p[2], s.fx_scale);
+    }
+  } else {
     q.w = (double)ty;
+  }
   s.x4[k] = q;
   s.xb[k] = make_float4((float)(p[0] - s.box.ctr[0]), (float)(p[1] - s.box.ctr[1]), (float)(p[2] - s.box.ctr[2]),
                         __int_as_float(cc[0]));

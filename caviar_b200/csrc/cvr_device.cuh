@@ -5,7 +5,9 @@
 //   x,y,z / vx,vy,vz   FP64 SoA positions (unwrapped between builds) and velocities
 //   ax,ay,az           real SoA accelerations (real = float in the mixed form, double in FP64)
 //   x4                 real4 cell-local position (r - centre of the atom's build cell) with the
-//                      type in .w: the only per-neighbour gather of the pair kernel (16 B mixed)
+//                      type in .w: the only per-neighbour gather of the pair kernel (16 B mixed);
+//                      in the mixed form's fixed-point mode (cubic box, see DevState::fixed) .x-.z
+//                      hold the bits of u = round(r * 2^32 / L) mod 2^32 instead
 //   xb                 float4 cell-local position at the last build (rebuild trigger)
 //   cell,id,type,mol   int per atom; id = the caller's atom index
 //   nlist              uint32 entries: atom j in bits 0-22, stencil offset dx+R, dy+R, dz+R
@@ -63,6 +65,9 @@ template <typename real> struct DevState {
   float thr_sq;                 // (skin/2)^2 rebuild threshold
   int regular_images;           // rl <= ghost_cutoff <= L/2 on every periodic axis: every image pair
                                 // clearly inside rl has its reference ghost (no per-pair image test)
+  int fixed;                    // mixed form only: x4 holds 32-bit fixed-point coordinates, so a pair's
+                                // minimum-image displacement is one wrapping int32 subtraction per axis
+  double fx_scale;              // 2^32 / L (fixed-point units per length; cubic box)
   double *x, *y, *z, *vx, *vy, *vz;
   real *ax, *ay, *az;
   typename V4<real>::t *x4;
@@ -84,5 +89,13 @@ template <typename real> struct DevState {
   double *mass_inv;  // per type (device)
   double *mass;      // per type (device)
 };
+
+// 32-bit fixed-point coordinate u = round(p * 2^32 / L) mod 2^32.  The
+// difference of two such coordinates, read as a signed int32, is the
+// minimum-image displacement in units of L / 2^32 whenever the true
+// displacement is below L / 2 (the wrap of the integer is the periodic wrap).
+__device__ __forceinline__ float fixed_coord(double p, double scale) {
+  return __uint_as_float((uint32_t)(unsigned long long)__double2ll_rn(p * scale));
+}
 
 }  // namespace cvr

@@ -158,15 +158,39 @@ __device__ __forceinline__ void pair_term(PairAcc<real> &A, real dx, real dy, re
   if (EV) A.vir -= (double)(c * r2);
 }
 
-template <typename real, int TPA, bool LJ, bool EWR, bool EV, bool ONE_TYPE>
+// Pair displacement r_j - r_i.  Cell-local form: (x4_j - x4_i) + the entry's
+// stencil offset.  Fixed-point form (FIXED, mixed precision only): the
+// wrapping int32 difference of the 32-bit coordinates, converted to float in
+// units of L / 2^32 (the pair kernel's coefficients are scaled to match).
+template <typename real, bool FIXED, typename real4>
+__device__ __forceinline__ void pair_disp(const real4 &xj, const real4 &xi, uint32_t e, const Stencil<real> &st,
+                                          real &dx, real &dy, real &dz) {
+  if constexpr (FIXED) {
+    (void)e;
+    (void)st;
+    dx = (real)(int)(__float_as_uint(xj.x) - __float_as_uint(xi.x));
+    dy = (real)(int)(__float_as_uint(xj.y) - __float_as_uint(xi.y));
+    dz = (real)(int)(__float_as_uint(xj.z) - __float_as_uint(xi.z));
+  } else {
+    real ox, oy, oz;
+    st.get(e, ox, oy, oz);
+    dx = (xj.x - xi.x) + ox;
+    dy = (xj.y - xi.y) + oy;
+    dz = (xj.z - xi.z) + oz;
+  }
+}
+
+// FIXED: x4 holds fixed-point coordinates; coef_g and ew are in units of
+// L / 2^32 and fscale = 2^32 / L turns the summed force back into length
+// units (the virial and energies come out unscaled).  Otherwise fscale = 1.
+template <typename real, int TPA, bool LJ, bool EWR, bool EV, bool ONE_TYPE, bool FIXED>
 __global__ void __launch_bounds__(128, CVR_PAIR_MINB) k_pair(DevState<real> s, const PairCoef<real> *__restrict__ coef_g,
-                                              const typename V4<real>::t *__restrict__ offs_g, EwrArgs<real> ew,
+                                              real fscale, EwrArgs<real> ew,
                                               int ignore_intra, int use_mol, double *__restrict__ partials) {
   using real4 = typename V4<real>::t;
   __shared__ PairCoef<real> coef[ONE_TYPE ? 1 : MAX_TYPES * MAX_TYPES];
   const int T = s.n_types;
   for (int t = threadIdx.x; t < (ONE_TYPE ? 1 : T * T); t += blockDim.x) coef[t] = coef_g[t];
-  (void)offs_g;
   Stencil<real> st;
   st.bias = (real)(sizeof(real) == 4 ? 8388608.0 : 4503599627370496.0) + (real)s.cells.R;
   st.wx = (real)s.cells.w[0];
@@ -206,10 +230,10 @@ __global__ void __launch_bounds__(128, CVR_PAIR_MINB) k_pair(DevState<real> s, c
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
           if (k + u < cnt) {
-            real ox, oy, oz;
-            st.get(e[u], ox, oy, oz);
-            pair_term<real, LJ, EWR, EV>(A, (xj[u].x - xi.x) + ox, (xj[u].y - xi.y) + oy, (xj[u].z - xi.z) + oz,
-                                         ONE_TYPE ? c1 : ci[type_of(xj[u].w)], sm[u], ignore_intra, ew);
+            real dx, dy, dz;
+            pair_disp<real, FIXED>(xj[u], xi, e[u], st, dx, dy, dz);
+            pair_term<real, LJ, EWR, EV>(A, dx, dy, dz, ONE_TYPE ? c1 : ci[type_of(xj[u].w)], sm[u], ignore_intra,
+                                         ew);
           }
         }
       }
@@ -233,10 +257,10 @@ __global__ void __launch_bounds__(128, CVR_PAIR_MINB) k_pair(DevState<real> s, c
         }
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-          real ox, oy, oz;
-          st.get(e[u], ox, oy, oz);
-          pair_term<real, LJ, EWR, EV>(A, (xj[u].x - xi.x) + ox, (xj[u].y - xi.y) + oy, (xj[u].z - xi.z) + oz,
-                                       ONE_TYPE ? c1 : ci[type_of(xj[u].w)], sm[u], ignore_intra, ew);
+          real dx, dy, dz;
+          pair_disp<real, FIXED>(xj[u], xi, e[u], st, dx, dy, dz);
+          pair_term<real, LJ, EWR, EV>(A, dx, dy, dz, ONE_TYPE ? c1 : ci[type_of(xj[u].w)], sm[u], ignore_intra,
+                                       ew);
         }
       }
       for (; k < cnt; k += TPA) {
@@ -245,10 +269,9 @@ __global__ void __launch_bounds__(128, CVR_PAIR_MINB) k_pair(DevState<real> s, c
         const int j0 = (int)(e0 & INDEX_MASK);
         const real4 xj0 = s.x4[j0];
         const bool sm0 = use_mol && (moli == s.mol[j0]);
-        real ox, oy, oz;
-        st.get(e0, ox, oy, oz);
-        pair_term<real, LJ, EWR, EV>(A, (xj0.x - xi.x) + ox, (xj0.y - xi.y) + oy, (xj0.z - xi.z) + oz,
-                                     ONE_TYPE ? c1 : ci[type_of(xj0.w)], sm0, ignore_intra, ew);
+        real dx, dy, dz;
+        pair_disp<real, FIXED>(xj0, xi, e0, st, dx, dy, dz);
+        pair_term<real, LJ, EWR, EV>(A, dx, dy, dz, ONE_TYPE ? c1 : ci[type_of(xj0.w)], sm0, ignore_intra, ew);
       }
     }
   }
@@ -259,7 +282,7 @@ __global__ void __launch_bounds__(128, CVR_PAIR_MINB) k_pair(DevState<real> s, c
     A.fz += __shfl_xor_sync(0xffffffffu, A.fz, o);
   }
   if (valid && lane == 0) {
-    const real mi = (real)s.mass_inv[ti];
+    const real mi = (real)s.mass_inv[ti] * fscale;
     s.ax[i] = A.fx * mi;
     s.ay[i] = A.fy * mi;
     s.az[i] = A.fz * mi;
@@ -687,6 +710,13 @@ __device__ __forceinline__ bool update_local(DevState<real> &s, int i, const dou
   q.x = (real)loc[0];
   q.y = (real)loc[1];
   q.z = (real)loc[2];
+  if constexpr (sizeof(real) == 4) {
+    if (s.fixed) {
+      q.x = fixed_coord(p[0], s.fx_scale);
+      q.y = fixed_coord(p[1], s.fx_scale);
+      q.z = fixed_coord(p[2], s.fx_scale);
+    }
+  }
   s.x4[i] = q;
   const float4 b = s.xb[i];
   const float ex = (float)(p[0] - s.box.ctr[0]) - b.x, ey = (float)(p[1] - s.box.ctr[1]) - b.y,

@@ -133,7 +133,10 @@ int cvr_set_langevin(cvr_ctx *c, double temperature, double friction, double kb,
                      uint64_t seed);
 
 /* CVR_PREC_MIXED (default) or CVR_PREC_FP64.  No reference counterpart
- * (the reference is FP64 only). */
+ * (the reference is FP64 only).  In the mixed form, a cubic box whose listed
+ * pairs stay below L/2 apart and that has at most 256 cells per axis gets
+ * fixed-point pair displacements: positions as round(r 2^32 / L) mod 2^32,
+ * the minimum image as a wrapping int32 difference (resolution L / 2^32). */
 int cvr_set_precision(cvr_ctx *ctx, int precision);
 
 /* Thermostat applied after the velocity update of each velocity-Verlet step,
@@ -201,7 +204,9 @@ int64_t cvr_launch_count(const cvr_ctx *ctx);     /* kernels launched by this co
 void *cvr_get_stream(const cvr_ctx *ctx);         /* the cudaStream_t the context launches on */
 /* out[0..len): n, cells x, y, z, list capacity per atom, list builds, lanes
  * per atom, k-vectors, stencil radius, largest neighbour count, error bits,
- * step, total list entries (index 12 costs a device-to-host copy). */
+ * step, total list entries (index 12 costs a device-to-host copy), 1 if the
+ * mixed form's pair kernel uses fixed-point displacements (cubic box, see
+ * cvr_set_precision). */
 int cvr_get_info(const cvr_ctx *ctx, int64_t *out, int len);
 
 /* Kernel timing: when on, CUDA events bracket every launch of the named

@@ -120,6 +120,37 @@ def test_lj4000_vs_oracle(cuda_lib, oracle_lib, prec):
     check_forces(acc, o.state()[2], prec)
 
 
+@pytest.mark.parametrize("stretch_z", [1.0, 1.07])
+def test_fixed_point_and_cell_local_forms(cuda_lib, oracle_lib, stretch_z):
+    """The mixed form takes fixed-point pair displacements in a cubic box and
+    the cell-local FP32 form otherwise; both stay within the mixed tolerance
+    of the FP64 oracle (forces, LJ energy, virial), and so does a 60-step run
+    (positions within 1e-5, forces 1e-4, FP64 form the comparison)."""
+    from caviar_b200 import workloads as W
+    s = W.fcc_lattice(10, 0.8442, 0.72, seed=4, jitter=0.1)
+    s.hi = np.asarray(s.lo, np.float64) + s.box * np.array([1.0, 1.0, stretch_z])
+    o = oracle_lib.Oracle(s)
+    o.setup()
+    sim = sim_for(cuda_lib, s, "mixed")
+    acc, th = sim.compute_forces()
+    assert sim.info()["fixed_point"] == (1 if stretch_z == 1.0 else 0)
+    assert np.array_equal(sim.pairs(), o.pairs())
+    check_forces(acc, o.state()[2], "mixed")
+    sc = o.energy()
+    assert abs(th["e_lj"] - sc["e_lj"]) <= 1e-5 * abs(sc["e_lj"])
+    assert abs(th["virial"] - sc["virial"]) <= 1e-5 * abs(sc["virial"])
+    ref = sim_for(cuda_lib, s, "fp64")
+    assert ref.info()["fixed_point"] == 0
+    sim.run(60)
+    ref.run(60)
+    p1, _, a1 = sim.state()
+    p2, _, a2 = ref.state()
+    dp = p1 - p2
+    dp -= s.box * np.round(dp / s.box)
+    assert np.abs(dp).max() < 1e-5
+    assert force_errors(a1, a2)[0] < 1e-4
+
+
 def test_deterministic(cuda_lib):
     from caviar_b200 import workloads as W
     s = W.config_lj_4000()
