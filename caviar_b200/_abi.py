@@ -23,12 +23,13 @@ REBUILD_DISPLACEMENT, REBUILD_REFERENCE, REBUILD_EVERY_STEP = 0, 1, 2
 TH_KEYS = ["step", "ke", "temperature", "e_lj", "e_ewald_r", "e_ewald_k", "e_self", "virial", "pressure", "builds"]
 N_THERMO = len(TH_KEYS)
 KT_PAIR, KT_KSPACE, KT_INTEGRATE, KT_BUILD = 0, 1, 2, 3
+LIST_AUTO, LIST_THREAD, LIST_WARP = 0, 1, 2
 
 # Every symbol declared in include/caviar_b200.h.
 EXPORTED = ["cvr_create", "cvr_destroy", "cvr_set_neighborlist", "cvr_set_lj", "cvr_set_ewald_r", "cvr_set_ewald_k",
             "cvr_set_integrator", "cvr_set_langevin", "cvr_set_berendsen", "cvr_set_nose_hoover",
             "cvr_clear_thermostat", "cvr_set_ewald_k_geometry",
-            "cvr_set_ewald_slab_correction", "cvr_set_precision", "cvr_set_state", "cvr_build_neighbors", "cvr_compute_forces",
+            "cvr_set_ewald_slab_correction", "cvr_set_precision", "cvr_set_list_kernel", "cvr_set_state", "cvr_build_neighbors", "cvr_compute_forces",
             "cvr_run", "cvr_get_state", "cvr_get_pairs", "cvr_get_sk", "cvr_get_scalars", "cvr_last_error",
             "cvr_launch_count", "cvr_get_stream", "cvr_get_info", "cvr_set_kernel_timing", "cvr_kernel_time",
             "cvr_structure_factor_noalloc", "cvr_casl_run_file", "cvr_batch_create", "cvr_batch_destroy",
@@ -69,6 +70,7 @@ def load(path: str = LIB_PATH):
     L.cvr_set_langevin.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                    ctypes.c_uint64]
     L.cvr_set_precision.argtypes = [vp, ctypes.c_int]
+    L.cvr_set_list_kernel.argtypes = [vp, ctypes.c_int]
     L.cvr_set_berendsen.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                     ctypes.c_double, ctypes.c_double]
     L.cvr_set_nose_hoover.argtypes = [vp, ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_double,
@@ -125,7 +127,8 @@ class Simulation:
     """One periodic system on one GPU, driven through the C ABI."""
 
     def __init__(self, system=None, *, precision: int = PREC_MIXED, policy: int = REBUILD_DISPLACEMENT,
-                 device: int = 0, lo=None, hi=None, bc=(1, 1, 1), mass=None, charge=None):
+                 device: int = 0, lo=None, hi=None, bc=(1, 1, 1), mass=None, charge=None,
+                 list_kernel: int = LIST_AUTO):
         self.L = load()
         if system is not None:
             lo, hi, bc, mass, charge = system.lo, system.hi, system.bc, system.mass, system.charge
@@ -142,6 +145,7 @@ class Simulation:
         self.h = h
         self.n = 0
         self._check(self.L.cvr_set_precision(self.h, precision))
+        self._check(self.L.cvr_set_list_kernel(self.h, list_kernel))
         if system is not None:
             self.configure(system, policy)
             self.set_state(system.pos, system.vel, system.type, system.mol)

@@ -99,6 +99,7 @@ struct cvr_ctx {
   double w[3] = {1, 1, 1};
   int tpa = 1, log2_tpa = 0, cap = 0, n_pad = 0;
   int fixed = 0;  // mixed form: fixed-point pair displacements (choose_fixed)
+  int list_kernel = CVR_LIST_AUTO;  // list search kernel (cvr_set_list_kernel)
   // k space
   int nk = 0, nxy = 0, kM = 1, kp = 2;
   std::vector<int4> kint;
@@ -582,6 +583,13 @@ int alloc_list(cvr_ctx *c, int cap) {
 }
 
 // ------------------------------------------------------------- launches
+// The list search kernel: by default small systems (a warp per atom fills
+// the GPU) take the warp kernel, the rest one thread per atom.
+int list_kernel_kind(const cvr_ctx *c) {
+  if (c->list_kernel != CVR_LIST_AUTO) return c->list_kernel;
+  return (c->n * 32 <= 4 * 1024 * 1024) ? CVR_LIST_WARP : CVR_LIST_THREAD;
+}
+
 template <typename real>
 void launch_build(cvr_ctx *c, int count_only) {
   Bracket br(c, CVR_KT_BUILD);
@@ -595,10 +603,12 @@ void launch_build(cvr_ctx *c, int count_only) {
   k_bin_scatter<real><<<grid_for(n, 256), 256, 0, c->stream>>>(s);
   k_rank<real><<<grid_for(n, 256), 256, 0, c->stream>>>(s);
   k_permute<real><<<grid_for(std::max<int64_t>(n, c->ncells), 256), 256, 0, c->stream>>>(s);
-  if ((int64_t)n * 32 <= 4 * 1024 * 1024)  // small systems: one warp per atom fills the GPU
+  const int kind = list_kernel_kind(c);
+  if (kind == CVR_LIST_WARP) {
     k_build_list_warp<real><<<grid_for((int64_t)n * 32, 128), 128, 0, c->stream>>>(s, count_only, c->log2_tpa);
-  else
+  } else {
     k_build_list<real><<<grid_for(n, 128), 128, 0, c->stream>>>(s, count_only, c->log2_tpa);
+  }
   c->launches += 8;
 }
 
@@ -1581,6 +1591,13 @@ int cvr_clear_thermostat(cvr_ctx *c) {
   if (!c) return CVR_ERR_INVALID;
   c->tstat = ThermostatArgs{};
   c->epoch++;
+  return CVR_OK;
+}
+
+int cvr_set_list_kernel(cvr_ctx *c, int kind) {
+  if (!c) return CVR_ERR_INVALID;
+  if (kind < CVR_LIST_AUTO || kind > CVR_LIST_WARP) return fail(c, CVR_ERR_INVALID, "unknown list kernel");
+  c->list_kernel = kind;
   return CVR_OK;
 }
 

@@ -213,11 +213,16 @@ __global__ void __launch_bounds__(128, CVR_PAIR_MINB) k_pair(DevState<real> s, c
     PairCoef<real> c1;
     if (ONE_TYPE) c1 = coef[0];
     if (TPA == 1) {
-      // one lane per atom: entries in quads, one 16-byte load per four
+      // one lane per atom: entries in quads, one 16-byte load per four; the
+      // next quad is loaded before this one's neighbours are gathered, so
+      // the list stream's HBM latency overlaps the gathers and the math
       const uint4 *q4 = reinterpret_cast<const uint4 *>(s.nlist) + i;
+      uint4 nxt = make_uint4(0u, 0u, 0u, 0u);
+      if (cnt > 0) nxt = __ldcs(q4);
       for (int k = 0; k < cnt; k += 4) {
-        const uint4 e4 = __ldcs(q4);
+        const uint4 e4 = nxt;
         q4 += s.n_pad;
+        if (k + 4 < cnt) nxt = __ldcs(q4);
         const uint32_t e[4] = {e4.x, e4.y, e4.z, e4.w};
         real4 xj[4];
         bool sm[4];

@@ -132,6 +132,17 @@ int cvr_set_integrator(cvr_ctx *ctx, double dt, double k_b);
 int cvr_set_langevin(cvr_ctx *c, double temperature, double friction, double kb, double kbt, int rng,
                      uint64_t seed);
 
+/* Verlet-list search kernel (a tuning and testing knob; both kernels build
+ * the same pair set, Neighborlist::update_verlet_list_from_cell_list,
+ * neighborlist.cpp:515-573): CVR_LIST_AUTO picks by system size (a warp per
+ * atom up to 131072 atoms, else a thread per atom), CVR_LIST_THREAD one
+ * thread per atom, CVR_LIST_WARP one warp per atom.  Takes effect at the
+ * next list build. */
+#define CVR_LIST_AUTO 0
+#define CVR_LIST_THREAD 1
+#define CVR_LIST_WARP 2
+int cvr_set_list_kernel(cvr_ctx *ctx, int kind);
+
 /* CVR_PREC_MIXED (default) or CVR_PREC_FP64.  No reference counterpart
  * (the reference is FP64 only).  In the mixed form, a cubic box whose listed
  * pairs stay below L/2 apart and that has at most 256 cells per axis gets

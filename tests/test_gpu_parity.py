@@ -151,6 +151,64 @@ def test_fixed_point_and_cell_local_forms(cuda_lib, oracle_lib, stretch_z):
     assert force_errors(a1, a2)[0] < 1e-4
 
 
+LIST_KERNELS = ["thread", "warp"]
+
+
+def _lattice(nc, bc=(1, 1, 1), seed=5):
+    from caviar_b200 import workloads as W
+    s = W.fcc_lattice(nc, 0.8442, 0.72, seed=seed, jitter=0.1)
+    s.bc = bc
+    return s
+
+
+@pytest.mark.parametrize("bc", [(1, 1, 1), (1, 0, 1)])
+def test_list_kernels_same_pair_set(cuda_lib, oracle_lib, bc):
+    """Both list-search kernels (one thread per atom, one warp per atom)
+    build the reference's pair set, and the FP64 forces from their lists
+    agree to rounding."""
+    s = _lattice(10, bc)
+    o = oracle_lib.Oracle(s)
+    o.setup()
+    ref = o.pairs()
+    acc = {}
+    for name in LIST_KERNELS:
+        kind = getattr(cuda_lib, "LIST_" + name.upper())
+        sim = cuda_lib.Simulation(s, precision=cuda_lib.PREC_FP64, list_kernel=kind)
+        a, _ = sim.compute_forces()
+        assert np.array_equal(sim.pairs(), ref), name
+        acc[name] = a
+        sim.close()
+    for name in LIST_KERNELS[1:]:
+        assert force_errors(acc[name], acc["thread"])[0] < 1e-13
+
+
+def test_list_kernels_large_system_and_run(cuda_lib):
+    """186,624 atoms (the size class where one thread per atom is the
+    default): the warp kernel gives the same pair set at setup, and after a
+    50-step run with several rebuilds the trajectories agree to FP32
+    rounding and the lists to pairs within rounding of rl."""
+    s = _lattice(36)
+    out = {}
+    for name in ("thread", "warp"):
+        kind = getattr(cuda_lib, "LIST_" + name.upper())
+        sim = cuda_lib.Simulation(s, precision=cuda_lib.PREC_MIXED, list_kernel=kind)
+        sim.build_neighbors(True)
+        p0 = sim.pairs()
+        sim.run(50)
+        assert sim.info()["builds"] >= 3
+        sim.build_neighbors(True)
+        out[name] = (p0, sim.pairs(), sim.state())
+        sim.close()
+    assert np.array_equal(out["thread"][0], out["warp"][0])
+    pa, pb = out["thread"][2][0], out["warp"][2][0]
+    dp = pa - pb
+    dp -= s.box * np.round(dp / s.box)
+    assert np.abs(dp).max() < 1e-5
+    # after identical-to-rounding runs the two lists may differ only by pairs within rounding of rl
+    a, b = out["thread"][1], out["warp"][1]
+    assert abs(len(a) - len(b)) <= 1e-5 * len(a)
+
+
 def test_deterministic(cuda_lib):
     from caviar_b200 import workloads as W
     s = W.config_lj_4000()
