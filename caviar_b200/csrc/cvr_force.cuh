@@ -17,6 +17,7 @@
 // one pass over the list.  Energies and virial are FP64 block sums.
 #pragma once
 #include "cvr_device.cuh"
+#include <type_traits>
 
 // List entries each pair-kernel lane has in flight, and the minimum resident
 // blocks the pair kernel is compiled for.
@@ -207,7 +208,8 @@ __global__ void __launch_bounds__(128, CVR_PAIR_MINB) k_pair(DevState<real> s, c
   if (valid) {
     const real4 xi = s.x4[i];
     ti = type_of(xi.w);
-    const int moli = use_mol ? s.mol[i] : 0;
+    const bool um = !ONE_TYPE && use_mol;  // the single-type instantiation runs without molecules
+    const int moli = um ? s.mol[i] : 0;
     const int cnt = s.ncount[i];
     const PairCoef<real> *ci = coef + (ONE_TYPE ? 0 : ti * T);
     PairCoef<real> c1;
@@ -215,33 +217,40 @@ __global__ void __launch_bounds__(128, CVR_PAIR_MINB) k_pair(DevState<real> s, c
     if (TPA == 1) {
       // one lane per atom: entries in quads, one 16-byte load per four; the
       // next quad is loaded before this one's neighbours are gathered, so
-      // the list stream's HBM latency overlaps the gathers and the math
+      // the list stream's HBM latency overlaps the gathers and the math.
+      // Full quads need no per-entry count test; the last, partial one does.
       const uint4 *q4 = reinterpret_cast<const uint4 *>(s.nlist) + i;
       uint4 nxt = make_uint4(0u, 0u, 0u, 0u);
       if (cnt > 0) nxt = __ldcs(q4);
-      for (int k = 0; k < cnt; k += 4) {
-        const uint4 e4 = nxt;
-        q4 += s.n_pad;
-        if (k + 4 < cnt) nxt = __ldcs(q4);
+      const int full = cnt & ~3;
+      auto quad = [&](const uint4 &e4, int nv, auto check) {
+        constexpr bool CHECK = decltype(check)::value;
         const uint32_t e[4] = {e4.x, e4.y, e4.z, e4.w};
         real4 xj[4];
         bool sm[4];
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
-          const int j = (k + u < cnt) ? (int)(e[u] & INDEX_MASK) : i;
+          const int j = (!CHECK || u < nv) ? (int)(e[u] & INDEX_MASK) : i;
           xj[u] = s.x4[j];
-          sm[u] = use_mol && (moli == s.mol[j]);
+          sm[u] = um && (moli == s.mol[j]);
         }
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
-          if (k + u < cnt) {
+          if (!CHECK || u < nv) {
             real dx, dy, dz;
             pair_disp<real, FIXED>(xj[u], xi, e[u], st, dx, dy, dz);
             pair_term<real, LJ, EWR, EV>(A, dx, dy, dz, ONE_TYPE ? c1 : ci[type_of(xj[u].w)], sm[u], ignore_intra,
                                          ew);
           }
         }
+      };
+      for (int k = 0; k < full; k += 4) {
+        const uint4 e4 = nxt;
+        q4 += s.n_pad;
+        if (k + 4 < cnt) nxt = __ldcs(q4);
+        quad(e4, 4, std::false_type{});
       }
+      if (cnt > full) quad(nxt, cnt - full, std::true_type{});
     } else {
       const size_t stride = (size_t)s.n_pad * TPA;
       const uint32_t *row = s.nlist + (size_t)i * TPA + lane;
@@ -258,7 +267,7 @@ __global__ void __launch_bounds__(128, CVR_PAIR_MINB) k_pair(DevState<real> s, c
         for (int u = 0; u < U; ++u) {
           const int j = (int)(e[u] & INDEX_MASK);
           xj[u] = s.x4[j];
-          sm[u] = use_mol && (moli == s.mol[j]);
+          sm[u] = um && (moli == s.mol[j]);
         }
 #pragma unroll
         for (int u = 0; u < U; ++u) {
@@ -273,7 +282,7 @@ __global__ void __launch_bounds__(128, CVR_PAIR_MINB) k_pair(DevState<real> s, c
         row += stride;
         const int j0 = (int)(e0 & INDEX_MASK);
         const real4 xj0 = s.x4[j0];
-        const bool sm0 = use_mol && (moli == s.mol[j0]);
+        const bool sm0 = um && (moli == s.mol[j0]);
         real dx, dy, dz;
         pair_disp<real, FIXED>(xj0, xi, e0, st, dx, dy, dz);
         pair_term<real, LJ, EWR, EV>(A, dx, dy, dz, ONE_TYPE ? c1 : ci[type_of(xj0.w)], sm0, ignore_intra, ew);
