@@ -22,6 +22,13 @@
 #include "cvr_device.cuh"
 #include "cvr_force.cuh"
 
+// Stencil radius in cells: cells are at least rl / R wide, so every pair
+// within rl is at most R cells apart on each axis (R = 1 was measured: the
+// pair kernel gathers better, the list search costs more, the step is slower).
+#ifndef CVR_STENCIL_R
+#define CVR_STENCIL_R 2
+#endif
+
 using namespace cvr;
 
 namespace {
@@ -95,17 +102,18 @@ struct cvr_ctx {
   int64_t n = 0;
   bool have_state = false, list_valid = false, setup_done = false, use_mol = false;
   int64_t step = 0;
-  int R = 2, nc[3] = {1, 1, 1}, ncells = 1;
+  int R = CVR_STENCIL_R, nc[3] = {1, 1, 1}, ncells = 1;
   double w[3] = {1, 1, 1};
   int tpa = 1, log2_tpa = 0, cap = 0, n_pad = 0;
   int fixed = 0;  // mixed form: fixed-point pair displacements (choose_fixed)
+  bool refreshed = false;  // refresh() has run for the current settings and atom count
   int list_kernel = CVR_LIST_AUTO;  // list search kernel (cvr_set_list_kernel)
   // k space
   int nk = 0, nxy = 0, kM = 1, kp = 2;
   std::vector<int4> kint;
   std::vector<double> fk;
   std::vector<int2> kxy, kpm;
-  double e_self = 0, total_mass = 0;
+  double e_self = 0, total_mass = 0, q2_sum = 0;  // q2_sum = sum of q_i^2 over the atoms
   // device memory
   std::vector<std::pair<void **, size_t>> atom_bufs;
   // per atom
@@ -1263,8 +1271,16 @@ int ensure_ready(cvr_ctx *c) {
 }
 
 // Re-derive everything that depends on the settings (cells, tables, k-set).
+// Ewald self energy -(alpha / sqrt(pi)) k_e sum q^2 (electrostatic_ewald_k/energy.cpp:49).
+double self_energy(const cvr_ctx *c) {
+  return c->ewk_on ? -0.56418958354775628695 * c->ewk_alpha * c->q2_sum * c->ewk_ke : 0.0;
+}
+
 int refresh(cvr_ctx *c) {
   if (!c->have_state || !c->nl_set) return CVR_OK;
+  c->epoch++;  // settings may change what the step graphs bake in
+  c->refreshed = false;
+  c->e_self = self_energy(c);
   if (int r = setup_cells(c)) return r;
   if (int r = alloc_cells(c)) return r;
   choose_fixed(c);
@@ -1293,6 +1309,7 @@ int refresh(cvr_ctx *c) {
   }
   c->list_valid = false;
   c->setup_done = false;
+  c->refreshed = true;
   return CVR_OK;
 }
 
@@ -1618,6 +1635,7 @@ int cvr_set_state(cvr_ctx *c, int64_t n, const double *pos, const double *vel, c
     if (type[i] < 0 || type[i] >= c->n_types) return fail(c, CVR_ERR_INVALID, "atom type out of range");
   cudaSetDevice(c->device);
   if (n != c->n || !c->x) {
+    c->refreshed = false;
     if (int r = alloc_atoms(c, n)) return r;
     if (int r = dalloc(c, &c->stage, 9 * (size_t)n)) return r;
     c->cap = 0;
@@ -1631,14 +1649,18 @@ int cvr_set_state(cvr_ctx *c, int64_t n, const double *pos, const double *vel, c
   CVR_CUDA(c, cudaMemcpyAsync(c->stage_i, type, (size_t)n * sizeof(int32_t), cudaMemcpyHostToDevice, c->stream));
   if (mol) CVR_CUDA(c, cudaMemcpyAsync(c->stage_i + n, mol, (size_t)n * sizeof(int32_t), cudaMemcpyHostToDevice, c->stream));
   c->have_state = true;
+  const bool mol_changed = (mol != nullptr) != c->use_mol;
   c->use_mol = mol != nullptr;
   double q2 = 0, mt = 0;
   for (int64_t i = 0; i < n; ++i) {
     q2 += c->charge[type[i]] * c->charge[type[i]];
     mt += c->mass[type[i]];
   }
+  // the step graphs bake these in (thermo kernel, pair-kernel choice)
+  if (mol_changed || mt != c->total_mass || q2 != c->q2_sum) c->epoch++;
   c->total_mass = mt;
-  c->e_self = c->ewk_on ? -0.56418958354775628695 * c->ewk_alpha * q2 * c->ewk_ke : 0.0;  // energy.cpp:49
+  c->q2_sum = q2;
+  c->e_self = self_energy(c);
   if (c->precision == CVR_PREC_FP64) {
     DevState<double> s = dev_state<double>(c);
     k_scatter_state<double><<<grid_for(n, 256), 256, 0, c->stream>>>(s, c->stage, vel ? c->stage + 3 * n : nullptr,
@@ -1651,9 +1673,14 @@ int cvr_set_state(cvr_ctx *c, int64_t n, const double *pos, const double *vel, c
   c->launches++;
   CVR_CUDA(c, cudaMemsetAsync(c->flags, 0, 4 * sizeof(int), c->stream));
   c->step = 0;
-  if (int r = refresh(c)) return r;
-  // e_self depends on the k-space settings; recompute after refresh
-  c->e_self = c->ewk_on ? -0.56418958354775628695 * c->ewk_alpha * q2 * c->ewk_ke : 0.0;
+  if (!c->refreshed || mol_changed) {
+    if (int r = refresh(c)) return r;
+  } else {
+    // same atom count and settings: cells, tables and buffers stay (and so
+    // do the step graphs); only the list and the forces are redone
+    c->list_valid = false;
+    c->setup_done = false;
+  }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return fail(c, CVR_ERR_CUDA, cudaGetErrorString(e));
   return CVR_OK;

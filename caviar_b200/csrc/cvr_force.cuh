@@ -121,10 +121,22 @@ template <typename real> struct EwrArgs {
 // EV adds energies + virial (FP64 per thread, FP64 block sums into
 // partials[block*3 + {e_lj, e_ewr, virial}]).  Entries are unrolled by
 // CVR_PAIR_UNROLL so that several neighbour gathers are in flight per lane.
+// Energies and virial: each group of entries (a quad, or one unrolled round)
+// is summed in `real`, then added to the FP64 per-atom totals (ev_flush),
+// one conversion per group instead of per pair.
 template <typename real> struct PairAcc {
   real fx, fy, fz;
   double e_lj, e_ew, vir;
+  real g_lj, g_ew, g_vir;
 };
+
+template <typename real>
+__device__ __forceinline__ void ev_flush(PairAcc<real> &A) {
+  A.e_lj += (double)A.g_lj;
+  A.e_ew += (double)A.g_ew;
+  A.vir += (double)A.g_vir;
+  A.g_lj = A.g_ew = A.g_vir = (real)0;
+}
 
 template <typename real, bool LJ, bool EWR, bool EV>
 __device__ __forceinline__ void pair_term(PairAcc<real> &A, real dx, real dy, real dz, const PairCoef<real> &pc,
@@ -139,7 +151,7 @@ __device__ __forceinline__ void pair_term(PairAcc<real> &A, real dx, real dy, re
     const bool in = (r2 <= pc.rc2) && !(same_mol && ignore_intra);
     const real cl = r2i * s6 * (pc.eps24 - pc.eps48 * s6) + pc.K;
     c = in ? cl : (real)0;
-    if (EV && in) A.e_lj += (double)(pc.e4 * (s6 * s6 - s6) + pc.C1 * r2 + pc.C0);
+    if (EV && in) A.g_lj += pc.e4 * (s6 * s6 - s6) + pc.C1 * r2 + pc.C0;
   }
   if (EWR) {
     // electrostatic_ewald_r.cpp:179-198: every list pair, coincident skipped
@@ -150,13 +162,13 @@ __device__ __forceinline__ void pair_term(PairAcc<real> &A, real dx, real dy, re
       const real sv = (ew.two_alpha_spi * fast_exp(-ew.alpha2 * r2) + erfcv * rinv) * (rinv * rinv);
       const real lam = same_mol ? pc.lam : (real)1;
       c -= lam * pc.qq * sv;
-      if (EV) A.e_ew += (double)(lam * pc.qq * erfcv * rinv);
+      if (EV) A.g_ew += lam * pc.qq * erfcv * rinv;
     }
   }
   A.fx += c * dx;
   A.fy += c * dy;
   A.fz += c * dz;
-  if (EV) A.vir -= (double)(c * r2);
+  if (EV) A.g_vir -= c * r2;
 }
 
 // Pair displacement r_j - r_i.  Cell-local form: (x4_j - x4_i) + the entry's
@@ -203,7 +215,7 @@ __global__ void __launch_bounds__(128, CVR_PAIR_MINB) k_pair(DevState<real> s, c
   const int gid = blockIdx.x * blockDim.x + threadIdx.x;
   const int i = gid / TPA, lane = gid % TPA;
   const bool valid = i < s.n;
-  PairAcc<real> A{0, 0, 0, 0.0, 0.0, 0.0};
+  PairAcc<real> A{0, 0, 0, 0.0, 0.0, 0.0, 0, 0, 0};
   int ti = 0;
   if (valid) {
     const real4 xi = s.x4[i];
@@ -243,6 +255,7 @@ __global__ void __launch_bounds__(128, CVR_PAIR_MINB) k_pair(DevState<real> s, c
                                          ew);
           }
         }
+        if (EV) ev_flush(A);
       };
       for (int k = 0; k < full; k += 4) {
         const uint4 e4 = nxt;
@@ -276,6 +289,7 @@ __global__ void __launch_bounds__(128, CVR_PAIR_MINB) k_pair(DevState<real> s, c
           pair_term<real, LJ, EWR, EV>(A, dx, dy, dz, ONE_TYPE ? c1 : ci[type_of(xj[u].w)], sm[u], ignore_intra,
                                        ew);
         }
+        if (EV) ev_flush(A);
       }
       for (; k < cnt; k += TPA) {
         const uint32_t e0 = __ldcs(row);
@@ -287,6 +301,7 @@ __global__ void __launch_bounds__(128, CVR_PAIR_MINB) k_pair(DevState<real> s, c
         pair_disp<real, FIXED>(xj0, xi, e0, st, dx, dy, dz);
         pair_term<real, LJ, EWR, EV>(A, dx, dy, dz, ONE_TYPE ? c1 : ci[type_of(xj0.w)], sm0, ignore_intra, ew);
       }
+      if (EV) ev_flush(A);
     }
   }
 #pragma unroll
