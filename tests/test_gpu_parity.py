@@ -209,6 +209,26 @@ def test_list_kernels_large_system_and_run(cuda_lib):
     assert abs(len(a) - len(b)) <= 1e-5 * len(a)
 
 
+@pytest.mark.parametrize("name", ["lj500", "ions500"])
+def test_set_state_again_matches_fresh_context(cuda_lib, name):
+    """A context whose state is set again (same atom count and settings:
+    cells, tables and step graphs are kept) continues exactly like a fresh
+    context given that state: trajectories and thermo (self energy
+    included) bit-identical."""
+    s, _ = load_ref_fixture(name)
+    a = sim_for(cuda_lib, s, "mixed")
+    a.run(25, 25)
+    a.set_state(s.pos, s.vel, s.type, s.mol)
+    ta = a.run(25, 25)
+    b = sim_for(cuda_lib, s, "mixed")
+    tb = b.run(25, 25)
+    for x, y in zip(a.state(), b.state()):
+        assert np.array_equal(x, y)
+    assert np.array_equal(ta, tb)
+    if s.ewald_k is not None:
+        assert ta[0, cuda_lib.TH_KEYS.index("e_self")] != 0.0
+
+
 def test_deterministic(cuda_lib):
     from caviar_b200 import workloads as W
     s = W.config_lj_4000()
