@@ -332,6 +332,76 @@ __global__ void __launch_bounds__(128) k_build_list_warp(DevState<real> s, int c
   const int nc0 = s.cells.nc[0], nc1 = s.cells.nc[1], nc2 = s.cells.nc[2];
   const unsigned lt = (1u << lane) - 1u;
   int cnt = 0;
+  if (nc0 >= S) {
+    // Row mode: the stencil's S*S rows (dz, dy), each at most three
+    // contiguous atom ranges (the sx = -1, 0, +1 pieces of the unwrapped x
+    // range [cx-R, cx+R]).  The lanes first load every piece's range in one
+    // parallel round trip, then the warp sweeps the pieces in stencil order,
+    // 32 candidates at a time (the same entries, in the same order, as the
+    // cell-by-cell sweep below).
+    constexpr int KP = (3 * (2 * MAX_STENCIL_R + 1) * (2 * MAX_STENCIL_R + 1) + 31) / 32;
+    const int P = 3 * S * S;
+    int pst[KP], plen[KP];
+#pragma unroll
+    for (int k = 0; k < KP; ++k) {
+      const int p = 32 * k + lane;
+      pst[k] = 0;
+      plen[k] = 0;
+      if (p < P) {
+        const int r = p / 3, sx = p % 3 - 1;
+        const int dz = r / S - R, dy = r % S - R;
+        const int sz = floor_div(cz + dz, nc2), sy = floor_div(cy + dy, nc1);
+        int ua = cx - R, ub = cx + R;
+        if (sx < 0) ub = min(ub, -1);
+        if (sx == 0) {
+          ua = max(ua, 0);
+          ub = min(ub, nc0 - 1);
+        }
+        if (sx > 0) ua = max(ua, nc0);
+        const bool live = ua <= ub && (sz == 0 || s.box.bc[2]) && (sy == 0 || s.box.bc[1]) && (sx == 0 || s.box.bc[0]);
+        if (live) {
+          const int rowbase = nc0 * (cy + dy - sy * nc1 + nc1 * (cz + dz - sz * nc2));
+          pst[k] = s.cell_start[rowbase + ua - sx * nc0];
+          plen[k] = s.cell_start[rowbase + ub - sx * nc0 + 1] - pst[k];
+        }
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < KP; ++k) {
+      for (int src = 0; src < 32; ++src) {
+        const int p = 32 * k + src;
+        if (p >= P) break;
+        const int len = __shfl_sync(0xffffffffu, plen[k], src);
+        if (len == 0) continue;
+        const int jb = __shfl_sync(0xffffffffu, pst[k], src);
+        const int r = p / 3, sx = p % 3 - 1;
+        const int dz = r / S - R, dy = r % S - R;
+        const int sz = floor_div(cz + dz, nc2), sy = floor_div(cy + dy, nc1);
+        const float bx = sx * s.box.Lf[0] - xi.x, by = sy * s.box.Lf[1] - xi.y, bz = sz * s.box.Lf[2] - xi.z;
+        const bool shifted = (sx | sy | sz) != 0;
+        const bool fast_ok = !shifted || s.regular_images;
+        const int self = shifted ? -1 : i;
+        const int dxc = sx * nc0 - cx;  // dx = cell_x(j) + dxc
+        for (int base = 0; base < len; base += 32) {
+          const int j = jb + base + lane;
+          bool ok = false;
+          float4 q = xi;
+          if (base + lane < len && j != self) {
+            q = s.xb[j];
+            const float ex = q.x + bx, ey = q.y + by, ez = q.z + bz;
+            const float d2 = ex * ex + ey * ey + ez * ez;
+            if (d2 < s.rl_sq_hi) ok = (d2 <= s.rl_sq_lo && fast_ok) || in_list_slow(s, pi, gi, j, d2, sx, sy, sz);
+          }
+          const unsigned m = __ballot_sync(0xffffffffu, ok);
+          if (ok && !count_only) {
+            const int k2 = cnt + __popc(m & lt);
+            if (k2 < s.cap) row[list_slot(k2, log2_tpa, stride)] = list_entry(j, __float_as_int(q.w) + dxc, dy, dz, R, S);
+          }
+          cnt += __popc(m);
+        }
+      }
+    }
+  } else
   for (int dz = -R; dz <= R; ++dz) {
     const int sz = floor_div(cz + dz, nc2);
     if (sz != 0 && !s.box.bc[2]) continue;
