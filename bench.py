@@ -48,17 +48,53 @@ def dist_env():
 
 
 class Clocks:
-    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+    """SM clocks and clock-event (throttle) reasons sampled during a region:
+    NVML polled every 20 ms from a thread (read-only queries), else
+    nvidia-smi at its 200 ms minimum."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, index: int):
         self.index = index
         self.p = None
         self.f = None
+        self.samples = None
+        self.mx = None
+        self.stop = None
+        self.t = None
+
+    def _nvml_start(self):
+        import threading
+        import pynvml
+        pynvml.nvmlInit()
+        h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+        self.mx = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+        bits = [pynvml.nvmlClocksEventReasonHwSlowdown, pynvml.nvmlClocksEventReasonHwThermalSlowdown,
+                pynvml.nvmlClocksEventReasonSwThermalSlowdown, pynvml.nvmlClocksEventReasonSwPowerCap]
+        self.samples = []
+        self.stop = threading.Event()
+
+        def poll():
+            while not self.stop.is_set():
+                try:
+                    sm = float(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM))
+                    r = int(pynvml.nvmlDeviceGetCurrentClocksEventReasons(h))
+                    self.samples.append((sm, [nm for nm, bit in zip(self.NAMES, bits) if r & bit]))
+                except Exception:
+                    pass
+                self.stop.wait(0.02)
+
+        self.t = threading.Thread(target=poll, daemon=True)
+        self.t.start()
 
     def __enter__(self):
+        try:
+            self._nvml_start()
+            return self
+        except Exception:
+            self.samples = None
         try:
             self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
@@ -69,6 +105,9 @@ class Clocks:
         return self
 
     def __exit__(self, *a):
+        if self.t:
+            self.stop.set()
+            self.t.join(timeout=2)
         if self.p:
             self.p.terminate()
             try:
@@ -77,6 +116,12 @@ class Clocks:
                 self.p.kill()
 
     def summary(self):
+        if self.samples is not None:
+            if not self.samples:
+                return None
+            reasons = sorted({nm for _, rs in self.samples for nm in rs})
+            return {"sm_mhz": statistics.median([sm for sm, _ in self.samples]), "sm_max_mhz": self.mx,
+                    "reasons": reasons, "samples": len(self.samples), "source": "nvml, 20 ms"}
         if not self.f:
             return None
         try:
@@ -90,7 +135,6 @@ class Clocks:
             except Exception:
                 pass
         sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for r in rows:
             r = [x.strip() for x in r]
             try:
@@ -98,12 +142,13 @@ class Clocks:
                 mx = float(r[2])
             except (ValueError, IndexError):
                 continue
-            for k, nm in enumerate(names):
+            for k, nm in enumerate(self.NAMES):
                 if len(r) > 5 + k and r[5 + k].lower() == "active":
                     reasons.add(nm)
         if not sm:
             return None
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm),
+                "source": "nvidia-smi, 200 ms"}
 
 
 def measured_peaks():
@@ -437,7 +482,7 @@ def reference_arm(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=500)
+    ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--cpu-budget", type=float, default=20.0)
