@@ -297,7 +297,7 @@ def gpu_arm(args):
     if world > 1:
         import torch.distributed as td
         torch.cuda.set_device(local)
-        td.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+        td.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
         dist = td
     else:
         torch.cuda.set_device(0)
@@ -354,9 +354,11 @@ def gpu_arm(args):
     d2h = n * (3 * 8 + 3 * 8)
     sim2.close()
 
-    # --- secondary lines: FP64 form, 8K ions, force error (rank 0 only)
+    # --- secondary lines (FP64 form, 8K ions, replicas, adjoint, force error)
+    # and the CPU baseline: single-GPU runs only (under torchrun the other
+    # ranks would wait for them at the closing barrier)
     sec = {}
-    if rank == 0:
+    if world == 1:
         sim64 = abi.Simulation(s_lj, precision=abi.PREC_FP64, device=local)
         ms64 = time_run(sim64, torch, steps, warmup)
         sec["lj_1m_fp64"] = {"value": n * steps / (ms64 / 1e3), "ms_per_step": ms64 / steps}
@@ -367,7 +369,7 @@ def gpu_arm(args):
         sec["mixed_over_fp64"] = {"lj_1m": value / world / sec["lj_1m_fp64"]["value"],
                                   "ions_8k": ion["mixed"]["value"] / ion["fp64"]["value"]}
         sec["replicas_1024"] = replica_line(abi, W, torch, args.replica_steps)
-        sec["adjoint_4000"] = adjoint_line(abi, W, torch)
+        sec["adjoint_4000"] = adjoint_line(abi, W, torch, args.adjoint_steps)
         g1, m1 = force_error(abi, W.fcc_lattice(64, 0.8442, 0.72, seed=3, jitter=0.1))
         g2, m2 = force_error(abi, W.config_ions_8000(seed=2))
         sec["force_rel_err_mixed_vs_fp64"] = {"lj_1m": {"global": g1, "max_over_rms": m1},
@@ -384,7 +386,7 @@ def gpu_arm(args):
     sim.close()
 
     cpu = None
-    if rank == 0 and not args.no_cpu_baseline:
+    if world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(s_lj, budget_s=args.cpu_budget)
 
     if rank == 0:
