@@ -32,6 +32,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/caviar_b200.h"
+#include "cvr_device.cuh"
 
 namespace {
 
@@ -73,15 +74,7 @@ __device__ __forceinline__ float2 conjf_if(float2 a, bool c) {
   return a;
 }
 
-// erfc(x) for x >= 0 from its rational-exponential approximation
-// erfc(x) = t (a1 + t (a2 + t (a3 + t (a4 + t a5)))) exp(-x^2), t = 1 / (1 + p x),
-// absolute error below 1.5e-7 (Abramowitz & Stegun, Handbook of Mathematical
-// Functions, 1964, eq. 7.1.26).  ex = exp(-x^2), which the force needs anyway.
-__device__ __forceinline__ float erfc_as(float x, float ex) {
-  const float t = __fdividef(1.f, fmaf(0.3275911f, x, 1.f));
-  return t * fmaf(t, fmaf(t, fmaf(t, fmaf(t, 1.061405429f, -1.453152027f), 1.421413741f), -0.284496736f),
-                  0.254829592f) * ex;
-}
+using cvr::erfc_as;  // Abramowitz & Stegun 7.1.26 (cvr_device.cuh)
 
 template <int TPB, int NV>
 __device__ __forceinline__ void block_sum(double (&v)[NV], double *red, double *out) {

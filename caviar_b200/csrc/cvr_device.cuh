@@ -90,6 +90,17 @@ template <typename real> struct DevState {
   double *mass;      // per type (device)
 };
 
+// erfc(x) for x >= 0 from its rational-exponential approximation
+// erfc(x) = t (a1 + t (a2 + t (a3 + t (a4 + t a5)))) exp(-x^2), t = 1 / (1 + p x),
+// absolute error below 1.5e-7 (Abramowitz & Stegun, Handbook of Mathematical
+// Functions, 1964, eq. 7.1.26).  ex = exp(-x^2), which the Ewald real-space
+// force needs anyway.  Used by the FP32 (mixed) kernels only.
+__device__ __forceinline__ float erfc_as(float x, float ex) {
+  const float t = __fdividef(1.f, fmaf(0.3275911f, x, 1.f));
+  return t * fmaf(t, fmaf(t, fmaf(t, fmaf(t, 1.061405429f, -1.453152027f), 1.421413741f), -0.284496736f),
+                  0.254829592f) * ex;
+}
+
 // 32-bit fixed-point coordinate u = round(p * 2^32 / L) mod 2^32.  The
 // difference of two such coordinates, read as a signed int32, is the
 // minimum-image displacement in units of L / 2^32 whenever the true

@@ -48,7 +48,6 @@ __device__ __forceinline__ float fast_rsqrt(float x) { return rsqrtf(x); }
 __device__ __forceinline__ double fast_rsqrt(double x) { return rsqrt(x); }
 __device__ __forceinline__ float fast_exp(float x) { return __expf(x); }
 __device__ __forceinline__ double fast_exp(double x) { return exp(x); }
-__device__ __forceinline__ float erfc_r(float x) { return erfcf(x); }
 __device__ __forceinline__ double erfc_r(double x) { return erfc(x); }
 __device__ __forceinline__ int type_of(float w) { return __float_as_int(w); }
 __device__ __forceinline__ int type_of(double w) { return (int)w; }
@@ -158,8 +157,13 @@ __device__ __forceinline__ void pair_term(PairAcc<real> &A, real dx, real dy, re
     if (r2 > (real)0 && (ew.cut2 < (real)0 || r2 <= ew.cut2)) {
       const real rinv = fast_rsqrt(r2);
       const real r = r2 * rinv;
-      const real erfcv = erfc_r(ew.alpha * r);
-      const real sv = (ew.two_alpha_spi * fast_exp(-ew.alpha2 * r2) + erfcv * rinv) * (rinv * rinv);
+      const real ex = fast_exp(-ew.alpha2 * r2);  // exp(-(alpha r)^2)
+      real erfcv;
+      if constexpr (sizeof(real) == 4)
+        erfcv = erfc_as(ew.alpha * r, ex);  // shares ex with the force term
+      else
+        erfcv = erfc_r(ew.alpha * r);
+      const real sv = (ew.two_alpha_spi * ex + erfcv * rinv) * (rinv * rinv);
       const real lam = same_mol ? pc.lam : (real)1;
       c -= lam * pc.qq * sv;
       if (EV) A.g_ew += lam * pc.qq * erfcv * rinv;
