@@ -138,7 +138,7 @@ struct cvr_ctx {
   // flags: [flag, err, max_count, n_builds]
   int *flags{};
   double *d_mass_inv{}, *d_mass{}, *d_charge{};
-  void *d_coef{}, *d_offs{};
+  void *d_coef{};
   // partials
   double *ev_part{}, *ke_part{}, *ek_part{};
   int n_ev_blocks = 0, n_ke_blocks = 0, n_ek_blocks = 0;
@@ -415,17 +415,9 @@ int upload_tables(cvr_ctx *c) {
         if (!c->lam.empty()) p.lam = c->lam[a * T + b];
       }
     }
-  const int S = 2 * c->R + 1;
-  std::vector<double4> od(S * S * S);
-  for (int code = 0; code < S * S * S; ++code) {
-    const int dx = code % S - c->R, dy = (code / S) % S - c->R, dz = code / (S * S) - c->R;
-    od[code] = make_double4(dx * c->w[0], dy * c->w[1], dz * c->w[2], 0.0);
-  }
   if (dbl) {
     if (int r = dalloc(c, (PairCoef<double> **)&c->d_coef, T * T)) return r;
     CVR_CUDA(c, cudaMemcpyAsync(c->d_coef, cd.data(), T * T * sizeof(PairCoef<double>), cudaMemcpyHostToDevice, c->stream));
-    if (int r = dalloc(c, (double4 **)&c->d_offs, S * S * S)) return r;
-    CVR_CUDA(c, cudaMemcpyAsync(c->d_offs, od.data(), od.size() * sizeof(double4), cudaMemcpyHostToDevice, c->stream));
   } else {
     // fixed-point form: lengths in units of h = L / 2^32 (r2 -> r2 / h^2; the
     // force coefficient c -> c h^2, so c * du summed and times 1/h is the force)
@@ -437,15 +429,8 @@ int upload_tables(cvr_ctx *c) {
                               (float)(p.rc2 > 0 ? p.rc2 / h2 : p.rc2),
                               (float)(p.qq / h), (float)p.e4, (float)p.C0, (float)(p.C1 * h2), (float)p.lam};
     }
-    std::vector<float4> of(S * S * S);
-    for (int code = 0; code < S * S * S; ++code) {
-      const int dx = code % S - c->R, dy = (code / S) % S - c->R, dz = code / (S * S) - c->R;
-      of[code] = make_float4(dx * (float)c->w[0], dy * (float)c->w[1], dz * (float)c->w[2], 0.f);
-    }
     if (int r = dalloc(c, (PairCoef<float> **)&c->d_coef, T * T)) return r;
     CVR_CUDA(c, cudaMemcpyAsync(c->d_coef, cf.data(), T * T * sizeof(PairCoef<float>), cudaMemcpyHostToDevice, c->stream));
-    if (int r = dalloc(c, (float4 **)&c->d_offs, S * S * S)) return r;
-    CVR_CUDA(c, cudaMemcpyAsync(c->d_offs, of.data(), of.size() * sizeof(float4), cudaMemcpyHostToDevice, c->stream));
   }
   std::vector<double> mi(T), m(T);
   for (int t = 0; t < T; ++t) {
