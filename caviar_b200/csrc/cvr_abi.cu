@@ -788,7 +788,7 @@ void launch_thermo(cvr_ctx *c, double *out) {
   t.n_builds = c->flags + 3;
   t.counters = c->counters;
   t.out = out;
-  k_thermo<<<1, 256, 0, c->stream>>>(t);
+  k_thermo<<<1, THERMO_THREADS, 0, c->stream>>>(t);
   c->launches++;
 }
 

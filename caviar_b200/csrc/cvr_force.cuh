@@ -1327,38 +1327,61 @@ struct ThermoArgs {
   double *out;          // base of the records, CVR_N_THERMO doubles each
 };
 
-__global__ void __launch_bounds__(256) k_thermo(ThermoArgs a) {
-  __shared__ double acc[8][256];
+// One block of THERMO_THREADS: each thread sums its strided share of the
+// block partials (loops unrolled so that several loads are in flight), then
+// warp shuffles and one warp finish the sums (a fixed order).
+constexpr int THERMO_THREADS = 1024;
+__global__ void __launch_bounds__(THERMO_THREADS) k_thermo(ThermoArgs a) {
+  __shared__ double red[8][32];
   double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  for (int b = threadIdx.x; b < a.n_ke; b += blockDim.x)
-    for (int q = 0; q < 4; ++q) v[q] += a.ke_part[(size_t)b * 4 + q];
+#pragma unroll 4
+  for (int b = threadIdx.x; b < a.n_ke; b += blockDim.x) {
+    const double4 k = *reinterpret_cast<const double4 *>(a.ke_part + (size_t)b * 4);
+    v[0] += k.x;
+    v[1] += k.y;
+    v[2] += k.z;
+    v[3] += k.w;
+  }
+#pragma unroll 4
   for (int b = threadIdx.x; b < a.n_ev; b += blockDim.x)
     for (int q = 0; q < 3; ++q) v[4 + q] += a.ev_part[(size_t)b * 3 + q];
+#pragma unroll 4
   for (int b = threadIdx.x; b < a.n_ek; b += blockDim.x) v[7] += a.ek_part[b];
-  for (int q = 0; q < 8; ++q) acc[q][threadIdx.x] = v[q];
-  __syncthreads();
-  for (int st = blockDim.x / 2; st > 0; st >>= 1) {
-    if ((int)threadIdx.x < st)
-      for (int q = 0; q < 8; ++q) acc[q][threadIdx.x] += acc[q][threadIdx.x + st];
-    __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    double x = v[q];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    if (lane == 0) red[q][warp] = x;
   }
-  if (threadIdx.x == 0) {
+  __syncthreads();
+  if (warp != 0) return;
+  double acc[8];
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    double x = (lane < nw) ? red[q][lane] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    acc[q] = x;
+  }
+  if (lane == 0) {
     const long long rec = a.counters[1]++;
     double *out = a.out + rec * 10;
-    const double mv2 = acc[0][0];
+    const double mv2 = acc[0];
     double ke = 0.5 * mv2;
     if (a.com_removed && a.total_mass > 0) {
-      const double px = acc[1][0], py = acc[2][0], pz = acc[3][0];
+      const double px = acc[1], py = acc[2], pz = acc[3];
       ke -= 0.5 * (px * px + py * py + pz * pz) / a.total_mass;
     }
     const double temp = (a.dof > 0) ? 2.0 * ke / (a.k_b * a.dof) : 0.0;
-    const double vir = acc[6][0];
+    const double vir = acc[6];
     out[0] = (double)a.counters[0];
     out[1] = ke;
     out[2] = temp;
-    out[3] = acc[4][0];
-    out[4] = acc[5][0];
-    out[5] = a.ek_coef * acc[7][0];
+    out[3] = acc[4];
+    out[4] = acc[5];
+    out[5] = a.ek_coef * acc[7];
     if (a.dipole) {
       const double *M = a.dipole + 3;
       out[5] += 0.5 * a.dipole_coef * (M[0] * M[0] + M[1] * M[1] + M[2] * M[2]);
