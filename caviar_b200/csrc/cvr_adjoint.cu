@@ -43,6 +43,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/caviar_b200.h"
+#include "cvr_device.cuh"
 
 namespace {
 
@@ -256,6 +257,12 @@ template <typename real> struct PairOut {
   real dc_e, dc_s, dU_e, dU_s, cq;
 };
 
+// FP32 (mixed) pair terms use the hardware reciprocal / reciprocal square
+// root / exponential and erfc from Abramowitz & Stegun 7.1.26 sharing the
+// Gaussian (erfc_as); the FP64 form keeps the correctly rounded functions.
+__device__ __forceinline__ float adj_rcp(float x) { return __fdividef(1.f, x); }
+__device__ __forceinline__ double adj_rcp(double x) { return 1.0 / x; }
+
 template <typename real>
 __device__ __forceinline__ PairOut<real> pair_terms(const Params &p, int tp, real qq, real r2, bool need_d2,
                                                     bool need_param, bool need_energy) {
@@ -264,7 +271,7 @@ __device__ __forceinline__ PairOut<real> pair_terms(const Params &p, int tp, rea
   const real e = (real)p.eps[tp];
   if (r2 <= (real)p.rc_lj2 && e != (real)0) {
     const real sg = (real)p.sig[tp], rc2 = (real)p.rc_lj2;
-    const real r2i = (real)1 / r2, s2 = sg * sg * r2i, s6 = s2 * s2 * s2, s12 = s6 * s6;
+    const real r2i = adj_rcp(r2), s2 = sg * sg * r2i, s6 = s2 * s2 * s2, s12 = s6 * s6;
     const real c2 = sg * sg / rc2, c6 = c2 * c2 * c2, c12 = c6 * c6;
     const real ce = (real)4 * ((-(real)12 * s12 + (real)6 * s6) * r2i + ((real)12 * c12 - (real)6 * c6) / rc2);
     o.c = e * ce;
@@ -285,8 +292,18 @@ __device__ __forceinline__ PairOut<real> pair_terms(const Params &p, int tp, rea
   }
   if (r2 <= (real)p.rc_r2 && p.k_e != 0.0) {
     const real al = (real)p.alpha, beta = (real)(2.0 * p.alpha * 0.56418958354775628695);
-    const real r = sqrt(r2), ri = (real)1 / r;
-    const real G = exp(-al * al * r2), ec = erfc(al * r);
+    real r, ri, G, ec;
+    if constexpr (sizeof(real) == 4) {
+      ri = rsqrtf(r2);
+      r = r2 * ri;
+      G = __expf(-al * al * r2);
+      ec = cvr::erfc_as(al * r, G);
+    } else {
+      r = sqrt(r2);
+      ri = (real)1 / r;
+      G = exp(-al * al * r2);
+      ec = erfc(al * r);
+    }
     const real E1 = -beta * G * ri - ec * ri * ri;
     const real cq = (real)p.k_e * E1 * ri;
     o.cq = cq;
