@@ -120,14 +120,17 @@ def test_lj4000_vs_oracle(cuda_lib, oracle_lib, prec):
     check_forces(acc, o.state()[2], prec)
 
 
-@pytest.mark.parametrize("stretch_z", [1.0, 1.07])
-def test_fixed_point_and_cell_local_forms(cuda_lib, oracle_lib, stretch_z):
-    """The mixed form takes fixed-point pair displacements in a cubic box and
-    the cell-local FP32 form otherwise; both stay within the mixed tolerance
-    of the FP64 oracle (forces, LJ energy, virial), and so does a 60-step run
-    (positions within 1e-5, forces 1e-4, FP64 form the comparison)."""
+@pytest.mark.parametrize("stretch_z,bc", [(1.0, (1, 1, 1)), (1.07, (1, 1, 1)), (1.0, (1, 1, 0))])
+def test_fixed_point_and_cell_local_forms(cuda_lib, oracle_lib, stretch_z, bc):
+    """The mixed form takes fixed-point pair displacements in a cubic box
+    (periodic or not: a listed pair never spans half the box, so the integer
+    wrap never applies to it) and the cell-local FP32 form otherwise; both
+    stay within the mixed tolerance of the FP64 oracle (forces, LJ energy,
+    virial), and so does a 60-step run (positions within 1e-5, forces 1e-4,
+    FP64 form the comparison)."""
     from caviar_b200 import workloads as W
     s = W.fcc_lattice(10, 0.8442, 0.72, seed=4, jitter=0.1)
+    s.bc = bc
     s.hi = np.asarray(s.lo, np.float64) + s.box * np.array([1.0, 1.0, stretch_z])
     o = oracle_lib.Oracle(s)
     o.setup()
