@@ -129,10 +129,10 @@ template <typename real> struct PairAcc {
   real g_lj, g_ew, g_vir;
 };
 
-template <typename real>
+template <bool LJ, bool EWR, typename real>
 __device__ __forceinline__ void ev_flush(PairAcc<real> &A) {
-  A.e_lj += (double)A.g_lj;
-  A.e_ew += (double)A.g_ew;
+  if (LJ) A.e_lj += (double)A.g_lj;
+  if (EWR) A.e_ew += (double)A.g_ew;
   A.vir += (double)A.g_vir;
   A.g_lj = A.g_ew = A.g_vir = (real)0;
 }
@@ -259,7 +259,7 @@ __global__ void __launch_bounds__(128, CVR_PAIR_MINB) k_pair(DevState<real> s, c
                                          ew);
           }
         }
-        if (EV) ev_flush(A);
+        if (EV) ev_flush<LJ, EWR>(A);
       };
       for (int k = 0; k < full; k += 4) {
         const uint4 e4 = nxt;
@@ -293,7 +293,7 @@ __global__ void __launch_bounds__(128, CVR_PAIR_MINB) k_pair(DevState<real> s, c
           pair_term<real, LJ, EWR, EV>(A, dx, dy, dz, ONE_TYPE ? c1 : ci[type_of(xj[u].w)], sm[u], ignore_intra,
                                        ew);
         }
-        if (EV) ev_flush(A);
+        if (EV) ev_flush<LJ, EWR>(A);
       }
       for (; k < cnt; k += TPA) {
         const uint32_t e0 = __ldcs(row);
@@ -305,7 +305,7 @@ __global__ void __launch_bounds__(128, CVR_PAIR_MINB) k_pair(DevState<real> s, c
         pair_disp<real, FIXED>(xj0, xi, e0, st, dx, dy, dz);
         pair_term<real, LJ, EWR, EV>(A, dx, dy, dz, ONE_TYPE ? c1 : ci[type_of(xj0.w)], sm0, ignore_intra, ew);
       }
-      if (EV) ev_flush(A);
+      if (EV) ev_flush<LJ, EWR>(A);
     }
   }
 #pragma unroll
@@ -726,29 +726,33 @@ __global__ void __launch_bounds__(512, sizeof(real) == 4 ? CVR_KF_MINB : 1) k_kf
 template <typename real>
 __device__ __forceinline__ bool update_local(DevState<real> &s, int i, const double (&p)[3]) {
   bool need = false;
-  int cc[3];
-  cell_xyz(s, s.cell[i], cc[0], cc[1], cc[2]);
-  double loc[3];
   int code = 0, mul = 1;
+  if (s.policy == 1) {
 #pragma unroll
-  for (int d = 0; d < 3; ++d) {
-    loc[d] = p[d] - (s.box.lo[d] + (cc[d] + 0.5) * s.cells.w[d]);
-    if (s.policy == 1) {
+    for (int d = 0; d < 3; ++d) {
       if (s.box.bc[d] == 1 && (p[d] < s.box.lo[d] || p[d] > s.box.hi[d])) need = true;  // owned wrap
       code += (ghost_val(p[d], s.box.gclo[d], s.box.gchi[d], s.box.bc[d]) + 1) * mul;
       mul *= 3;
     }
   }
-  typename V4<real>::t q = s.x4[i];
-  q.x = (real)loc[0];
-  q.y = (real)loc[1];
-  q.z = (real)loc[2];
+  typename V4<real>::t q;
+  bool fx = false;
   if constexpr (sizeof(real) == 4) {
-    if (s.fixed) {
+    if (s.fixed) {  // fixed point: no cell frame, the type from the type array
       q.x = fixed_coord(p[0], s.fx_scale);
       q.y = fixed_coord(p[1], s.fx_scale);
       q.z = fixed_coord(p[2], s.fx_scale);
+      q.w = __int_as_float(s.type[i]);
+      fx = true;
     }
+  }
+  if (!fx) {
+    int cc[3];
+    cell_xyz(s, s.cell[i], cc[0], cc[1], cc[2]);
+    q = s.x4[i];
+    q.x = (real)(p[0] - (s.box.lo[0] + (cc[0] + 0.5) * s.cells.w[0]));
+    q.y = (real)(p[1] - (s.box.lo[1] + (cc[1] + 0.5) * s.cells.w[1]));
+    q.z = (real)(p[2] - (s.box.lo[2] + (cc[2] + 0.5) * s.cells.w[2]));
   }
   s.x4[i] = q;
   const float4 b = s.xb[i];
