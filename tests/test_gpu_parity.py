@@ -154,6 +154,26 @@ def test_fixed_point_and_cell_local_forms(cuda_lib, oracle_lib, stretch_z, bc):
     assert force_errors(a1, a2)[0] < 1e-4
 
 
+def test_fine_grid_box_uses_cell_local_form(cuda_lib, oracle_lib):
+    """A cubic box with more than 256 cells per axis (a 4000-atom lattice
+    cluster in L = 400: 285 cells) keeps the cell-local FP32 form, because
+    the fixed-point step L / 2^32 would be coarser than the FP32 spacing of
+    cell-local coordinates; pair set bit-exact, forces within the mixed
+    tolerance of the FP64 oracle."""
+    from caviar_b200 import workloads as W
+    s = W.fcc_lattice(10, 0.8442, 0.72, seed=6, jitter=0.1)
+    s.pos = s.pos + (200.0 - 0.5 * s.box[0])
+    s.lo, s.hi = np.zeros(3), np.full(3, 400.0)
+    o = oracle_lib.Oracle(s)
+    o.setup()
+    sim = sim_for(cuda_lib, s, "mixed")
+    acc, _ = sim.compute_forces()
+    info = sim.info()
+    assert info["ncx"] > 256 and info["fixed_point"] == 0
+    assert np.array_equal(sim.pairs(), o.pairs())
+    check_forces(acc, o.state()[2], "mixed")
+
+
 LIST_KERNELS = ["thread", "warp"]
 
 
