@@ -393,7 +393,8 @@ def gpu_arm(args):
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps, "warmup": warmup,
             "ms_per_step": ms_max / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "fp32 pair/k-space math, fp64 positions + S(k) + energy/virial sums",
+            "dtype": "fp32",
+            "precision": "fp32 pair/k-space math, fp64 positions + S(k) + energy/virial sums",
             "data": "synthetic (seeded FCC lattice + Maxwell-Boltzmann velocities)",
             "config": {"workload": "LJ fluid N=1048576 (FCC 64^3, rho*=0.8442, T*=0.72, rc=2.5, skin=0.3, dt=0.005), "
                                    "mixed precision", "n_atoms": n, "parallelism": f"replicas x{world}",
