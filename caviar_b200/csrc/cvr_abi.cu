@@ -1599,6 +1599,7 @@ int cvr_clear_thermostat(cvr_ctx *c) {
 int cvr_set_list_kernel(cvr_ctx *c, int kind) {
   if (!c) return CVR_ERR_INVALID;
   if (kind < CVR_LIST_AUTO || kind > CVR_LIST_WARP) return fail(c, CVR_ERR_INVALID, "unknown list kernel");
+  if (kind != c->list_kernel) c->epoch++;  // the step graphs bake the list kernel in
   c->list_kernel = kind;
   return CVR_OK;
 }
