@@ -9,8 +9,9 @@
 //   atom_data basic <name>     ghost_cutoff, k_b, set_domain|domain, add_type_mass t m,
 //                              add_type_charge t q, add_xyz_data_file file_name "<f>"
 //                              [read_velocity] [last_frame] [replace_data],
-//                              set_owned_position|set_owned_velocity i x y z
-//                              (atom_data.cpp:78-306, atom_data/add_xyz_data_file.cpp:22-168)
+//                              set_owned_position|set_owned_velocity i x y z,
+//                              add_random_velocity seed amplitude
+//                              (atom_data.cpp:78-306, 597-616, atom_data/add_xyz_data_file.cpp:22-168)
 //   neighborlist basic <name>  set_atom_data|atom_data, set_domain|domain, cutoff,
 //                              cutoff_extra_coef, build_cell_list,
 //                              make_verlet_list_from_cell_list, rebuild_test, dt
@@ -63,7 +64,8 @@
 // rebuild_policy displacement|reference, thermo_step N, thermo_file "<f>",
 // state_file "<f>" (FP64 binary dump of the final state, id order);
 // (atom_data) add_state_file file_name "<f>" [replace_data] (reads that dump
-// back: positions and velocities bit for bit); (writer) potential_energy_step
+// back: positions and velocities bit for bit), write_state_file "<f>" (the
+// same dump of the atoms as loaded so far, acceleration zero); (writer) potential_energy_step
 // N and file_name_potential_energy "<f>" (LJ + Ewald potential energy, which
 // the reference writer lacks), precision N (significant digits of every
 // writer number; 17 makes an xyz frame an exact FP64 restart file).
@@ -78,6 +80,7 @@
 #include <cstring>
 #include <fstream>
 #include <map>
+#include <random>
 #include <memory>
 #include <sstream>
 #include <stdexcept>
@@ -407,6 +410,51 @@ struct Script {
     }
   }
 
+  // Atom_data::add_random_velocity (atom_data.cpp:597-616): every velocity
+  // component uniform in [-amplitude, amplitude] from std::mt19937(seed) in
+  // atom order (x, y, z per atom), then the mass-weighted centre-of-mass
+  // velocity (owned_velocity_cm, kinetic_energy.cpp:413-457) subtracted from
+  // the atoms whose type has a mass.  The same standard-library generator and
+  // distribution as the reference build, so the same bits.
+  void add_random_velocity(Atom_data &a, unsigned int seed, double amplitude) {
+    std::mt19937 mt(seed);
+    std::uniform_real_distribution<double> dist(-amplitude, amplitude);
+    const int64_t n = a.n();
+    a.vel.assign((size_t)n * 3, 0.0);
+    for (int64_t i = 0; i < n; ++i)
+      for (int d = 0; d < 3; ++d) a.vel[3 * (size_t)i + d] = dist(mt);
+    auto mass_of = [&](int64_t i) {
+      const int t = a.type[(size_t)i];
+      return (t >= 0 && t < (int)a.mass.size()) ? a.mass[(size_t)t] : 0.0;
+    };
+    double vcm[3] = {0.0, 0.0, 0.0}, msum = 0.0;
+    for (int64_t i = 0; i < n; ++i) {
+      const double m = mass_of(i);
+      msum += m;
+      for (int d = 0; d < 3; ++d) vcm[d] += a.vel[3 * (size_t)i + d] * m;
+    }
+    for (int d = 0; d < 3; ++d) vcm[d] = vcm[d] / msum;
+    for (int64_t i = 0; i < n; ++i)
+      if (mass_of(i) != 0.0)
+        for (int d = 0; d < 3; ++d) a.vel[3 * (size_t)i + d] -= vcm[d];
+  }
+
+  // The atoms as loaded so far, in the md_simulator state_file format
+  // (acceleration zero): a checkpoint of a prepared input state.
+  void write_state_file(const Atom_data &a, const std::string &file) {
+    const std::string p = (file[0] == '/') ? file : dir + "/" + file;
+    FILE *sf = std::fopen(p.c_str(), "wb");
+    if (!sf) err("cannot write " + p);
+    const int64_t n = a.n();
+    std::vector<double> vel = a.vel, acc((size_t)n * 3, 0.0);
+    vel.resize((size_t)n * 3, 0.0);
+    std::fwrite(&n, 8, 1, sf);
+    std::fwrite(a.pos.data(), 8, (size_t)n * 3, sf);
+    std::fwrite(vel.data(), 8, (size_t)n * 3, sf);
+    std::fwrite(acc.data(), 8, (size_t)n * 3, sf);
+    std::fclose(sf);
+  }
+
   // FP64 binary state written by md_simulator state_file: n, pos[3n], vel[3n], acc[3n]
   void add_state_file(Atom_data &a) {
     std::string file;
@@ -536,6 +584,13 @@ struct Script {
         a.pressure_process = integer() != 0;  // atom_data.cpp:137-146
       } else if (t == "add_state_file") {
         add_state_file(a);
+      } else if (t == "add_random_velocity") {
+        const long long seed = integer();
+        double amplitude = real();
+        if (amplitude < 0) amplitude = -amplitude;  // atom_data.cpp:280-289
+        add_random_velocity(a, (unsigned int)seed, amplitude);
+      } else if (t == "write_state_file") {
+        write_state_file(a, word());
       } else err("atom_data: '" + t + "' is not on the B200 hot path");
     }
   }

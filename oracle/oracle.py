@@ -376,7 +376,7 @@ def harness_available() -> bool:
 
 def run_reference(system, mode: str = "forces", nsteps: int = 0, rebuild_test: bool = False,
                   timeout: Optional[float] = None, budget_s: float = 0.0, extra: str = "",
-                  collect=()) -> Dict[str, np.ndarray]:
+                  collect=(), mode_args=()) -> Dict[str, np.ndarray]:
     """Run the unmodified reference on `system` ("forces" or "run") and return
     its FP64 output blocks plus the harness's own wall time.  budget_s > 0
     stops a run after the step that crosses the budget (at least 2 steps).
@@ -393,6 +393,7 @@ def run_reference(system, mode: str = "forces", nsteps: int = 0, rebuild_test: b
             f.write(casl_script(system, nsteps, rebuild_test, extra))
         write_state(state, system)
         args = [HARNESS_PATH, script, state, mode, out] + ([str(nsteps), repr(float(budget_s))] if mode == "run" else [])
+        args += [str(x) for x in mode_args]  # e.g. randvel: seed, amplitude
         t0 = time.perf_counter()
         p = subprocess.run(args, cwd=d, capture_output=True, text=True, timeout=timeout)
         wall = time.perf_counter() - t0

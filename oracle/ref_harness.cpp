@@ -6,6 +6,7 @@
 // Usage:
 //   ref_harness <script.casl> <state.bin> forces <out.bin>
 //   ref_harness <script.casl> <state.bin> run    <out.bin> <nsteps> [budget_seconds]
+//   ref_harness <script.casl> <state.bin> randvel <out.bin> <seed> <amplitude>
 //
 // The CASL script defines the objects (domain box, atom_data basic,
 // neighborlist basic, force fields, md_simulator basic) with the reference's
@@ -24,6 +25,10 @@
 // virial, and the wall time of the first step (which includes setup) and of
 // the remaining steps.  With a budget, it stops after the first step whose end
 // exceeds the budget (at least two steps) and reports how many ran.
+//
+// "randvel" calls Atom_data::add_random_velocity(seed, amplitude) on the loaded
+// atoms (uniform velocities from the reference's mt19937, centre-of-mass
+// motion removed) and dumps the owned state.
 //
 // state.bin (little endian):
 //   int64 n; then n records of { int32 type; int32 mol; double pos[3]; double vel[3]; }
@@ -311,6 +316,15 @@ int main(int argc, char **argv)
     out.scalar("wall_rest", t_rest);
     out.scalar("steps_done", (double)done);
     out.scalar("n_ghost", (double)ad->atom_struct_ghost.position.size());
+  }
+  else if (mode == "randvel")
+  {
+    // the reference's own Atom_data::add_random_velocity (atom_data.cpp:597-616)
+    // on the loaded atoms: argv[5] = seed, argv[6] = amplitude
+    const unsigned int seed = (argc > 5) ? (unsigned int)std::strtoul(argv[5], nullptr, 10) : 0u;
+    const double amplitude = (argc > 6) ? std::atof(argv[6]) : 1.0;
+    ad->add_random_velocity(seed, amplitude);
+    dump_owned();
   }
   else
   {

@@ -283,6 +283,22 @@ def slab_correction() -> None:
     np.savez_compressed(os.path.join(HERE, "ref_slab_correction300.npz"), **out)
 
 
+def random_velocity500(seed: int = 7, amplitude: float = 1.5) -> None:
+    """Atom_data::add_random_velocity of the unmodified reference on a
+    two-species system with different masses (the centre-of-mass correction
+    is mass-weighted): its velocities, for the CASL front end's keyword."""
+    s = W.fcc_lattice(5, 0.8442, 0.72, seed=9, jitter=0.05)
+    rng = np.random.default_rng(9)
+    s.type = (rng.random(s.n) < 0.4).astype(np.int32)
+    s.mass = np.array([1.0, 2.5])
+    s.charge = np.zeros(2)
+    s.lj = W.LJParams(cutoff=2.5, epsilon=np.ones((2, 2)), sigma=np.ones((2, 2)))
+    r = O.run_reference(s, "randvel", mode_args=(seed, amplitude))
+    order = np.argsort(r["id"].astype(np.int64))
+    np.savez_compressed(os.path.join(HERE, "ref_randvel500.npz"), pos=s.pos, type=s.type, mass=s.mass,
+                        box=s.box, seed=seed, amplitude=amplitude, vel=r["vel"].reshape(-1, 3)[order])
+
+
 def main():
     ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     g = ewald_n100(ref_root)
@@ -298,6 +314,7 @@ def main():
     thermostats()
     ewald_slab()
     slab_correction()
+    random_velocity500()
     print("golden fixtures written to", HERE)
 
 

@@ -64,6 +64,34 @@ def test_requires_integrator_type(cuda_lib, tmp_path):
     assert "integrator_type" in str(e.value)
 
 
+def test_add_random_velocity_matches_reference(cuda_lib, tmp_path):
+    """atom_data add_random_velocity seed amplitude gives the velocities of
+    the reference's own Atom_data::add_random_velocity (fixture from the
+    unmodified reference: two species, masses 1 and 2.5, mass-weighted
+    centre-of-mass removal) bit for bit; write_state_file dumps the prepared
+    atoms (CPU: the script has no md_simulator run)."""
+    d = np.load(os.path.join(GOLDEN, "ref_randvel500.npz"))
+    L = float(d["box"][0])
+    pos, typ = d["pos"], d["type"]
+    with open(tmp_path / "state.xyz", "w") as f:
+        f.write(f"{len(pos)}\nstate\n")
+        for t, p in zip(typ, pos):
+            f.write(f"{int(t)} " + " ".join(repr(float(x)) for x in p) + "\n")
+    script = "\n".join([
+        "domain box dom", f"dom xmin 0.0 xmax {L!r}", f"dom ymin 0.0 ymax {L!r}", f"dom zmin 0.0 zmax {L!r}",
+        "dom boundary_condition 1 1 1", "dom generate", "atom_data basic adata", "adata set_domain dom",
+        "adata add_type_mass 0 1.0", "adata add_type_mass 1 2.5",
+        'adata add_xyz_data_file file_name "state.xyz"',
+        f"adata add_random_velocity {int(d['seed'])} {float(d['amplitude'])!r}",
+        'adata write_state_file "prepared.bin"', "exit", ""])
+    (tmp_path / "rv.casl").write_text(script)
+    cuda_lib.run_casl(str(tmp_path / "rv.casl"))
+    raw = np.fromfile(tmp_path / "prepared.bin", dtype=np.float64, offset=8)
+    n = len(pos)
+    assert np.array_equal(raw[:3 * n].reshape(n, 3), pos)
+    assert np.array_equal(raw[3 * n:6 * n].reshape(n, 3), d["vel"])
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", ["lj500", "ions500"])
 def test_reference_script_reproduces_reference_trajectory(cuda_lib, tmp_path, name):
