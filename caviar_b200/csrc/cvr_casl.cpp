@@ -10,7 +10,7 @@
 //                              add_type_charge t q, add_xyz_data_file file_name "<f>"
 //                              [read_velocity] [last_frame] [replace_data],
 //                              set_owned_position|set_owned_velocity i x y z,
-//                              add_random_velocity seed amplitude
+//                              add_random_velocity seed amplitude, msd_process (accepted, no effect)
 //                              (atom_data.cpp:78-306, 597-616, atom_data/add_xyz_data_file.cpp:22-168)
 //   neighborlist basic <name>  set_atom_data|atom_data, set_domain|domain, cutoff,
 //                              cutoff_extra_coef, build_cell_list,
@@ -33,7 +33,8 @@
 //                              add_neighborlist|neighborlist, add_writer|writer,
 //                              integrator_type velocity_verlet|velocity_verlet_langevin,
 //                              temperature, friction, kb, kbt, dt, initial_step,
-//                              final_step, final_step_add, run (md_simulator.cpp:58-233)
+//                              final_step, final_step_add, initial_time, final_time,
+//                              run (md_simulator.cpp:58-233)
 //   writer atom_data <name>    set_atom_data|atom_data, set_domain|domain, energy_step,
 //                              temperature_step, pressure_step, volume_step, xyz_step,
 //                              file_name_energy|_temperature|_pressure|_volume|_xyz,
@@ -163,7 +164,7 @@ struct Domain : Object {
 struct Atom_data : Object {
   Domain *domain = nullptr;
   double ghost_cutoff = -1.0, k_b = -1.0;
-  bool temperature_process = false, pressure_process = false;
+  bool temperature_process = false, pressure_process = false, msd_process = false;
   std::vector<double> mass, charge;
   std::vector<int32_t> type, mol;
   std::vector<double> pos, vel;
@@ -266,7 +267,8 @@ struct Md_simulator : Object {
   std::vector<Neighborlist *> neighborlist;
   double dt = -1.0;
   int64_t initial_step = 0, final_step = 0;
-  bool vv = false, use_step = false;
+  double initial_time = 0.0, final_time = 0.0;
+  bool vv = false, use_step = false, use_time = false;
   int precision = CVR_PREC_MIXED, policy = CVR_REBUILD_DISPLACEMENT;
   int64_t thermo_step = 0;
   std::string thermo_file, state_file;
@@ -582,6 +584,11 @@ struct Script {
         a.temperature_process = integer() != 0;
       } else if (t == "pressure_process") {
         a.pressure_process = integer() != 0;  // atom_data.cpp:137-146
+      } else if (t == "msd_process") {
+        // atom_data.cpp:127-136: switches on the reference's displacement
+        // counters, read only by its msd writer and by an external virial that
+        // its pressure excludes (kinetic_energy.cpp:288); no effect here
+        a.msd_process = integer() != 0;
       } else if (t == "add_state_file") {
         add_state_file(a);
       } else if (t == "add_random_velocity") {
@@ -782,6 +789,8 @@ struct Script {
       else if (t == "initial_step") m.initial_step = integer(), m.use_step = true;
       else if (t == "final_step") m.final_step = integer(), m.use_step = true;
       else if (t == "final_step_add") m.final_step += integer(), m.use_step = true;
+      else if (t == "initial_time") m.initial_time = real(), m.use_time = true;  // md_simulator.cpp:71-80
+      else if (t == "final_time") m.final_time = real(), m.use_time = true;
       else if (t == "precision") {
         const std::string v = word();
         if (v == "mixed") m.precision = CVR_PREC_MIXED;
@@ -942,7 +951,15 @@ struct Script {
     if (!a) err("md_simulator: set_atom_data first");
     if (!m.vv) err("md_simulator: set 'integrator_type velocity_verlet' (the reference leaves it unset)");
     if (m.dt < 0) err("expected 'dt' input");
-    if (!m.use_step) err("simulator md: verify_settings: please assign 'time' or 'step' variables.");
+    // Md_simulator::verify_settings (md_simulator.cpp:276-282) and setup
+    // (:508-512): times become steps as `(int)time / dt` -- the time is
+    // truncated to an integer before the division, as the reference does.
+    if (m.use_time && m.use_step) err("simulator md: verify_settings: cannot use both 'time' and 'step'.");
+    if (!(m.use_time || m.use_step)) err("simulator md: verify_settings: please assign 'time' or 'step' variables.");
+    if (m.use_time) {
+      m.initial_step = (int)((double)(int)m.initial_time / m.dt);
+      m.final_step = (int)((double)(int)m.final_time / m.dt);
+    }
     if (m.neighborlist.size() != 1) err("the B200 path takes exactly one neighborlist");
     Neighborlist *nl = m.neighborlist[0];
     Domain *d = a->domain ? a->domain : nl->domain;

@@ -64,6 +64,41 @@ def test_requires_integrator_type(cuda_lib, tmp_path):
     assert "integrator_type" in str(e.value)
 
 
+def test_time_and_step_settings_are_exclusive(cuda_lib, tmp_path):
+    """md_simulator takes its run length from steps or from times, not both
+    (Md_simulator::verify_settings, md_simulator.cpp:276-282); atom_data
+    msd_process is accepted."""
+    s, _ = load_ref_fixture("lj500")
+    from oracle import oracle as O
+    body = O.casl_script(s, 5).replace("adata set_domain dom\n", "adata set_domain dom\nadata msd_process 1\n")
+    body += "sim final_time 1.0\nsim run\n"
+    p = tmp_path / "r.casl"
+    p.write_text(body)
+    with pytest.raises(cuda_lib.CvrError) as e:
+        cuda_lib.run_casl(str(p))
+    assert "cannot use both 'time' and 'step'" in str(e.value)
+
+
+@pytest.mark.gpu
+def test_final_time_counts_steps_like_the_reference(cuda_lib, tmp_path):
+    """final_time T runs (int)T / dt steps, the reference's conversion
+    (md_simulator.cpp:508-512: the time is truncated before the division):
+    final_time 1.9 at dt 0.005 ends in the state of final_step 200."""
+    s, _ = load_ref_fixture("lj500")
+    states = []
+    for tag, extra in (("t", ["sim final_time 1.9"]), ("s", [])):
+        d = tmp_path / tag
+        d.mkdir()
+        path = script_for(s, str(d), 200, extra + ['sim state_file "out.bin"'])
+        if tag == "t":
+            text = open(path).read().replace("sim initial_step 0\n", "").replace("sim final_step 200\n", "")
+            assert "initial_step" not in text and "final_step" not in text
+            open(path, "w").write(text)
+        cuda_lib.run_casl(path)
+        states.append(np.fromfile(d / "out.bin", dtype=np.float64, offset=8))
+    assert np.array_equal(states[0], states[1])
+
+
 def test_add_random_velocity_matches_reference(cuda_lib, tmp_path):
     """atom_data add_random_velocity seed amplitude gives the velocities of
     the reference's own Atom_data::add_random_velocity (fixture from the
