@@ -34,6 +34,7 @@
 //                              integrator_type velocity_verlet|velocity_verlet_langevin,
 //                              temperature, friction, kb, kbt, dt, initial_step,
 //                              final_step, final_step_add, initial_time, final_time,
+//                              remove_force_field|neighborlist|writer|constraint,
 //                              run (md_simulator.cpp:58-233)
 //   writer atom_data <name>    set_atom_data|atom_data, set_domain|domain, energy_step,
 //                              temperature_step, pressure_step, volume_step, xyz_step,
@@ -748,6 +749,13 @@ struct Script {
     }
   }
 
+  template <typename T>
+  void remove_from(std::vector<T *> &v, T *o, const char *what) {
+    auto it = std::find(v.begin(), v.end(), o);
+    if (it == v.end()) err(std::string("Unknown ") + what + " to remove.");
+    v.erase(it);
+  }
+
   void read_md(Md_simulator &m) {
     while (!cur->done()) {
       const std::string t = word();
@@ -756,6 +764,11 @@ struct Script {
       else if (t == "add_neighborlist" || t == "neighborlist") m.neighborlist.push_back(find<Neighborlist>(word()));
       else if (t == "add_writer" || t == "writer") m.writer.push_back(find<Writer>(word()));
       else if (t == "add_constraint" || t == "constraint") m.constraint.push_back(find<Thermostat>(word()));
+      // md_simulator.cpp:107-150: remove the named object from the simulator's list
+      else if (t == "remove_force_field") remove_from(m.force_field, find<Force_field>(word()), "force_field");
+      else if (t == "remove_neighborlist") remove_from(m.neighborlist, find<Neighborlist>(word()), "neighborlist");
+      else if (t == "remove_writer") remove_from(m.writer, find<Writer>(word()), "writer");
+      else if (t == "remove_constraint") remove_from(m.constraint, find<Thermostat>(word()), "constraint");
       else if (t == "integrator_type") {
         const std::string v = word();
         if (v == "velocity_verlet") {

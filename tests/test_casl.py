@@ -99,6 +99,24 @@ def test_final_time_counts_steps_like_the_reference(cuda_lib, tmp_path):
     assert np.array_equal(states[0], states[1])
 
 
+def test_remove_objects_from_the_simulator(cuda_lib, tmp_path):
+    """md_simulator remove_* drops the named object from the simulator's list
+    (md_simulator.cpp:107-150): removing the only neighbour list leaves a
+    simulator the B200 path refuses; removing an object the simulator does
+    not hold is the reference's 'Unknown ... to remove.' error."""
+    s, _ = load_ref_fixture("lj500")
+    from oracle import oracle as O
+    base = O.casl_script(s, 5)
+    (tmp_path / "a.casl").write_text(base + "sim remove_neighborlist neigh\nsim run\n")
+    with pytest.raises(cuda_lib.CvrError) as e:
+        cuda_lib.run_casl(str(tmp_path / "a.casl"))
+    assert "exactly one neighborlist" in str(e.value)
+    (tmp_path / "b.casl").write_text(base + "sim remove_force_field f_lj\nsim remove_force_field f_lj\n")
+    with pytest.raises(cuda_lib.CvrError) as e:
+        cuda_lib.run_casl(str(tmp_path / "b.casl"))
+    assert "Unknown force_field to remove." in str(e.value)
+
+
 def test_add_random_velocity_matches_reference(cuda_lib, tmp_path):
     """atom_data add_random_velocity seed amplitude gives the velocities of
     the reference's own Atom_data::add_random_velocity (fixture from the
