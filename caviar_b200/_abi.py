@@ -36,7 +36,7 @@ EXPORTED = ["cvr_create", "cvr_destroy", "cvr_set_neighborlist", "cvr_set_lj", "
             "cvr_batch_set_forces", "cvr_batch_set_state", "cvr_batch_run", "cvr_batch_get_state", "cvr_batch_info",
             "cvr_batch_last_error", "cvr_batch_stream", "cvr_adj_create", "cvr_adj_destroy", "cvr_adj_set_params",
             "cvr_adj_set_state", "cvr_adj_forces", "cvr_adj_force_vjp", "cvr_adj_loss", "cvr_adj_loss_grad",
-            "cvr_adj_last_error", "cvr_adj_stream"]
+            "cvr_adj_last_error", "cvr_adj_stream", "cvr_measure_fma_peak"]
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int32)

@@ -1509,6 +1509,7 @@ int cvr_set_integrator(cvr_ctx *c, double dt, double k_b) {
   if (!c) return CVR_ERR_INVALID;
   if (!(dt >= 0)) return fail(c, CVR_ERR_INVALID, "expected 'dt' input");
   if (!(k_b > 0)) return fail(c, CVR_ERR_INVALID, "k_b is not set.");
+  if (dt != c->dt || k_b != c->k_b) c->epoch++;  // the step graphs bake dt and k_b in
   c->dt = dt;
   c->k_b = k_b;
   return CVR_OK;

@@ -268,6 +268,7 @@ struct Md_simulator : Object {
   std::vector<Neighborlist *> neighborlist;
   double dt = -1.0;
   int64_t initial_step = 0, final_step = 0;
+  int64_t current_step = 0;  // Md_simulator::current_step: final_step after a run
   double initial_time = 0.0, final_time = 0.0;
   bool vv = false, use_step = false, use_time = false;
   int precision = CVR_PREC_MIXED, policy = CVR_REBUILD_DISPLACEMENT;
@@ -801,7 +802,10 @@ struct Script {
       } else if (t == "dt") m.dt = real();
       else if (t == "initial_step") m.initial_step = integer(), m.use_step = true;
       else if (t == "final_step") m.final_step = integer(), m.use_step = true;
-      else if (t == "final_step_add") m.final_step += integer(), m.use_step = true;
+      else if (t == "final_step_add") {  // md_simulator.cpp:91-97: does not select step mode
+        m.final_step += integer();
+        m.initial_step = m.current_step;
+      }
       else if (t == "initial_time") m.initial_time = real(), m.use_time = true;  // md_simulator.cpp:71-80
       else if (t == "final_time") m.final_time = real(), m.use_time = true;
       else if (t == "precision") {
@@ -1081,7 +1085,7 @@ struct Script {
       std::fclose(sf);
     }
     cvr_destroy(ctx);
-    m.initial_step = m.final_step;
+    m.current_step = m.final_step;  // the reference's run loop leaves current_step == final_step
   }
 
   void execute() {

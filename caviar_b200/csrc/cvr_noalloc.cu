@@ -16,7 +16,10 @@
 // g_sk_scratch as a device address (in host code it names a host-side stand-in):
 // the first call on each device looks up the real address with
 // cudaGetSymbolAddress, with that device current, and passes it to the
-// kernels.  Make that first call before any stream capture.
+// kernels.  Make that first call before any stream capture.  The address is
+// kept per device ordinal for the rest of the process, so the entry point must
+// not be used again on a device after cudaDeviceReset (the module is loaded
+// anew there and the kept address no longer names the array).
 //
 // Every call on a device shares the one array, and the array keeps the last
 // call's contents.  Each call writes every partial it later reads, so nothing
@@ -35,6 +38,15 @@ namespace {
 constexpr int kMaxDevices = 64;
 constexpr int kChunkAtoms = 64;  // atoms per shared-memory stage
 constexpr int kThreads = 256;    // k-vectors per block
+constexpr int kMaxK = 30;        // largest k_max per axis
+
+// k_max <= 30 on every axis gives at most (2*30)^3 = 216000 k-vectors, one
+// partial each per chunk; the array holds at least one chunk of them.
+static_assert(8 * kMaxK * kMaxK * kMaxK <= CVR_NOALLOC_SK_SCRATCH, "scratch must hold one chunk at k_max 30");
+
+// Dynamic shared memory of k_sk_noalloc_partial at k_max 30 (the largest any
+// call needs): phase tables of one stage of atoms plus their charges.
+constexpr size_t kMaxSmem = (size_t)kChunkAtoms * 3 * (kMaxK + 1) * 16 + kChunkAtoms * sizeof(double);
 
 __device__ __align__(256) double2 g_sk_scratch[CVR_NOALLOC_SK_SCRATCH];
 
@@ -135,19 +147,12 @@ extern "C" int cvr_structure_factor_noalloc(const double *pos, const double *q, 
   if (err && err_len) err[0] = '\0';
   if (!pos || !q || !sk || !box_len || n <= 0 || n > (int64_t)1 << 30)
     return say(err, err_len, CVR_ERR_INVALID, "pos, q, sk, box_len must be non-null and 0 < n <= 2^30");
-  if (kx_max < 0 || ky_max < 0 || kz_max < 0 || kx_max > 30 || ky_max > 30 || kz_max > 30)
+  if (kx_max < 0 || ky_max < 0 || kz_max < 0 || kx_max > kMaxK || ky_max > kMaxK || kz_max > kMaxK)
     return say(err, err_len, CVR_ERR_INVALID, "k_max per axis must be in [0, 30]");
   for (int d = 0; d < 3; ++d)
     if (!(box_len[d] > 0)) return say(err, err_len, CVR_ERR_INVALID, "box lengths must be positive");
-  const int64_t nk64 = (int64_t)(2 * kx_max) * (2 * ky_max) * (2 * kz_max);
-  if (nk64 == 0) return CVR_OK;
-  if (nk64 > CVR_NOALLOC_SK_SCRATCH) {
-    char m[160];
-    std::snprintf(m, sizeof(m), "%lld k-vectors exceed the fixed scratch of %d (one partial per k-vector)",
-                  (long long)nk64, CVR_NOALLOC_SK_SCRATCH);
-    return say(err, err_len, CVR_ERR_CAPACITY, m);
-  }
-  const int nk = (int)nk64;
+  const int nk = (2 * kx_max) * (2 * ky_max) * (2 * kz_max);  // <= 216000, see kMaxK
+  if (nk == 0) return CVR_OK;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
     return say(err, err_len, CVR_ERR_CUDA, "no usable current CUDA device");
@@ -155,8 +160,13 @@ extern "C" int cvr_structure_factor_noalloc(const double *pos, const double *q, 
   {
     std::lock_guard<std::mutex> g(g_lock);
     if (!g_scratch_ptr[dev]) {
+      // Set-up, once per device with that device current: the array's device
+      // address, and the kernel's shared-memory limit for the largest k_max
+      // (set once here, so that concurrent calls never lower it for each other).
       void *p = nullptr;
-      const cudaError_t e = cudaGetSymbolAddress(&p, g_sk_scratch);
+      cudaError_t e = cudaGetSymbolAddress(&p, g_sk_scratch);
+      if (e != cudaSuccess) return say(err, err_len, CVR_ERR_CUDA, cudaGetErrorString(e));
+      e = cudaFuncSetAttribute(k_sk_noalloc_partial, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem);
       if (e != cudaSuccess) return say(err, err_len, CVR_ERR_CUDA, cudaGetErrorString(e));
       g_scratch_ptr[dev] = static_cast<double2 *>(p);
     }
@@ -172,17 +182,14 @@ extern "C" int cvr_structure_factor_noalloc(const double *pos, const double *q, 
   const int chunk_atoms = (int)(stages_per_chunk * kChunkAtoms);
   const int nchunks = (int)((n + chunk_atoms - 1) / chunk_atoms);
   const int kp = (kx_max > ky_max ? (kx_max > kz_max ? kx_max : kz_max) : (ky_max > kz_max ? ky_max : kz_max)) + 1;
-  const size_t smem = (size_t)kChunkAtoms * 3 * kp * sizeof(double2) + kChunkAtoms * sizeof(double);
-  cudaError_t e = cudaFuncSetAttribute(k_sk_noalloc_partial, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)(smem > 48 * 1024 ? smem : 48 * 1024));
-  if (e != cudaSuccess) return say(err, err_len, CVR_ERR_CUDA, cudaGetErrorString(e));
+  const size_t smem = (size_t)kChunkAtoms * 3 * kp * sizeof(double2) + kChunkAtoms * sizeof(double);  // <= kMaxSmem
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const double3 inv_L = make_double3(1.0 / box_len[0], 1.0 / box_len[1], 1.0 / box_len[2]);
   dim3 g1((nk + kThreads - 1) / kThreads, nchunks);
   k_sk_noalloc_partial<<<g1, kThreads, smem, st>>>(pos, q, (int)n, chunk_atoms, inv_L, kx_max, ky_max, kz_max, nk,
                                                    scratch);
   k_sk_noalloc_reduce<<<(nk + kThreads - 1) / kThreads, kThreads, 0, st>>>(scratch, nchunks, nk, sk);
-  e = cudaGetLastError();
+  const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return say(err, err_len, CVR_ERR_CUDA, cudaGetErrorString(e));
   return CVR_OK;
 }

@@ -79,6 +79,48 @@ def test_time_and_step_settings_are_exclusive(cuda_lib, tmp_path):
     assert "cannot use both 'time' and 'step'" in str(e.value)
 
 
+def test_final_step_add_alone_selects_no_run_length(cuda_lib, tmp_path):
+    """final_step_add adds to final_step and restarts from the current step
+    but, as in the reference (md_simulator.cpp:91-97), does not select step
+    mode: a script with only final_step_add fails verify_settings."""
+    s, _ = load_ref_fixture("lj500")
+    from oracle import oracle as O
+    body = O.casl_script(s, 5).replace("sim initial_step 0\n", "").replace("sim final_step 5\n", "")
+    assert "final_step" not in body and "initial_step" not in body
+    body += "sim final_step_add 5\nsim run\n"
+    p = tmp_path / "r.casl"
+    p.write_text(body)
+    with pytest.raises(cuda_lib.CvrError) as e:
+        cuda_lib.run_casl(str(p))
+    assert "please assign 'time' or 'step' variables" in str(e.value)
+
+
+@pytest.mark.gpu
+def test_final_step_add_with_final_time(cuda_lib, tmp_path):
+    """final_step_add restarts from the current step: `final_step 200, run,
+    final_step_add 200, run` runs steps [0, 200) then [200, 400).  With
+    final_time set, final_step_add is accepted and has no effect: each run
+    recomputes its steps from the times ((int)1.0 / 0.005 = 200), as the
+    reference's verify_settings does.  Both scripts end in the same state."""
+    s, _ = load_ref_fixture("lj500")
+    states = []
+    for tag in ("step", "time"):
+        d = tmp_path / tag
+        d.mkdir()
+        path = script_for(s, str(d), 200, [])
+        text = open(path).read()
+        if tag == "step":
+            text = text.replace("sim run\n", 'sim run\nsim final_step_add 200\nsim state_file "out.bin"\nsim run\n', 1)
+        else:
+            text = text.replace("sim initial_step 0\n", "").replace("sim final_step 200\n", "")
+            text = text.replace("sim run\n", "sim final_time 1.0\nsim final_step_add 3\nsim run\n"
+                                'sim final_step_add 60\nsim state_file "out.bin"\nsim run\n', 1)
+        open(path, "w").write(text)
+        cuda_lib.run_casl(path)
+        states.append(np.fromfile(d / "out.bin", dtype=np.float64, offset=8))
+    assert np.array_equal(states[0], states[1])
+
+
 @pytest.mark.gpu
 def test_final_time_counts_steps_like_the_reference(cuda_lib, tmp_path):
     """final_time T runs (int)T / dt steps, the reference's conversion

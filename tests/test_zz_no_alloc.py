@@ -77,9 +77,18 @@ def test_noalloc_structure_factor_matches_regular_path(cuda_lib):
 
 
 def test_noalloc_rejects_sizes_beyond_the_maximum(cuda_lib):
+    import torch
     f = _entry(cuda_lib)
     box = (ctypes.c_double * 3)(10.0, 10.0, 10.0)
     err = ctypes.create_string_buffer(256)
-    dummy = ctypes.c_void_p(16)  # never dereferenced: the call must fail before any launch
-    rc = f(dummy, dummy, 100, box, 31, 31, 31, dummy, None, err, 256)
+    # real device buffers of the stated sizes, so that nothing could read
+    # through a bad address even if a check came after a launch
+    pos = torch.zeros((100, 3), dtype=torch.float64, device="cuda")
+    q = torch.zeros(100, dtype=torch.float64, device="cuda")
+    out = torch.zeros((8, 2), dtype=torch.float64, device="cuda")
+    rc = f(pos.data_ptr(), q.data_ptr(), 100, box, 31, 31, 31, out.data_ptr(), None, err, 256)
     assert rc == 1 and b"k_max" in err.value
+    rc = f(pos.data_ptr(), q.data_ptr(), 0, box, 1, 1, 1, out.data_ptr(), None, err, 256)
+    assert rc == 1
+    torch.cuda.synchronize()
+    assert not out.any()
