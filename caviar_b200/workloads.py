@@ -175,9 +175,11 @@ def random_ions(n: int, box: float, seed: int, min_sep: float = 0.9, temperature
                     ewald_k=ek, name=f"ions_N{n}_L{box:g}")
 
 
-def config_lj_4000(seed: int = 1) -> MDSystem:
-    """4000 LJ atoms, FCC 10^3 cells, rho* = 0.8442, T* = 0.72, rc 2.5, skin 0.3, dt 0.005."""
-    return fcc_lattice(10, 0.8442, 0.72, seed)
+def config_lj_4000(seed: int = 1, jitter: float = 0.0) -> MDSystem:
+    """4000 LJ atoms, FCC 10^3 cells, rho* = 0.8442, T* = 0.72, rc 2.5, skin 0.3, dt 0.005
+    (jitter > 0 displaces the lattice sites, for force checks away from the
+    perfect lattice, where every force vanishes)."""
+    return fcc_lattice(10, 0.8442, 0.72, seed, jitter=jitter)
 
 
 def config_ions_8000(seed: int = 2) -> MDSystem:
@@ -185,9 +187,10 @@ def config_ions_8000(seed: int = 2) -> MDSystem:
     return random_ions(8000, 40.0, seed)
 
 
-def config_lj_1m(seed: int = 3) -> MDSystem:
-    """1,048,576 LJ atoms, FCC 64^3 cells, rho* = 0.8442, T* = 0.72, rc 2.5, skin 0.3."""
-    return fcc_lattice(64, 0.8442, 0.72, seed)
+def config_lj_1m(seed: int = 3, jitter: float = 0.0) -> MDSystem:
+    """1,048,576 LJ atoms, FCC 64^3 cells, rho* = 0.8442, T* = 0.72, rc 2.5, skin 0.3
+    (jitter as in config_lj_4000)."""
+    return fcc_lattice(64, 0.8442, 0.72, seed, jitter=jitter)
 
 
 @dataclasses.dataclass

@@ -47,8 +47,25 @@ GPU tests never need the reference at run time).
    the slab Ewald sum: forces and a 10-step run with the normal axis z, and
    forces with the normal axis x.
 
-Usage:  python tests/golden/make_golden.py [/path/to/reference]
+9. ref_bench_lj4000.npz, ref_bench_ions8000.npz, ref_bench_lj1m.npz -- the
+   unmodified reference on the benchmark systems themselves (the seeded
+   generators of caviar_b200.workloads: 4000-atom LJ fluid, 8000 ions with
+   Ewald alpha 0.3 / rc 10 / kmax 8, the 1,048,576-atom LJ fluid): the
+   SHA-256 and size of its canonical pair set (checked here against the C
+   restatement's, so the restatement is pinned at these sizes too),
+   accelerations (every one for the two small systems, every 64th atom by
+   id for the 1M system), virial, kinetic energy, S(k) and the k-space and
+   self energies, and short trajectories (100 steps of the 4000-atom fluid,
+   3 of the ions) under the reference's own rebuild trigger.  The LJ force
+   states are the generators' lattices with sites displaced by up to 0.1
+   (every force vanishes on the perfect lattice); the trajectories start
+   from the benchmark states themselves.
+
+Usage:  python tests/golden/make_golden.py [/path/to/reference] [--bench-only]
+The reference root defaults to $CAVIAR_REFERENCE_ROOT, else to a directory
+named `reference` beside this repository.
 """
+import hashlib
 import json
 import os
 import re
@@ -299,8 +316,61 @@ def random_velocity500(seed: int = 7, amplitude: float = 1.5) -> None:
                         box=s.box, seed=seed, amplitude=amplitude, vel=r["vel"].reshape(-1, 3)[order])
 
 
+def pair_digest(pairs: np.ndarray) -> str:
+    """SHA-256 of a canonical pair set (n x 5 int32, little endian, row major)."""
+    return hashlib.sha256(np.ascontiguousarray(pairs, dtype="<i4").tobytes()).hexdigest()
+
+
+BENCH_SYSTEMS = {
+    # name: (generator, keyword arguments of the force state, trajectory steps,
+    #        stride of the stored accelerations).  The LJ force states displace
+    #        the lattice sites by up to 0.1 (on the perfect lattice every force
+    #        vanishes); trajectories start from the benchmark state itself.
+    "lj4000": (W.config_lj_4000, {"jitter": 0.1}, 100, 1),
+    "ions8000": (W.config_ions_8000, {}, 3, 1),
+    "lj1m": (W.config_lj_1m, {"jitter": 0.1}, 0, 64),
+}
+
+
+def bench_systems() -> None:
+    for name, (gen, kw, nsteps, stride) in BENCH_SYSTEMS.items():
+        s = gen(**kw)
+        f = O.run_reference(s, "forces")
+        order = np.argsort(f["id"].astype(np.int64))
+        acc = f["acc"].reshape(-1, 3)[order]
+        pairs = f["pairs"].reshape(-1, 5)
+        o = O.Oracle(s)
+        o.setup()
+        opairs = o.pairs()
+        assert np.array_equal(opairs, pairs), f"{name}: restatement pair set differs from the reference's"
+        del opairs
+        d = dict(generator=gen.__name__, generator_kwargs=json.dumps(kw), n=s.n, pairs_sha256=pair_digest(pairs),
+                 npairs=pairs.shape[0],
+                 acc_stride=stride, ref_acc=acc[::stride], ref_virial=f["virial"], ref_ke=f["ke"],
+                 ref_sk=f.get("sk", np.zeros(0)), ref_ek=f.get("ek_kspace", 0.0), ref_eself=f.get("ek_self", 0.0),
+                 run_steps=nsteps)
+        if nsteps:
+            r = O.run_reference(gen(), "run", nsteps=nsteps)
+            order = np.argsort(r["id"].astype(np.int64))
+            d.update(run_pos=r["pos"].reshape(-1, 3)[order], run_vel=r["vel"].reshape(-1, 3)[order],
+                     run_ke=r["ke_trace"])
+        np.savez_compressed(os.path.join(HERE, f"ref_bench_{name}.npz"), **d)
+        print(name, "pairs", pairs.shape[0], "ok")
+
+
+def reference_root() -> str:
+    args = [a for a in sys.argv[1:] if not a.startswith("--")]
+    if args:
+        return args[0]
+    return os.environ.get("CAVIAR_REFERENCE_ROOT", os.path.join(os.path.dirname(ROOT), "reference"))
+
+
 def main():
-    ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref_root = reference_root()
+    if "--bench-only" in sys.argv:
+        O.build(ref_root)
+        bench_systems()
+        return
     g = ewald_n100(ref_root)
     with open(os.path.join(HERE, "ewald_n100.json"), "w") as f:
         json.dump(g, f, indent=0)
@@ -315,6 +385,7 @@ def main():
     ewald_slab()
     slab_correction()
     random_velocity500()
+    bench_systems()
     print("golden fixtures written to", HERE)
 
 

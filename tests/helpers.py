@@ -9,6 +9,10 @@ from caviar_b200 import workloads as W
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 
+def golden_path(name):
+    return os.path.join(GOLDEN, name)
+
+
 def load_ref_fixture(name):
     d = np.load(os.path.join(GOLDEN, f"ref_{name}.npz"))
     T = len(d["mass"])

@@ -9,7 +9,7 @@ Tolerances (stated here, used below):
   * pair sets: bit-exact (same sorted canonical pair set);
   * FP64 form: accelerations within 1e-12 relative (global), energies/virial 1e-11;
   * mixed form: global relative force error ||dF|| / ||F|| <= 1e-5 and
-    per-atom max |dF_i| <= 1e-4 * rms|F|; energies/virial 1e-5 relative.
+    per-atom max |dF_i| <= 1e-5 * rms|F|; energies/virial 1e-5 relative.
 """
 import numpy as np
 import pytest
@@ -34,7 +34,7 @@ def check_forces(acc, ref, prec):
         assert g < 1e-12, (g, mx)
     else:
         assert g <= 1e-5, (g, mx)
-        assert mx <= 1e-4, (g, mx)
+        assert mx <= 1e-5, (g, mx)
     return g, mx
 
 
@@ -339,3 +339,29 @@ def test_graph_and_stream_paths_agree(cuda_lib):
     _, vel, _ = a.state()
     v = vel - vel.mean(axis=0)
     assert abs(th_a[-1, 1] - 0.5 * np.sum(v * v)) < 1e-10 * th_a[-1, 1]
+
+
+def test_changed_dt_reaches_the_step_graphs(cuda_lib):
+    """cvr_set_integrator between two runs: the graph path (which bakes dt
+    and k_b into its kernels) must follow the new values exactly like the
+    stream path, which reads them at every launch."""
+    from caviar_b200 import workloads as W
+    s = W.fcc_lattice(6, 0.8442, 0.72, seed=9, jitter=0.05)
+    a = sim_for(cuda_lib, s, "mixed")
+    b = sim_for(cuda_lib, s, "mixed")
+    b.set_kernel_timing(True)
+    for sim in (a, b):
+        sim.run(20)
+        sim.set_integrator(0.5 * s.dt, 2.0)
+    th_a = a.run(20, 10)
+    th_b = b.run(20, 10)
+    for x, y in zip(a.state(), b.state()):
+        assert np.array_equal(x, y)
+    assert np.array_equal(th_a, th_b)
+    # and the run really used the new values: a fresh context with them from the start
+    c = sim_for(cuda_lib, s, "mixed")
+    c.set_integrator(s.dt, 2.0)
+    c.run(20)
+    c.set_integrator(0.5 * s.dt, 2.0)
+    th_c = c.run(20, 10)
+    assert np.array_equal(th_a, th_c)
