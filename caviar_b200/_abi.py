@@ -97,8 +97,19 @@ def load(path: str = LIB_PATH):
     L.cvr_get_info.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), ctypes.c_int]
     L.cvr_set_kernel_timing.argtypes = [vp, ctypes.c_int]
     L.cvr_kernel_time.argtypes = [vp, ctypes.c_int, _dp, ctypes.POINTER(ctypes.c_int64)]
+    L.cvr_measure_fma_peak.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, _dp]
     _lib = L
     return L
+
+
+def fma_peak(device: int = 0, fp64: bool = False, iters: int = 2000):
+    """(TFLOP/s, ms) of the FMA-only peak kernel (cvr_measure_fma_peak)."""
+    L = load()
+    tf, ms = ctypes.c_double(0), ctypes.c_double(0)
+    rc = L.cvr_measure_fma_peak(device, int(fp64), iters, ctypes.byref(tf), ctypes.byref(ms))
+    if rc != OK:
+        raise CvrError(rc, "cvr_measure_fma_peak failed")
+    return tf.value, ms.value
 
 
 def run_casl(path: str) -> None:
@@ -182,6 +193,10 @@ class Simulation:
             kx, ky, kz = s.ewald_k.kmax
             self._check(self.L.cvr_set_ewald_k(self.h, s.ewald_k.alpha, kx, ky, kz, s.ewald_k.k_electrostatic))
         self._check(self.L.cvr_set_integrator(self.h, s.dt, s.k_b))
+
+    def set_integrator(self, dt: float, k_b: float = 1.0):
+        """md_simulator dt / atom_data k_b (md_simulator.cpp:58-233)."""
+        self._check(self.L.cvr_set_integrator(self.h, dt, k_b))
 
     def set_langevin(self, temperature: float, friction: float, kb: float = -1.0, kbt: float = -1.0,
                      rng: int = RNG_REFERENCE, seed: int = 0):

@@ -11,7 +11,7 @@ ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libcaviar_b200.so")
 SOURCES = [os.path.join(HERE, "csrc", "cvr_abi.cu"), os.path.join(HERE, "csrc", "cvr_noalloc.cu"),
            os.path.join(HERE, "csrc", "cvr_casl.cpp"), os.path.join(HERE, "csrc", "cvr_batch.cu"),
-           os.path.join(HERE, "csrc", "cvr_adjoint.cu")]
+           os.path.join(HERE, "csrc", "cvr_adjoint.cu"), os.path.join(HERE, "csrc", "cvr_peaks.cu")]
 CLI = os.path.join(HERE, "caviar_b200_casl")
 DEPS = SOURCES + [os.path.join(HERE, "csrc", f) for f in ("cvr_device.cuh", "cvr_build.cuh", "cvr_force.cuh", "cvr_main.cpp")] + [
     os.path.join(ROOT, "include", "caviar_b200.h")]

@@ -220,6 +220,13 @@ void *cvr_get_stream(const cvr_ctx *ctx);         /* the cudaStream_t the contex
  * cvr_set_precision). */
 int cvr_get_info(const cvr_ctx *ctx, int64_t *out, int len);
 
+/* Arithmetic-pipe peak of `device` for the compute side of the roofline (no
+ * reference counterpart): a kernel of independent fused multiply-adds only
+ * (FP32, or FP64 when fp64 != 0) filling every SM, `iters` rounds of 128 FMAs
+ * per thread, best of 5 launches timed with CUDA events; *tflops = 2 flops
+ * per FMA / time, *ms = that launch's time.  Synchronous. */
+int cvr_measure_fma_peak(int device, int fp64, int iters, double *tflops, double *ms);
+
 /* Kernel timing: when on, CUDA events bracket every launch of the named
  * kernel class on the context's stream; cvr_kernel_time returns the summed
  * milliseconds and the launch count since the last reset. */
@@ -338,9 +345,11 @@ int cvr_casl_run_file(const char *path, char *err, size_t err_len);
  *
  * Scratch: the chunk partial sums use one fixed device array of
  * CVR_NOALLOC_SK_SCRATCH complex doubles per GPU, held until process exit.
- * More k-vectors than that -> CVR_ERR_CAPACITY; k_max above 30 -> CVR_ERR_INVALID.
- * The first call on each device looks up that array's device address; make it
- * before any stream capture.  All calls share the array and it keeps the last
+ * Limit: k_max <= 30 per axis (at most 216000 k-vectors, which always fit);
+ * a larger k_max, n <= 0 or n > 2^30 -> CVR_ERR_INVALID before any launch.
+ * The first call on each device looks up that array's device address and
+ * keeps it for the process; make it before any stream capture, and do not
+ * call again on a device after cudaDeviceReset.  All calls share the array and it keeps the last
  * call's contents (every partial is written before it is read, so nothing
  * needs clearing); calls whose kernels overlap on the GPU race on it. */
 int cvr_structure_factor_noalloc(const double *pos, const double *q, int64_t n, const double box_len[3],
