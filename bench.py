@@ -160,6 +160,26 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
+def fma_peaks(abi, device: int):
+    """FP32 and FP64 FMA-pipe peaks of this GPU, measured now (cvr_measure_fma_peak:
+    FMA-only kernel filling every SM, best of 5, CUDA events), TFLOP/s."""
+    try:
+        f32, _ = abi.fma_peak(device, False, 2000)
+        f64, _ = abi.fma_peak(device, True, 1000)
+        return {"fp32_tflops": f32, "fp64_tflops": f64, "source": "cvr_measure_fma_peak, measured in this run"}
+    except Exception as e:  # pragma: no cover - reported, not hidden
+        return {"fp32_tflops": None, "fp64_tflops": None, "source": f"failed: {e}"}
+
+
+def lj_pair_flops_per_atom(n_cand: float, density: float, rc: float) -> float:
+    """Algorithmic FP32 flops of one atom's row in the LJ pair kernel: 8 per
+    list entry (displacement 3, r^2 5) and 15 more per pair inside rc (1/r^2,
+    (s/r)^6, the force coefficient and three force FMAs), FMA = 2; the pairs
+    inside rc of a uniform fluid number rho (4/3) pi rc^3."""
+    n_rc = density * 4.0 / 3.0 * np.pi * rc ** 3
+    return 8.0 * n_cand + 15.0 * n_rc
+
+
 def profiled_traffic(name: str):
     """dram bytes per launch of a kernel, from a committed ncu summary (profiles/)."""
     path = os.path.join(ROOT, "profiles", name)
@@ -239,9 +259,16 @@ def ions_line(abi, W, torch, steps: int, warmup: int, device: int = 0):
         kms, kn = si.kernel_time(abi.KT_KSPACE)
         pms, pn = si.kernel_time(abi.KT_PAIR)
         bms, _ = si.kernel_time(abi.KT_BUILD)
+        nk = si.info()["nk"]
         ion[nm] = {"value": s_ion.n * steps / (msi / 1e3), "ms_per_step": msi / steps,
                    "kernel_window_ms_per_step": msk / steps, "kspace_ms_per_step": kms / max(kn, 1),
-                   "pair_ms_per_step": pms / max(pn, 1), "build_ms_per_step": bms / steps}
+                   "pair_ms_per_step": pms / max(pn, 1), "build_ms_per_step": bms / steps,
+                   # algorithmic flops of the k-space pass: S(k) and the force each 4 FMA
+                   # (8 flops) per (k-vector, atom); of the pair pass: ~45 per list entry
+                   "kspace_flops_per_step": 2 * 8.0 * nk * s_ion.n,
+                   "kspace_tflops": 2 * 8.0 * nk * s_ion.n / (kms / max(kn, 1) / 1e3) / 1e12 if kms > 0 else None,
+                   "pair_tflops": 45.0 * si.info()["list_entries"] * 1.0 / (pms / max(pn, 1) / 1e3) / 1e12
+                   if pms > 0 else None}
         si.close()
     return ion
 
@@ -307,6 +334,7 @@ def gpu_arm(args):
     from caviar_b200 import workloads as W
 
     steps, warmup = args.steps, max(3, args.warmup)
+    peaks = fma_peaks(abi, local)
     s_lj = W.config_lj_1m(seed=3 + rank)
     n = s_lj.n
 
@@ -383,11 +411,23 @@ def gpu_arm(args):
     pair_avg_ms = pair_ms / max(pair_n, 1)
     achieved = bytes_launch / (pair_avg_ms / 1e3) / 1e9
     traffic = profiled_traffic("pair_lj1m.txt")
+    density = n / float(np.prod(np.asarray(s_lj.hi) - np.asarray(s_lj.lo)))
+    flops_launch = n * lj_pair_flops_per_atom(mean_cnt, density, s_lj.lj.cutoff)
+    fp32_achieved = flops_launch / (pair_avg_ms / 1e3) / 1e12
+    fp32_peak = peaks["fp32_tflops"]
+    # roofline: the pair kernel's arithmetic intensity against the ridge point
+    # (FP32 peak / HBM peak) says which roof binds it
+    ai = flops_launch / bytes_launch
+    ridge = (fp32_peak * 1e12) / (peak * 1e9) if fp32_peak else None
+    bound = "hbm" if (ridge is None or ai < ridge) else "fp32"
     sim.close()
 
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(s_lj, budget_s=args.cpu_budget)
+        sec["ions_8k_mixed"]["cpu_baseline"] = cpu_baseline_ions(min(15.0, args.cpu_budget))
+        sec["replicas_1024"]["cpu_baseline"] = cpu_baseline_replicas(min(10.0, args.cpu_budget))
+        sec["adjoint_4000"]["cpu_baseline"] = cpu_baseline_adjoint()
 
     if rank == 0:
         line = {
@@ -402,9 +442,15 @@ def gpu_arm(args):
                            int(4 * mean_cnt * n / 1e6), int(n * 24 / 1e6)),
                        "rebuild_policy": "displacement (skin/2)", "list_builds_in_window": builds,
                        "mean_neighbours": mean_cnt},
-            "roofline": {"bound": "hbm", "kernel": "k_pair (LJ, full Verlet list)", "achieved": achieved,
+            "roofline": {"bound": bound, "kernel": "k_pair (LJ, full Verlet list)", "achieved": achieved,
                          "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                          "peak_source": peak_kind, "bytes_per_launch": bytes_launch,
+                         "fp32": {"achieved": fp32_achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                                  "frac": fp32_achieved / fp32_peak if fp32_peak else None,
+                                  "flops_per_launch": flops_launch, "peak_source": peaks["source"]},
+                         "arithmetic_intensity_flop_per_byte": ai, "ridge_flop_per_byte": ridge,
+                         "limiter": "neither roof: latency of the neighbour gathers (ncu: long-scoreboard "
+                                    "stalls, profiles/pair_lj1m.txt)",
                          "avg_launch_ms": pair_avg_ms, "launches": pair_n,
                          "share_of_step": pair_ms / ms_k if ms_k > 0 else None,
                          "timing": "pair kernel bracketed by CUDA events on the context stream over a second "
@@ -417,6 +463,7 @@ def gpu_arm(args):
                     "note": "cvr_set_state from pinned host buffers + cvr_run (setup, K steps, per-step thermo "
                             "record read back) + cvr_get_state to pinned host buffers"},
             "gpu_launches": launches,
+            "fma_peaks": peaks,
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
             "secondary": sec,
@@ -452,6 +499,76 @@ def cpu_baseline(s, budget_s: float = 20.0):
     return {"value": s.n / per, "unit": UNIT, "cores": 1, "kind": "reference",
             "sample": f"{k} velocity-Verlet steps of the same {s.n}-atom system after a setup step "
                       f"({first:.1f} s); serial reference (its OpenMP build does not compile)"}
+
+
+def cpu_baseline_ions(budget_s: float = 15.0):
+    """The unmodified reference on the 8000-ion Ewald system (config of the
+    ions line): whole steps after its setup step until budget_s, 1 core."""
+    from caviar_b200 import workloads as W
+    s = W.config_ions_8000(seed=2)
+    try:
+        res = reference_step_time(s, 100, budget_s)
+    except Exception as e:  # pragma: no cover - reported, not hidden
+        return {"value": None, "unit": UNIT, "cores": 1, "kind": "reference", "sample": f"failed: {e}"}
+    if res is None:
+        return {"value": None, "unit": UNIT, "cores": 1, "kind": "reference", "sample": "harness not built"}
+    per, k, first = res
+    return {"value": s.n / per, "unit": UNIT, "cores": 1, "kind": "reference",
+            "sample": f"{k} velocity-Verlet steps of the same 8000-ion system after a setup step ({first:.1f} s)"}
+
+
+def cpu_baseline_replicas(budget_s: float = 10.0, procs: int = 8):
+    """The unmodified reference on replicas of the batch, one process per
+    core running concurrently: the replicas at the batch's size octiles
+    (its sizes are uniform, so they represent it), each advanced whole steps
+    until budget_s after its setup step; aggregate = sum of each process's
+    atom-steps/s.  Each replica runs with neighbour-list radius = ghost
+    cutoff = L/2 (cutoff_extra_coef 1), the largest its one-ghost-image
+    scheme allows (workloads.replica_system)."""
+    from concurrent.futures import ThreadPoolExecutor
+    from caviar_b200 import workloads as W
+    from oracle import oracle as O
+    if not O.harness_available():
+        return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": "harness not built"}
+    procs = max(1, min(procs, os.cpu_count() or 1))
+    b = W.replica_batch()
+    order = np.argsort(b.n, kind="stable")
+    picks = [int(order[min(len(order) - 1, int((q + 0.5) * len(order) / procs))]) for q in range(procs)]
+
+    def one(r):
+        s = W.replica_system(b, r)
+        res = O.run_reference(s, "run", nsteps=100000, budget_s=budget_s, timeout=budget_s * 10 + 300)
+        k = int(res["steps_done"]) - 1
+        return s.n, float(res["wall_rest"]) / max(k, 1), k
+    try:
+        with ThreadPoolExecutor(procs) as ex:
+            got = list(ex.map(one, picks))
+    except Exception as e:  # pragma: no cover - reported, not hidden
+        return {"value": None, "unit": UNIT, "cores": procs, "kind": "reference", "sample": f"failed: {e}"}
+    value = sum(n / per for n, per, _ in got)
+    return {"value": value, "unit": UNIT, "cores": procs, "kind": "reference",
+            "sample": f"{procs} concurrent reference processes, replicas of " +
+                      ", ".join(f"{n} atoms ({k} steps)" for n, _, k in got) +
+                      " (the batch's size octiles), aggregate of their atom-steps/s"}
+
+
+def cpu_baseline_adjoint(nsteps: int = 3):
+    """The FP64 C restatement of the trajectory adjoint (oracle/adjoint.c; the
+    reference has no gradients) on the 4000-atom mixture: loss and full
+    gradient of an nsteps-step trajectory with a checkpoint every step
+    (forward, re-run segments, reverse sweep), 1 core."""
+    from caviar_b200 import workloads as W
+    from oracle import oracle as O
+    s = W.adjoint_mixture()
+    try:
+        a = O.AdjOracle(s)
+        t0 = time.perf_counter()
+        a.loss_grad(s.pos, s.vel, nsteps, 1)
+        dt = time.perf_counter() - t0
+    except Exception as e:  # pragma: no cover - reported, not hidden
+        return {"value": None, "unit": "gradient atom-steps/s", "cores": 1, "kind": "port", "sample": f"failed: {e}"}
+    return {"value": 4000 * nsteps / dt, "unit": "gradient atom-steps/s", "cores": 1, "kind": "port",
+            "sample": f"loss + gradient over {nsteps} steps, checkpoint every step ({dt:.1f} s), FP64 restatement"}
 
 
 def reference_arm(args):

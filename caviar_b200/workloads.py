@@ -251,6 +251,27 @@ def replica_batch(n_rep: int = 1024, seed: int = 4, n_min: int = 64, n_max: int 
                         rc_r=boxes / 2)
 
 
+def replica_system(b: ReplicaBatch, r: int) -> MDSystem:
+    """Replica r as a system the reference's own objects can run: neighbour
+    list radius = ghost cutoff = L/2 with cutoff_extra_coef 1 (the largest
+    radius its one-ghost-image scheme allows, so its Ewald real-space sum,
+    which has no cutoff of its own, covers the replica's minimum-image pairs
+    within L/2; the list is rebuilt every step), LJ up to rc_lj, Ewald alpha
+    and k_max as the batch."""
+    o = b.offsets
+    sl = slice(int(o[r]), int(o[r + 1]))
+    L = float(b.box[r])
+    T = len(b.mass)
+    return MDSystem(lo=np.zeros(3), hi=np.full(3, L), mass=np.asarray(b.mass, np.float64),
+                    charge=np.asarray(b.charge, np.float64), pos=b.pos[sl].copy(), vel=b.vel[sl].copy(),
+                    type=b.type[sl].astype(np.int32), cutoff=0.5 * L, coef=1.0, ghost_cutoff=0.5 * L, dt=b.dt,
+                    lj=LJParams(cutoff=float(b.rc_lj[r]), epsilon=np.asarray(b.epsilon).reshape(T, T),
+                                sigma=np.asarray(b.sigma).reshape(T, T)),
+                    ewald_r=EwaldRParams(alpha=b.alpha, k_electrostatic=b.k_e),
+                    ewald_k=EwaldKParams(alpha=b.alpha, kmax=(b.kmax, b.kmax, b.kmax), k_electrostatic=b.k_e),
+                    name=f"replica{r}_N{int(b.n[r])}")
+
+
 @dataclasses.dataclass
 class AdjointSystem:
     """One periodic cube for the trajectory adjoint: LJ + Ewald (explicit

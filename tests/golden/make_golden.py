@@ -61,7 +61,14 @@ GPU tests never need the reference at run time).
    (every force vanishes on the perfect lattice); the trajectories start
    from the benchmark states themselves.
 
-Usage:  python tests/golden/make_golden.py [/path/to/reference] [--bench-only]
+10. ref_replicas.npz -- the unmodified reference on twelve replicas of the
+   batch workload (64 ... 2048 atoms, every size class boundary), each run as
+   its own system with neighbour-list radius = ghost cutoff = L/2
+   (cutoff_extra_coef 1, the largest its one-ghost-image scheme allows; its
+   Ewald real-space sum then covers the minimum-image pairs within L/2):
+   accelerations, virial, kinetic energy, k-space and self energies.
+
+Usage:  python tests/golden/make_golden.py [/path/to/reference] [--bench-only | --replicas-only]
 The reference root defaults to $CAVIAR_REFERENCE_ROOT, else to a directory
 named `reference` beside this repository.
 """
@@ -316,6 +323,32 @@ def random_velocity500(seed: int = 7, amplitude: float = 1.5) -> None:
                         box=s.box, seed=seed, amplitude=amplitude, vel=r["vel"].reshape(-1, 3)[order])
 
 
+# replica sizes of the batch tests: every size class and class boundary
+REPLICA_SIZES = [64, 100, 257, 511, 512, 513, 777, 1024, 1025, 1500, 2047, 2048]
+
+
+def replicas() -> None:
+    """The unmodified reference on each replica of replica_batch(sizes=
+    REPLICA_SIZES, seed=5), run as its own system (workloads.replica_system:
+    list radius = ghost cutoff = L/2, cutoff_extra_coef 1): accelerations in
+    id order, virial, kinetic energy, k-space and self energies."""
+    b = W.replica_batch(sizes=REPLICA_SIZES, seed=5)
+    out = {"sizes": np.asarray(REPLICA_SIZES), "seed": 5}
+    acc, vir, ke, ek, es = [], [], [], [], []
+    for r in range(len(REPLICA_SIZES)):
+        s = W.replica_system(b, r)
+        f = O.run_reference(s, "forces")
+        order = np.argsort(f["id"].astype(np.int64))
+        acc.append(f["acc"].reshape(-1, 3)[order])
+        vir.append(float(f["virial"]))
+        ke.append(float(f["ke"]))
+        ek.append(float(f["ek_kspace"]))
+        es.append(float(f["ek_self"]))
+    out.update(acc=np.concatenate(acc), virial=np.asarray(vir), ke=np.asarray(ke), e_k=np.asarray(ek),
+               e_self=np.asarray(es))
+    np.savez_compressed(os.path.join(HERE, "ref_replicas.npz"), **out)
+
+
 def pair_digest(pairs: np.ndarray) -> str:
     """SHA-256 of a canonical pair set (n x 5 int32, little endian, row major)."""
     return hashlib.sha256(np.ascontiguousarray(pairs, dtype="<i4").tobytes()).hexdigest()
@@ -371,6 +404,10 @@ def main():
         O.build(ref_root)
         bench_systems()
         return
+    if "--replicas-only" in sys.argv:
+        O.build(ref_root)
+        replicas()
+        return
     g = ewald_n100(ref_root)
     with open(os.path.join(HERE, "ewald_n100.json"), "w") as f:
         json.dump(g, f, indent=0)
@@ -386,6 +423,7 @@ def main():
     slab_correction()
     random_velocity500()
     bench_systems()
+    replicas()
     print("golden fixtures written to", HERE)
 
 

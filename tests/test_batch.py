@@ -2,7 +2,10 @@
 persistent CTA per replica, all replicas in one graph launch.
 
 CPU: the minimum-image replica oracle agrees with the reference-pinned
-restatement on a box large enough for the reference's one-ghost-image scheme;
+restatement on a box large enough for the reference's one-ghost-image scheme,
+and with the unmodified reference itself on twelve replicas of the batch
+(tests/golden/ref_replicas.npz: each replica run by the reference as its own
+system with list radius = ghost cutoff = L/2);
 the 1024-replica generator has the stated shape; bad sizes are rejected.
 GPU: forces, energies and short trajectories of replicas across every size
 class agree with the FP64 replica oracle; split runs are bit-identical to one
@@ -12,7 +15,7 @@ import numpy as np
 import pytest
 
 from caviar_b200 import workloads as W
-from helpers import force_errors
+from helpers import force_errors, golden_path
 
 # Mixed precision: FP32 pair / k-space terms on hi/lo FP32 coordinates, FP64 sums.
 FORCE_TOL = 1e-5  # global ||dF|| / ||F||
@@ -57,6 +60,45 @@ def test_replica_oracle_matches_restatement(oracle_lib):
     for k_rep, k_orc in (("e_lj", "e_lj"), ("e_ewald_r", "e_ewald_r"), ("e_ewald_k", "e_ewald_k"),
                          ("e_self", "e_self"), ("virial", "virial")):
         assert abs(en[k_rep] - sc[k_orc]) <= 1e-10 * max(1.0, abs(sc[k_orc])), k_rep
+
+
+def reference_replicas():
+    d = np.load(golden_path("ref_replicas.npz"))
+    b = W.replica_batch(sizes=list(d["sizes"]), seed=int(d["seed"]))
+    return b, d
+
+
+def test_replica_oracle_matches_reference_at_batch_sizes(oracle_lib):
+    """The unmodified reference runs each replica as its own system when its
+    list radius and ghost cutoff are L/2 (cutoff_extra_coef 1); the
+    minimum-image replica oracle must give its accelerations, virial and
+    k-space / self energies on all twelve replicas (64 ... 2048 atoms)."""
+    b, d = reference_replicas()
+    o = b.offsets
+    for r in range(len(b.n)):
+        f, en = oracle_forces(oracle_lib, b, r)
+        acc = f / b.mass[b.type[replica(b, r)]][:, None]
+        ref = d["acc"][int(o[r]):int(o[r + 1])]
+        assert force_errors(acc, ref)[0] < 1e-12, b.n[r]
+        assert abs(en["virial"] - d["virial"][r]) <= 1e-10 * abs(d["virial"][r]), b.n[r]
+        assert abs(en["e_ewald_k"] - d["e_k"][r]) <= 1e-10 * abs(d["e_k"][r]), b.n[r]
+        assert abs(en["e_self"] - d["e_self"][r]) <= 1e-12 * abs(d["e_self"][r]), b.n[r]
+
+
+@pytest.mark.gpu
+def test_batch_forces_vs_reference(cuda_lib):
+    """The batch kernel's accelerations against the unmodified reference's
+    own, replica by replica (mixed tolerances above)."""
+    b, d = reference_replicas()
+    bt = make_batch(cuda_lib, b)
+    bt.run(0)
+    _, _, acc = bt.state()
+    o = b.offsets
+    for r in range(len(b.n)):
+        sl = slice(int(o[r]), int(o[r + 1]))
+        g, m, _ = force_errors(acc[sl], d["acc"][sl])
+        assert g < FORCE_TOL and m < MAX_TOL, (int(b.n[r]), g, m)
+    bt.close()
 
 
 def test_generator_shape():
