@@ -14,13 +14,17 @@ GPU tests never need the reference at run time).
    systems: accelerations, canonical pair set, virial, kinetic energy, S(k),
    k-space and self energies, and a short trajectory.
 
-3. nve_lj500.json -- the reference's NVE energy record over 10^4 steps of a
-   500-atom LJ fluid (FCC 5^3 cells, rho* 0.8442, T* 0.72, rc 2.5, skin 0.3,
-   dt 0.005): ten harness runs of 1000 steps, each continuing from the
+3. nve_lj500.json, nve_ions500.json -- the reference's NVE energy record
+   every 100 steps over 10^4 steps of a 500-atom LJ fluid (FCC 5^3 cells,
+   rho* 0.8442, T* 0.72, rc 2.5, skin 0.3, dt 0.005) and of 500 ions (+-1,
+   L = 16, LJ rc 2.5, Ewald alpha 0.6, real-space list radius 5.15, kmax 4,
+   dt 0.005; the ions start from the reference's own state after 2000 steps,
+   past the random start's relaxation, stored in the record): a hundred
+   harness runs of 100 steps, each continuing from the
    previous run's final positions and velocities; total energy = the
-   reference's kinetic energy + the LJ energy of its linear force-shifted
-   potential (which the reference lacks; the restatement's formula) at the
-   reference's positions.
+   reference's kinetic energy + the potential energies the restatement
+   evaluates at the reference's positions (the reference has no LJ energy
+   and no list-consistent Ewald real-space energy).
 
 4. writer_lj500/ -- the files the reference's `writer atom_data` writes for
    a 40-step run of that fluid (energy and temperature every 5 steps,
@@ -68,7 +72,7 @@ GPU tests never need the reference at run time).
    Ewald real-space sum then covers the minimum-image pairs within L/2):
    accelerations, virial, kinetic energy, k-space and self energies.
 
-Usage:  python tests/golden/make_golden.py [/path/to/reference] [--bench-only | --replicas-only]
+Usage:  python tests/golden/make_golden.py [/path/to/reference] [--bench-only | --replicas-only | --nve-only]
 The reference root defaults to $CAVIAR_REFERENCE_ROOT, else to a directory
 named `reference` beside this repository.
 """
@@ -157,8 +161,14 @@ def save_ref(name, s, nsteps=20):
     np.savez_compressed(os.path.join(HERE, f"ref_{name}.npz"), **d)
 
 
-def nve_lj500(nblocks: int = 10, block: int = 1000) -> dict:
-    s = W.fcc_lattice(5, 0.8442, 0.72, seed=7, jitter=0.05)
+def nve_trace(s, nblocks: int = 100, block: int = 100) -> list:
+    """Total energy of the reference's own NVE run every `block` steps:
+    `nblocks` harness runs of `block` steps, each continuing from the previous
+    run's final positions and velocities (a restart recomputes the forces of
+    those positions, as the continuing run has them); the energy of each
+    state is the reference's kinetic energy plus the potential energies the
+    restatement evaluates there (LJ of the reference's linear force-shifted
+    potential, Ewald real space over the list pairs, k space, self)."""
     cur = s.copy()
     e = []
     o = O.Oracle(cur, policy=O.POLICY_REFERENCE)
@@ -166,7 +176,7 @@ def nve_lj500(nblocks: int = 10, block: int = 1000) -> dict:
         o.set_atoms(cur.pos, cur.vel, cur.type)
         o.build_list()
         sc = o.energy()
-        e.append(sc["ke"] + sc["e_lj"])
+        e.append(sc["ke"] + sc["e_lj"] + sc["e_ewald_r"] + sc["e_ewald_k"] + sc["e_self"])
         if b == nblocks:
             break
         r = O.run_reference(cur, "run", block)
@@ -174,10 +184,36 @@ def nve_lj500(nblocks: int = 10, block: int = 1000) -> dict:
         cur = cur.copy()
         cur.pos = r["pos"].reshape(-1, 3)[order]
         cur.vel = r["vel"].reshape(-1, 3)[order]
-    e = np.array(e)
-    return {"system": "fcc_lattice(5, 0.8442, 0.72, seed=7, jitter=0.05)", "steps_per_record": block,
-            "total_energy": e.tolist(), "n": s.n,
-            "max_abs_dev_per_atom": float(np.abs(e - e[0]).max() / s.n)}
+    return e
+
+
+NVE_SYSTEMS = {
+    "lj500": ("fcc_lattice(5, 0.8442, 0.72, seed=7, jitter=0.05)",
+              lambda: W.fcc_lattice(5, 0.8442, 0.72, seed=7, jitter=0.05)),
+    "ions500": ("random_ions(500, 16.0, seed=13, rc=5.0, kmax=4, alpha=0.6)",
+                lambda: W.random_ions(500, 16.0, seed=13, rc=5.0, kmax=4, alpha=0.6)),
+}
+
+
+def nve(name: str, nblocks: int = 100, block: int = 100, equilibrate: int = 0) -> dict:
+    """The trace of NVE_SYSTEMS[name]; with equilibrate > 0 the trace starts
+    from the reference's own state after that many steps (past the start's
+    relaxation transient) and the record holds that state."""
+    desc, make = NVE_SYSTEMS[name]
+    s = make()
+    out = {"system": desc, "steps_per_record": block, "n": s.n, "equilibrate_steps": equilibrate}
+    if equilibrate:
+        r = O.run_reference(s, "run", equilibrate)
+        order = np.argsort(r["id"].astype(np.int64))
+        s.pos = r["pos"].reshape(-1, 3)[order]
+        s.vel = r["vel"].reshape(-1, 3)[order]
+        out["pos0"] = s.pos.tolist()
+        out["vel0"] = s.vel.tolist()
+    out["total_energy"] = nve_trace(s, nblocks, block)
+    return out
+
+
+NVE_EQUILIBRATE = {"lj500": 0, "ions500": 2000}
 
 
 WRITER_SCRIPT = """writer atom_data w
@@ -404,6 +440,12 @@ def main():
         O.build(ref_root)
         bench_systems()
         return
+    if "--nve-only" in sys.argv:
+        O.build(ref_root)
+        for name in NVE_SYSTEMS:
+            with open(os.path.join(HERE, f"nve_{name}.json"), "w") as f:
+                json.dump(nve(name, equilibrate=NVE_EQUILIBRATE[name]), f)
+        return
     if "--replicas-only" in sys.argv:
         O.build(ref_root)
         replicas()
@@ -414,8 +456,9 @@ def main():
     O.build(ref_root)
     for name, s in small_systems().items():
         save_ref(name, s)
-    with open(os.path.join(HERE, "nve_lj500.json"), "w") as f:
-        json.dump(nve_lj500(), f, indent=0)
+    for name in NVE_SYSTEMS:
+        with open(os.path.join(HERE, f"nve_{name}.json"), "w") as f:
+            json.dump(nve(name, equilibrate=NVE_EQUILIBRATE[name]), f)
     writer_lj500()
     langevin500()
     thermostats()
