@@ -24,6 +24,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
 HARNESS_PATH = os.path.join(HERE, "_ref", "ref_harness")
+# the reference with the B200 integration layer (`md_simulator b200` / `b200_fp64`)
+HARNESS_B200_PATH = os.path.join(HERE, "_ref", "ref_harness_b200")
 
 POLICY_DISPLACEMENT = 0
 POLICY_REFERENCE = 1
@@ -36,11 +38,14 @@ _lib = None
 
 def build(reference_root: Optional[str] = None, quiet: bool = True) -> None:
     """Compile the restatement (and, when the reference sources are present,
-    the reference harness) with oracle/Makefile."""
+    the reference harness, and the reference with the B200 integration layer
+    when libcaviar_b200.so is built) with oracle/Makefile."""
     out = subprocess.DEVNULL if quiet else None
     subprocess.run(["make", "-C", HERE], check=True, stdout=out)
     if reference_root and os.path.isdir(reference_root):
         subprocess.run(["make", "-C", HERE, "-j8", "ref", f"REF={reference_root}"], check=True, stdout=out)
+        if os.path.exists(os.path.join(os.path.dirname(HERE), "caviar_b200", "libcaviar_b200.so")):
+            subprocess.run(["make", "-C", HERE, "ref_b200", f"REF={reference_root}"], check=True, stdout=out)
 
 
 def lib():
@@ -280,7 +285,8 @@ class AdjOracle:
 # --------------------------------------------------------------- reference
 
 
-def casl_script(system, nsteps: int = 1, rebuild_test: bool = False, extra: str = "") -> str:
+def casl_script(system, nsteps: int = 1, rebuild_test: bool = False, extra: str = "",
+                simulator: str = "basic") -> str:
     """The CASL objects of the hot path, with the reference's own keywords
     (domain.cpp:206-266, atom_data.cpp:78-306, neighborlist.cpp:193-251,
     lj.cpp:42-147, electrostatic_ewald_r.cpp:38-88, electrostatic_ewald_k.cpp:48-143,
@@ -327,7 +333,7 @@ def casl_script(system, nsteps: int = 1, rebuild_test: bool = False, extra: str 
                   f"f_ek kx_max {kx}", f"f_ek ky_max {ky}", f"f_ek kz_max {kz}",
                   f"f_ek k_electrostatic {r(float(s.ewald_k.k_electrostatic))}",
                   "f_ek set_atom_data adata", "f_ek set_domain dom"]
-    lines += ["md_simulator basic sim", "sim set_atom_data adata", "sim integrator_type velocity_verlet"]
+    lines += [f"md_simulator {simulator} sim", "sim set_atom_data adata", "sim integrator_type velocity_verlet"]
     for f in ffs:
         lines.append(f"sim add_force_field {f}")
     lines += ["sim add_neighborlist neigh", "sim initial_step 0", f"sim final_step {max(1, nsteps)}",
@@ -376,23 +382,27 @@ def harness_available() -> bool:
 
 def run_reference(system, mode: str = "forces", nsteps: int = 0, rebuild_test: bool = False,
                   timeout: Optional[float] = None, budget_s: float = 0.0, extra: str = "",
-                  collect=(), mode_args=()) -> Dict[str, np.ndarray]:
+                  collect=(), mode_args=(), simulator: str = "basic",
+                  harness: str = HARNESS_PATH) -> Dict[str, np.ndarray]:
     """Run the unmodified reference on `system` ("forces" or "run") and return
     its FP64 output blocks plus the harness's own wall time.  budget_s > 0
     stops a run after the step that crosses the budget (at least 2 steps).
     `extra` is appended to the script (e.g. writer objects); the text of the
     files named in `collect` (written by the reference in its working
-    directory) comes back under "files"."""
-    if not harness_available():
-        raise FileNotFoundError(f"reference harness not built: {HARNESS_PATH}")
+    directory) comes back under "files".  Mode "runcall" calls the script's
+    simulator's own run(); `simulator` names its class (e.g. "b200" with
+    harness=HARNESS_B200_PATH, the reference built with the B200 integration
+    layer)."""
+    if not os.path.exists(harness):
+        raise FileNotFoundError(f"reference harness not built: {harness}")
     with tempfile.TemporaryDirectory() as d:
         script = os.path.join(d, "sys.casl")
         state = os.path.join(d, "state.bin")
         out = os.path.join(d, "out.bin")
         with open(script, "w") as f:
-            f.write(casl_script(system, nsteps, rebuild_test, extra))
+            f.write(casl_script(system, nsteps, rebuild_test, extra, simulator))
         write_state(state, system)
-        args = [HARNESS_PATH, script, state, mode, out] + ([str(nsteps), repr(float(budget_s))] if mode == "run" else [])
+        args = [harness, script, state, mode, out] + ([str(nsteps), repr(float(budget_s))] if mode == "run" else [])
         args += [str(x) for x in mode_args]  # e.g. randvel: seed, amplitude
         t0 = time.perf_counter()
         p = subprocess.run(args, cwd=d, capture_output=True, text=True, timeout=timeout)

@@ -7,6 +7,7 @@
 //   ref_harness <script.casl> <state.bin> forces <out.bin>
 //   ref_harness <script.casl> <state.bin> run    <out.bin> <nsteps> [budget_seconds]
 //   ref_harness <script.casl> <state.bin> randvel <out.bin> <seed> <amplitude>
+//   ref_harness <script.casl> <state.bin> runcall <out.bin>
 //
 // The CASL script defines the objects (domain box, atom_data basic,
 // neighborlist basic, force fields, md_simulator basic) with the reference's
@@ -316,6 +317,16 @@ int main(int argc, char **argv)
     out.scalar("wall_rest", t_rest);
     out.scalar("steps_done", (double)done);
     out.scalar("n_ghost", (double)ad->atom_struct_ghost.position.size());
+  }
+  else if (mode == "runcall")
+  {
+    // the simulator's own run() (md_simulator.cpp:235-274, or the B200
+    // adapter's override when the script names `md_simulator b200`), over the
+    // script's initial_step .. final_step, then the owned state
+    const double t0 = now_s();
+    sim->run();
+    out.scalar("wall", now_s() - t0);
+    dump_owned();
   }
   else if (mode == "randvel")
   {
