@@ -174,7 +174,7 @@ def nve_trace(s, nblocks: int = 100, block: int = 100) -> list:
     o = O.Oracle(cur, policy=O.POLICY_REFERENCE)
     for b in range(nblocks + 1):
         o.set_atoms(cur.pos, cur.vel, cur.type)
-        o.build_list()
+        o.setup()  # list and forces of this state (the k-space energy uses its S(k))
         sc = o.energy()
         e.append(sc["ke"] + sc["e_lj"] + sc["e_ewald_r"] + sc["e_ewald_k"] + sc["e_self"])
         if b == nblocks:
