@@ -60,6 +60,10 @@ struct KT {
 struct cvr_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
+  // side stream of the S(k) chain (phase tables, chunk partials, reduction),
+  // which runs beside the pair kernel; joined before the k-space force
+  cudaStream_t kstream = nullptr;
+  cudaEvent_t k_fork = nullptr, k_join = nullptr;
   // domain + types
   double lo[3], hi[3], L[3];
   int bc[3];
@@ -739,18 +743,28 @@ void launch_kforce(cvr_ctx *c, const DevState<real> &s, const KArgs<real> &a) {
   KForceTable<real, KMZ>::launch(c, s, a);
 }
 
+// S(k) of the current positions: phase tables, chunk partials, reduction
+// (S(k), energy partials, force coefficients), on stream st.
+template <typename real>
+void launch_sk(cvr_ctx *c, cudaStream_t st) {
+  DevState<real> s = dev_state<real>(c);
+  KArgs<real> a = kargs<real>(c);
+  k_phase<real><<<grid_for(3 * c->n, 256), 256, 0, st>>>(s, a);
+  dim3 g1(grid_for(((c->kM + KMG - 1) / KMG) * c->nxy, 128), c->nchunks);
+  k_sk_partial<real, KMG, KCH><<<g1, 128, sk_smem<real>(c), st>>>(s, a);
+  k_sk_reduce<real, KRW><<<c->n_ek_blocks, KRW * 32, 0, st>>>(s, a);
+  c->launches += 3;
+}
+
 template <typename real>
 int launch_kspace(cvr_ctx *c) {
   if (!c->ewk_on || c->nk == 0) return CVR_OK;
   Bracket br(c, CVR_KT_KSPACE);
+  launch_sk<real>(c, c->stream);
   DevState<real> s = dev_state<real>(c);
   KArgs<real> a = kargs<real>(c);
-  k_phase<real><<<grid_for(3 * c->n, 256), 256, 0, c->stream>>>(s, a);
-  dim3 g1(grid_for(((c->kM + KMG - 1) / KMG) * c->nxy, 128), c->nchunks);
-  k_sk_partial<real, KMG, KCH><<<g1, 128, sk_smem<real>(c), c->stream>>>(s, a);
-  k_sk_reduce<real, KRW><<<c->n_ek_blocks, KRW * 32, 0, c->stream>>>(s, a);
   launch_kforce<real>(c, s, a);
-  c->launches += 4;
+  c->launches += 1;
   return CVR_OK;
 }
 
@@ -880,8 +894,28 @@ int launch_slab(cvr_ctx *c) {
 
 template <typename real>
 int forces_now(cvr_ctx *c, bool ev) {
-  launch_pair<real>(c, ev);
-  if (int r = launch_kspace<real>(c)) return r;
+  if (c->ewk_on && c->nk > 0 && !c->timing) {
+    // The S(k) chain reads only positions and charges and the pair kernel
+    // writes only the accelerations and its energy partials, so the chain
+    // runs on the side stream beside the pair kernel (parallel branches in
+    // a captured step graph); the k-space force, which adds to the pair
+    // kernel's accelerations, waits for both.  With kernel timing on, the
+    // kernels run one after the other so that each class keeps its own
+    // event bracket.
+    CVR_CUDA(c, cudaEventRecord(c->k_fork, c->stream));
+    CVR_CUDA(c, cudaStreamWaitEvent(c->kstream, c->k_fork, 0));
+    launch_sk<real>(c, c->kstream);
+    CVR_CUDA(c, cudaEventRecord(c->k_join, c->kstream));
+    launch_pair<real>(c, ev);
+    CVR_CUDA(c, cudaStreamWaitEvent(c->stream, c->k_join, 0));
+    DevState<real> s = dev_state<real>(c);
+    KArgs<real> a = kargs<real>(c);
+    launch_kforce<real>(c, s, a);
+    c->launches += 1;
+  } else {
+    launch_pair<real>(c, ev);
+    if (int r = launch_kspace<real>(c)) return r;
+  }
   if (c->sc_on)
     if (int r = launch_slab<real>(c)) return r;
   if (c->ewk_on && c->dipole_mode) {
@@ -1369,7 +1403,19 @@ int cvr_create(cvr_ctx **out, const double lo[3], const double hi[3], const int 
     delete c;
     return CVR_ERR_CUDA;
   }
+  if (cudaStreamCreateWithFlags(&c->kstream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->k_fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->k_join, cudaEventDisableTiming) != cudaSuccess) {
+    if (c->kstream) cudaStreamDestroy(c->kstream);
+    if (c->k_fork) cudaEventDestroy(c->k_fork);
+    cudaStreamDestroy(c->stream);
+    delete c;
+    return CVR_ERR_CUDA;
+  }
   if (dalloc(c, &c->flags, 4) != CVR_OK || dalloc(c, &c->counters, 2) != CVR_OK) {
+    cudaEventDestroy(c->k_fork);
+    cudaEventDestroy(c->k_join);
+    cudaStreamDestroy(c->kstream);
     cudaStreamDestroy(c->stream);
     delete c;
     return CVR_ERR_NOMEM;
@@ -1393,6 +1439,10 @@ void cvr_destroy(cvr_ctx *c) {
       cudaEventDestroy(e.first);
       cudaEventDestroy(e.second);
     }
+  cudaStreamSynchronize(c->kstream);
+  cudaEventDestroy(c->k_fork);
+  cudaEventDestroy(c->k_join);
+  cudaStreamDestroy(c->kstream);
   cudaStreamDestroy(c->stream);
   delete c;
 }
@@ -1618,8 +1668,19 @@ int cvr_set_state(cvr_ctx *c, int64_t n, const double *pos, const double *vel, c
                   const int32_t *mol) {
   if (!c) return CVR_ERR_INVALID;
   if (n <= 0 || n > (int64_t)INDEX_MASK || !pos || !type) return fail(c, CVR_ERR_INVALID, "bad atom arrays");
-  for (int64_t i = 0; i < n; ++i)
-    if (type[i] < 0 || type[i] >= c->n_types) return fail(c, CVR_ERR_INVALID, "atom type out of range");
+  // atoms per type (validates every type; the charge and mass sums below
+  // then cost one term per type instead of a dependent chain over atoms)
+  std::vector<int64_t> per_type((size_t)c->n_types, 0);
+  {
+    const uint32_t nt = (uint32_t)c->n_types;
+    bool bad = false;
+    for (int64_t i = 0; i < n; ++i) {
+      const uint32_t t = (uint32_t)type[i];
+      bad |= t >= nt;
+      per_type[t < nt ? t : 0]++;
+    }
+    if (bad) return fail(c, CVR_ERR_INVALID, "atom type out of range");
+  }
   cudaSetDevice(c->device);
   if (n != c->n || !c->x) {
     c->refreshed = false;
@@ -1639,9 +1700,9 @@ int cvr_set_state(cvr_ctx *c, int64_t n, const double *pos, const double *vel, c
   const bool mol_changed = (mol != nullptr) != c->use_mol;
   c->use_mol = mol != nullptr;
   double q2 = 0, mt = 0;
-  for (int64_t i = 0; i < n; ++i) {
-    q2 += c->charge[type[i]] * c->charge[type[i]];
-    mt += c->mass[type[i]];
+  for (int t = 0; t < c->n_types; ++t) {
+    q2 += (double)per_type[(size_t)t] * (c->charge[t] * c->charge[t]);
+    mt += (double)per_type[(size_t)t] * c->mass[t];
   }
   // the step graphs bake these in (thermo kernel, pair-kernel choice)
   if (mol_changed || mt != c->total_mass || q2 != c->q2_sum) c->epoch++;
