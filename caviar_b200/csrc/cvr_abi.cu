@@ -33,8 +33,14 @@ using namespace cvr;
 
 namespace {
 
-constexpr int KCH = 64;    // atoms per S(k) chunk
-constexpr int KMG = 3;     // m-values per S(k) thread
+#ifndef CVR_KCH
+#define CVR_KCH 64
+#endif
+#ifndef CVR_KMG
+#define CVR_KMG 3
+#endif
+constexpr int KCH = CVR_KCH;  // atoms per S(k) chunk
+constexpr int KMG = CVR_KMG;  // m-values per S(k) thread
 constexpr int KMZ = 16;    // k-force: Z[m] held in registers up to this many m-values (kmax_z < 16)
 #ifndef CVR_KF_WMAX
 #define CVR_KF_WMAX 8
