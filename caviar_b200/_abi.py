@@ -36,7 +36,8 @@ EXPORTED = ["cvr_create", "cvr_destroy", "cvr_set_neighborlist", "cvr_set_lj", "
             "cvr_batch_set_forces", "cvr_batch_set_state", "cvr_batch_run", "cvr_batch_get_state", "cvr_batch_info",
             "cvr_batch_last_error", "cvr_batch_stream", "cvr_adj_create", "cvr_adj_destroy", "cvr_adj_set_params",
             "cvr_adj_set_state", "cvr_adj_forces", "cvr_adj_force_vjp", "cvr_adj_loss", "cvr_adj_loss_grad",
-            "cvr_adj_last_error", "cvr_adj_stream", "cvr_measure_fma_peak"]
+            "cvr_adj_last_error", "cvr_adj_stream", "cvr_measure_fma_peak", "cvr_set_lj_jump_tol",
+            "cvr_set_all_atom_test"]
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int32)
@@ -98,6 +99,8 @@ def load(path: str = LIB_PATH):
     L.cvr_set_kernel_timing.argtypes = [vp, ctypes.c_int]
     L.cvr_kernel_time.argtypes = [vp, ctypes.c_int, _dp, ctypes.POINTER(ctypes.c_int64)]
     L.cvr_measure_fma_peak.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, _dp]
+    L.cvr_set_lj_jump_tol.argtypes = [vp, ctypes.c_double]
+    L.cvr_set_all_atom_test.argtypes = [vp, ctypes.c_int]
     _lib = L
     return L
 
@@ -186,6 +189,8 @@ class Simulation:
             cl = None if s.lj.cutoff_list is None else s.lj.cutoff_list
             self._check(self.L.cvr_set_lj(self.h, s.lj.cutoff, _d(s.lj.epsilon), _d(s.lj.sigma), _d(cl),
                                           int(s.lj.ignore_intra_molecule)))
+        if s.lj is not None and getattr(s.lj, "jump_tol", 0.0) > 0:
+            self._check(self.L.cvr_set_lj_jump_tol(self.h, s.lj.jump_tol))
         if s.ewald_r is not None:
             self._check(self.L.cvr_set_ewald_r(self.h, s.ewald_r.alpha, s.ewald_r.k_electrostatic,
                                                _d(s.ewald_r.lam), s.ewald_r.cutoff))
@@ -197,6 +202,10 @@ class Simulation:
     def set_integrator(self, dt: float, k_b: float = 1.0):
         """md_simulator dt / atom_data k_b (md_simulator.cpp:58-233)."""
         self._check(self.L.cvr_set_integrator(self.h, dt, k_b))
+
+    def set_all_atom_test(self, on: bool = True):
+        """neighborlist all_atom_test (neighborlist.cpp:161-191): every owned pair and ghost image."""
+        self._check(self.L.cvr_set_all_atom_test(self.h, int(on)))
 
     def set_langevin(self, temperature: float, friction: float, kb: float = -1.0, kbt: float = -1.0,
                      rng: int = RNG_REFERENCE, seed: int = 0):

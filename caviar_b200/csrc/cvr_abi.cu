@@ -124,6 +124,8 @@ struct cvr_ctx {
   std::vector<double> fk;
   std::vector<int2> kxy, kpm;
   double e_self = 0, total_mass = 0, q2_sum = 0;  // q2_sum = sum of q_i^2 over the atoms
+  double jump_tol = 0;                              // LJ jump_tol (lj.cpp:118-127), <= 0 off
+  bool all_atom = false;                            // neighborlist all_atom_test (neighborlist.cpp:161-191)
   // device memory
   std::vector<std::pair<void **, size_t>> atom_bufs;
   // per atom
@@ -235,7 +237,9 @@ DevState<real> dev_state(cvr_ctx *c) {
   s.n_pad = c->n_pad;
   s.cap = c->cap;
   s.tpa = c->tpa;
-  s.policy = c->policy;
+  // all_atom_test: wrap and reclassify every step (the reference regenerates
+  // its ghosts every step and its list covers all of them)
+  s.policy = c->all_atom ? CVR_REBUILD_EVERY_STEP : c->policy;
   s.n_types = c->n_types;
   for (int d = 0; d < 3; ++d) {
     s.box.lo[d] = c->lo[d];
@@ -383,7 +387,7 @@ int setup_cells(cvr_ctx *c) {
 // Otherwise the cell-local FP32 form is used.
 void choose_fixed(cvr_ctx *c) {
   c->fixed = 0;
-  if (c->precision == CVR_PREC_FP64) return;
+  if (c->precision == CVR_PREC_FP64 || c->all_atom) return;
   const double rl = c->cutoff * c->coef;
   if (!(c->L[0] == c->L[1] && c->L[1] == c->L[2])) return;
   if (!(0.5 * c->L[0] > (2.0 * rl - c->cutoff) * (1.0 + 1e-6))) return;
@@ -424,6 +428,7 @@ int upload_tables(cvr_ctx *c) {
         p.qq = c->ewr_ke * c->charge[a] * c->charge[b];
         if (!c->lam.empty()) p.lam = c->lam[a * T + b];
       }
+      p.jump2 = (c->lj_on && c->jump_tol > 0) ? c->jump_tol : 0.0;
     }
   if (dbl) {
     if (int r = dalloc(c, (PairCoef<double> **)&c->d_coef, T * T)) return r;
@@ -437,7 +442,8 @@ int upload_tables(cvr_ctx *c) {
       const auto &p = cd[t];
       cf[t] = PairCoef<float>{(float)(p.sig2 / h2), (float)p.eps24, (float)p.eps48, (float)(p.K * h2),
                               (float)(p.rc2 > 0 ? p.rc2 / h2 : p.rc2),
-                              (float)(p.qq / h), (float)p.e4, (float)p.C0, (float)(p.C1 * h2), (float)p.lam};
+                              (float)(p.qq / h), (float)p.e4, (float)p.C0, (float)(p.C1 * h2), (float)p.lam,
+                              (float)(p.jump2 / h2)};
     }
     if (int r = dalloc(c, (PairCoef<float> **)&c->d_coef, T * T)) return r;
     CVR_CUDA(c, cudaMemcpyAsync(c->d_coef, cf.data(), T * T * sizeof(PairCoef<float>), cudaMemcpyHostToDevice, c->stream));
@@ -633,8 +639,8 @@ void launch_pair_t(cvr_ctx *c) {
 
 template <typename real, bool LJ, bool EWR, bool EV, bool FIXED>
 void launch_pair_tpa_f(cvr_ctx *c) {
-  // one type pair, no molecule tests: LJ constants in registers
-  const bool one = LJ && !EWR && c->n_types == 1 && !c->use_mol;
+  // one type pair, no molecule tests, no jump_tol clamp: LJ constants in registers
+  const bool one = LJ && !EWR && c->n_types == 1 && !c->use_mol && !(c->jump_tol > 0);
   switch (c->tpa) {
     case 1:
       one ? launch_pair_t<real, 1, LJ, EWR, EV, true, FIXED>(c) : launch_pair_t<real, 1, LJ, EWR, EV, false, FIXED>(c);
@@ -657,10 +663,38 @@ void launch_pair_tpa(cvr_ctx *c) {
   launch_pair_tpa_f<real, LJ, EWR, EV, false>(c);
 }
 
+// all_atom_test: every owned pair and every ghost image (k_pair_all), in
+// length units (the fixed-point form is off in this mode).
+template <typename real, bool LJ, bool EWR, bool EV>
+void launch_pair_all_t(cvr_ctx *c) {
+  DevState<real> s = dev_state<real>(c);
+  EwrArgs<real> ew;
+  ew.alpha = (real)c->ewr_alpha;
+  ew.alpha2 = (real)(c->ewr_alpha * c->ewr_alpha);
+  ew.two_alpha_spi = (real)(2.0 * c->ewr_alpha * 0.56418958354775628695);
+  ew.cut2 = (real)(c->ewr_cut >= 0 ? c->ewr_cut * c->ewr_cut : -1.0);
+  // n_ev_blocks >= the blocks that hold atoms; the rest store zero partials
+  k_pair_all<real, LJ, EWR, EV><<<c->n_ev_blocks, 128, 0, c->stream>>>(
+      s, (const PairCoef<real> *)c->d_coef, ew, c->ignore_intra, c->use_mol ? 1 : 0, c->ev_part);
+  c->launches++;
+}
+
+template <typename real, bool EV>
+void launch_pair_all(cvr_ctx *c) {
+  if (c->lj_on && c->ewr_on)
+    launch_pair_all_t<real, true, true, EV>(c);
+  else if (c->lj_on)
+    launch_pair_all_t<real, true, false, EV>(c);
+  else
+    launch_pair_all_t<real, false, true, EV>(c);
+}
+
 template <typename real>
 void launch_pair(cvr_ctx *c, bool ev) {
   Bracket br(c, CVR_KT_PAIR);
-  if (c->lj_on && c->ewr_on) {
+  if (c->all_atom && (c->lj_on || c->ewr_on)) {
+    ev ? launch_pair_all<real, true>(c) : launch_pair_all<real, false>(c);
+  } else if (c->lj_on && c->ewr_on) {
     ev ? launch_pair_tpa<real, true, true, true>(c) : launch_pair_tpa<real, true, true, false>(c);
   } else if (c->lj_on) {
     ev ? launch_pair_tpa<real, true, false, true>(c) : launch_pair_tpa<real, true, false, false>(c);
@@ -1338,8 +1372,52 @@ int refresh(cvr_ctx *c) {
   return CVR_OK;
 }
 
+// all_atom_test: every owned pair (no shift) and every owned atom with every
+// ghost image (atom a at shift s = -zone on the axes of a non-empty subset of
+// a's ghost zones), in the canonical orientation, from the build's ghost-zone
+// classes (the reference's list, neighborlist.cpp:161-191).
+int pairs_all_atom(cvr_ctx *c, std::vector<std::array<int32_t, 5>> &out) {
+  const int64_t n = c->n;
+  std::vector<int> ids(n);
+  std::vector<int8_t> g(n);
+  CVR_CUDA(c, cudaMemcpyAsync(ids.data(), c->id, n * 4, cudaMemcpyDeviceToHost, c->stream));
+  CVR_CUDA(c, cudaMemcpyAsync(g.data(), c->gcls, n, cudaMemcpyDeviceToHost, c->stream));
+  CVR_CUDA(c, cudaStreamSynchronize(c->stream));
+  out.clear();
+  for (int64_t i = 0; i < n; ++i)
+    for (int64_t j = i + 1; j < n; ++j)
+      out.push_back({std::min(ids[i], ids[j]), std::max(ids[i], ids[j]), 0, 0, 0});
+  for (int64_t a = 0; a < n; ++a) {
+    const int v[3] = {g[a] % 3 - 1, (g[a] / 3) % 3 - 1, g[a] / 9 - 1};
+    for (int m = 1; m < 8; ++m) {
+      int sh[3];
+      bool ok = true;
+      for (int d = 0; d < 3; ++d) {
+        const bool on = (m >> d) & 1;
+        if (on && v[d] == 0) ok = false;
+        sh[d] = on ? -v[d] : 0;
+      }
+      if (!ok) continue;
+      for (int64_t i = 0; i < n; ++i) {
+        int p = ids[i], q = ids[a], s3[3] = {sh[0], sh[1], sh[2]};
+        bool flip = p > q;
+        if (p == q) flip = std::make_tuple(s3[0], s3[1], s3[2]) < std::make_tuple(-s3[0], -s3[1], -s3[2]);
+        if (flip) {
+          std::swap(p, q);
+          for (int d = 0; d < 3; ++d) s3[d] = -s3[d];
+        }
+        out.push_back({p, q, s3[0], s3[1], s3[2]});
+      }
+    }
+  }
+  std::sort(out.begin(), out.end());
+  out.erase(std::unique(out.begin(), out.end()), out.end());
+  return CVR_OK;
+}
+
 template <typename real>
 int pairs_impl(cvr_ctx *c, std::vector<std::array<int32_t, 5>> &out) {
+  if (c->all_atom) return pairs_all_atom(c, out);
   const int64_t n = c->n;
   std::vector<int> cnt(n), ids(n), cells(n);
   std::vector<uint32_t> lst((size_t)c->cap * c->n_pad);
@@ -1484,6 +1562,22 @@ int cvr_set_lj(cvr_ctx *c, double cutoff, const double *eps, const double *sig, 
   c->cutl.clear();
   if (cutl) c->cutl.assign(cutl, cutl + T * T);
   c->ignore_intra = ignore_intra ? 1 : 0;
+  return refresh(c);
+}
+
+int cvr_set_all_atom_test(cvr_ctx *c, int on) {
+  if (!c) return CVR_ERR_INVALID;
+  if (on && c->n > CVR_ALL_ATOM_MAX) return fail(c, CVR_ERR_INVALID, "all_atom_test is for small systems");
+  cudaSetDevice(c->device);
+  c->all_atom = on != 0;
+  return refresh(c);
+}
+
+int cvr_set_lj_jump_tol(cvr_ctx *c, double jump_tol) {
+  if (!c) return CVR_ERR_INVALID;
+  if (!(jump_tol >= 0)) return fail(c, CVR_ERR_INVALID, "jump_tol have to be non-negative.");
+  cudaSetDevice(c->device);
+  c->jump_tol = jump_tol;
   return refresh(c);
 }
 
@@ -1674,6 +1768,7 @@ int cvr_set_state(cvr_ctx *c, int64_t n, const double *pos, const double *vel, c
                   const int32_t *mol) {
   if (!c) return CVR_ERR_INVALID;
   if (n <= 0 || n > (int64_t)INDEX_MASK || !pos || !type) return fail(c, CVR_ERR_INVALID, "bad atom arrays");
+  if (c->all_atom && n > CVR_ALL_ATOM_MAX) return fail(c, CVR_ERR_INVALID, "all_atom_test is for small systems");
   // atoms per type (validates every type; the charge and mass sums below
   // then cost one term per type instead of a dependent chain over atoms)
   std::vector<int64_t> per_type((size_t)c->n_types, 0);

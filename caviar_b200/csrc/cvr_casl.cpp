@@ -14,11 +14,12 @@
 //                              (atom_data.cpp:78-306, 597-616, atom_data/add_xyz_data_file.cpp:22-168)
 //   neighborlist basic <name>  set_atom_data|atom_data, set_domain|domain, cutoff,
 //                              cutoff_extra_coef, build_cell_list,
-//                              make_verlet_list_from_cell_list, rebuild_test, dt
+//                              make_verlet_list_from_cell_list, rebuild_test, all_atom_test, dt
 //                              (neighborlist.cpp:193-251)
 //   force_field lj <name>      cutoff, cutoff_list i j v, epsilon i j v, sigma i j v,
 //                              epsilon_atom i v, sigma_atom i v, lambda_s i j v,
-//                              lambda_e i j v, wca, ignore_intra_molecule,
+//                              lambda_e i j v, wca, ignore_intra_molecule, jump_tol v,
+//                              monitor_jump (accepted; the reference's per-pair print is not made),
 //                              make_off_diagonal_vectors, set_neighborlist|neighborlist,
 //                              set_atom_data|atom_data, set_domain|domain (lj.cpp:42-353)
 //   force_field electrostatic_ewald_r <name>  cutoff, alpha, k_electrostatic, lambda i j v,
@@ -48,7 +49,7 @@
 //                                  (constraint/nose_hoover.cpp:39-117); md_simulator add_constraint
 // plus the variables `real name value` / `int name value`, comments (#) and
 // `exit`.  Keywords of these objects that sit off the hot path (other
-// constraints, slab/dipole Ewald, jump_tol, msd/povray/ghost writers) are
+// constraints, msd/povray/ghost writers) are
 // rejected with a message instead of being ignored.
 //
 // Writers follow the reference: a line "step time value" (default stream
@@ -177,6 +178,7 @@ struct Neighborlist : Object {
   Domain *domain = nullptr;
   double cutoff = 0.0, coef = 1.12347;  // neighborlist.h:134
   bool rebuild_test = false, from_cell_list = false;
+  bool all_atom_test = false;  // neighborlist.cpp:161-191, 233-235
 };
 
 struct Force_field : Object {
@@ -204,6 +206,8 @@ struct Lj : Force_field {
   Mat epsilon, sigma, cutoff_list, lambda_s, lambda_e;
   std::vector<double> epsilon_atom, sigma_atom;
   bool by_array = false, by_atom = false, wca = false, cutoff_list_on = false, ignore_intra = false;
+  double jump_tol = 0.0;  // lj.cpp:118-127 (jump_fix when set)
+  bool monitor_jump = false;
 };
 
 struct Ewald_r : Force_field {
@@ -619,6 +623,8 @@ struct Script {
         nl.from_cell_list = true;
       } else if (t == "rebuild_test") {
         nl.rebuild_test = true;
+      } else if (t == "all_atom_test") {
+        nl.all_atom_test = true;
       } else if (t == "dt") {
         real();
       } else err("neighborlist: '" + t + "' is not supported on the B200 path");
@@ -666,6 +672,12 @@ struct Script {
         f.cutoff_list_on = true;
       } else if (t == "ignore_intra_molecule") {
         f.ignore_intra = true;
+      } else if (t == "jump_tol") {
+        f.jump_tol = real();
+        if (f.jump_tol < 0) err("jump_tol have to be non-negative.");
+      } else if (t == "monitor_jump") {
+        // the reference prints each clamped r^2 to stdout; accepted, no output here
+        f.monitor_jump = true;
       } else if (t == "make_off_diagonal_vectors") {
         // no effect on the forces
       } else err("force_field lj: '" + t + "' is not supported on the B200 path");
@@ -1004,6 +1016,7 @@ struct Script {
     check(cvr_set_precision(ctx, m.precision));
     const int policy = nl->rebuild_test ? CVR_REBUILD_EVERY_STEP : m.policy;
     check(cvr_set_neighborlist(ctx, nl->cutoff, nl->coef, a->ghost_cutoff, policy));
+    if (nl->all_atom_test) check(cvr_set_all_atom_test(ctx, 1));
     for (Force_field *f : m.force_field) {
       if (auto *lj = dynamic_cast<Lj *>(f)) {
         std::vector<double> eps, sig, cut;
@@ -1011,6 +1024,7 @@ struct Script {
         lj_tables(*lj, T, eps, sig, cut, use_cut);
         check(cvr_set_lj(ctx, lj->cutoff, eps.data(), sig.data(), use_cut ? cut.data() : nullptr,
                          lj->ignore_intra ? 1 : 0));
+        if (lj->jump_tol > 0) check(cvr_set_lj_jump_tol(ctx, lj->jump_tol));
       } else if (auto *er = dynamic_cast<Ewald_r *>(f)) {
         std::vector<double> lam(T * T, 1.0);
         for (int i = 0; i < T; ++i)

@@ -54,6 +54,7 @@ template <typename real> struct PairCoef {
   real qq;                     // k_e q_i q_j (Ewald real space)
   real e4, C0, C1;             // LJ energy: e4*(s6^2 - s6) + C1*r2 + C0
   real lam;                    // Ewald same-molecule scaling lambda (1 if unset)
+  real jump2;                  // LJ jump_tol: r^2 floor of the coefficient and virial (0: off)
 };
 
 template <typename real> struct DevState {

@@ -137,21 +137,28 @@ __device__ __forceinline__ void ev_flush(PairAcc<real> &A) {
   A.g_lj = A.g_ew = A.g_vir = (real)0;
 }
 
-template <typename real, bool LJ, bool EWR, bool EV>
+// JUMP (the multi-type kernels only): the reference's LJ jump_tol clamp
+// (lj.cpp:423-432): after the cutoff test, r^2 below jump_tol is raised to
+// it for the LJ coefficient (and the LJ virial and energy); the force keeps
+// the true displacement.
+template <typename real, bool LJ, bool EWR, bool EV, bool JUMP = false>
 __device__ __forceinline__ void pair_term(PairAcc<real> &A, real dx, real dy, real dz, const PairCoef<real> &pc,
                                           bool same_mol, int ignore_intra, const EwrArgs<real> &ew) {
   const real r2 = dx * dx + dy * dy + dz * dz;
-  real c = 0;
+  real c = 0, vir_lj = 0;
   if (LJ) {
     // lj.cpp:417-448: skip r^2 > rc^2 (rc2 < 0 when eps = 0)
-    const real r2i = fast_rcp(r2);
+    const real r2l = JUMP ? (r2 < pc.jump2 ? pc.jump2 : r2) : r2;
+    const real r2i = fast_rcp(r2l);
     const real s2 = pc.sig2 * r2i;
     const real s6 = s2 * s2 * s2;
     const bool in = (r2 <= pc.rc2) && !(same_mol && ignore_intra);
     const real cl = r2i * s6 * (pc.eps24 - pc.eps48 * s6) + pc.K;
     c = in ? cl : (real)0;
-    if (EV && in) A.g_lj += pc.e4 * (s6 * s6 - s6) + pc.C1 * r2 + pc.C0;
+    if (EV && in) A.g_lj += pc.e4 * (s6 * s6 - s6) + pc.C1 * r2l + pc.C0;
+    if (EV && JUMP) vir_lj = c * r2l;
   }
+  const real c_lj = c;
   if (EWR) {
     // electrostatic_ewald_r.cpp:179-198: every list pair, coincident skipped
     if (r2 > (real)0 && (ew.cut2 < (real)0 || r2 <= ew.cut2)) {
@@ -172,7 +179,12 @@ __device__ __forceinline__ void pair_term(PairAcc<real> &A, real dx, real dy, re
   A.fx += c * dx;
   A.fy += c * dy;
   A.fz += c * dz;
-  if (EV) A.g_vir -= c * r2;
+  if (EV) {
+    if (JUMP)
+      A.g_vir -= vir_lj + (c - c_lj) * r2;
+    else
+      A.g_vir -= c * r2;
+  }
 }
 
 // Pair displacement r_j - r_i.  Cell-local form: (x4_j - x4_i) + the entry's
@@ -255,7 +267,7 @@ __global__ void __launch_bounds__(128, CVR_PAIR_MINB) k_pair(DevState<real> s, c
           if (!CHECK || u < nv) {
             real dx, dy, dz;
             pair_disp<real, FIXED>(xj[u], xi, e[u], st, dx, dy, dz);
-            pair_term<real, LJ, EWR, EV>(A, dx, dy, dz, ONE_TYPE ? c1 : ci[type_of(xj[u].w)], sm[u], ignore_intra,
+            pair_term<real, LJ, EWR, EV, !ONE_TYPE>(A, dx, dy, dz, ONE_TYPE ? c1 : ci[type_of(xj[u].w)], sm[u], ignore_intra,
                                          ew);
           }
         }
@@ -290,7 +302,7 @@ __global__ void __launch_bounds__(128, CVR_PAIR_MINB) k_pair(DevState<real> s, c
         for (int u = 0; u < U; ++u) {
           real dx, dy, dz;
           pair_disp<real, FIXED>(xj[u], xi, e[u], st, dx, dy, dz);
-          pair_term<real, LJ, EWR, EV>(A, dx, dy, dz, ONE_TYPE ? c1 : ci[type_of(xj[u].w)], sm[u], ignore_intra,
+          pair_term<real, LJ, EWR, EV, !ONE_TYPE>(A, dx, dy, dz, ONE_TYPE ? c1 : ci[type_of(xj[u].w)], sm[u], ignore_intra,
                                        ew);
         }
         if (EV) ev_flush<LJ, EWR>(A);
@@ -303,7 +315,7 @@ __global__ void __launch_bounds__(128, CVR_PAIR_MINB) k_pair(DevState<real> s, c
         const bool sm0 = um && (moli == s.mol[j0]);
         real dx, dy, dz;
         pair_disp<real, FIXED>(xj0, xi, e0, st, dx, dy, dz);
-        pair_term<real, LJ, EWR, EV>(A, dx, dy, dz, ONE_TYPE ? c1 : ci[type_of(xj0.w)], sm0, ignore_intra, ew);
+        pair_term<real, LJ, EWR, EV, !ONE_TYPE>(A, dx, dy, dz, ONE_TYPE ? c1 : ci[type_of(xj0.w)], sm0, ignore_intra, ew);
       }
       if (EV) ev_flush<LJ, EWR>(A);
     }
@@ -323,6 +335,83 @@ __global__ void __launch_bounds__(128, CVR_PAIR_MINB) k_pair(DevState<real> s, c
   if (EV) {
     double v[3] = {0.5 * A.e_lj, 0.5 * A.e_ew, 0.5 * A.vir};  // full list: each pair twice
     block_sum_store<3>(v, partials);
+  }
+}
+
+// ------------------------------------------------ all-atom test (debug mode)
+// The reference's neighbour-list switch all_atom_test (neighborlist.cpp:
+// 161-191): the list holds every owned pair once and every owned atom with
+// every ghost image, with no distance test, so LJ keeps its own cutoff test
+// and the Ewald real-space sum runs over every pair and image.  One thread
+// per atom: every other atom at its direct displacement (no minimum image,
+// as the reference's owned-owned entries), then every current ghost image
+// (atom a at r_a + s L for each non-empty subset of the axes of a's ghost
+// zones, s = -zone, exchange_ghost_single_md_domain.cpp:59-215).  Positions
+// are the wrapped ones of this step's build (the mode rebuilds every step).
+// Energies: each owned pair once, each owned-ghost term with weight 1/2 (the
+// reference has no energy of this asymmetric sum); virial as the reference:
+// each owned pair once, an owned-ghost term when id_i < id_a (lj.cpp:451-453).
+// O(n (n + ghosts)): small systems only.
+template <typename real, bool LJ, bool EWR, bool EV>
+__global__ void __launch_bounds__(128) k_pair_all(DevState<real> s, const PairCoef<real> *__restrict__ coef_g,
+                                                  EwrArgs<real> ew, int ignore_intra, int use_mol,
+                                                  double *__restrict__ partials) {
+  __shared__ PairCoef<real> coef[MAX_TYPES * MAX_TYPES];
+  const int T = s.n_types;
+  for (int t = threadIdx.x; t < T * T; t += blockDim.x) coef[t] = coef_g[t];
+  __syncthreads();
+  if (*s.err) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double fx = 0, fy = 0, fz = 0, e_lj = 0, e_ew = 0, vir = 0;
+  int ti = 0;
+  if (i < s.n) {
+    const double xi = s.x[i], yi = s.y[i], zi = s.z[i];
+    ti = s.type[i];
+    const int mi = use_mol ? s.mol[i] : 0, idi = s.id[i];
+    const PairCoef<real> *ci = coef + ti * T;
+    // one pair term in `real` (displacement rounded from FP64), summed in
+    // FP64 with energy weight w_e and virial weight w_v
+    auto term = [&](double dx, double dy, double dz, int j, double w_e, double w_v) {
+      PairAcc<real> A{0, 0, 0, 0.0, 0.0, 0.0, 0, 0, 0};
+      const bool sm = use_mol && mi == s.mol[j];
+      pair_term<real, LJ, EWR, EV, true>(A, (real)dx, (real)dy, (real)dz, ci[s.type[j]], sm, ignore_intra, ew);
+      fx += (double)A.fx;
+      fy += (double)A.fy;
+      fz += (double)A.fz;
+      if (EV) {
+        e_lj += w_e * (double)A.g_lj;
+        e_ew += w_e * (double)A.g_ew;
+        vir += w_v * (double)A.g_vir;
+      }
+    };
+    // owned pairs: each end computes its own term, so energy and virial take half
+    for (int j = 0; j < s.n; ++j)
+      if (j != i) term(s.x[j] - xi, s.y[j] - yi, s.z[j] - zi, j, 0.5, 0.5);
+    for (int a = 0; a < s.n; ++a) {
+      const int code = s.gcls[a];
+      const int v[3] = {code % 3 - 1, (code / 3) % 3 - 1, code / 9 - 1};
+      if ((v[0] | v[1] | v[2]) == 0) continue;
+      for (int m = 1; m < 8; ++m) {
+        bool ok = true;
+        double sh[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          const bool on = (m >> d) & 1;
+          if (on && v[d] == 0) ok = false;
+          sh[d] = on ? -(double)v[d] * s.box.L[d] : 0.0;
+        }
+        if (!ok) continue;
+        term((s.x[a] + sh[0]) - xi, (s.y[a] + sh[1]) - yi, (s.z[a] + sh[2]) - zi, a, 0.5, idi < s.id[a] ? 1.0 : 0.0);
+      }
+    }
+    const double mi_inv = s.mass_inv[ti];
+    s.ax[i] = (real)(fx * mi_inv);
+    s.ay[i] = (real)(fy * mi_inv);
+    s.az[i] = (real)(fz * mi_inv);
+  }
+  if (EV) {
+    double v3[3] = {e_lj, e_ew, vir};
+    block_sum_store<3>(v3, partials);
   }
 }
 

@@ -37,6 +37,13 @@ namespace md_simulator
 
   namespace
   {
+    // Neighborlist::all_atom_test is protected (neighborlist.h); a derived
+    // class may name it, which yields a pointer to the member of the base.
+    struct NeighborlistSettings : Neighborlist
+    {
+      static bool all_atom_test_of(const Neighborlist *n) { return n->*(&NeighborlistSettings::all_atom_test); }
+    };
+
     // T x T row-major copy of a reference type-pair table (missing entries 0).
     std::vector<double> flat(const std::vector<std::vector<Real_t>> &m, size_t T)
     {
@@ -116,6 +123,8 @@ namespace md_simulator
     Neighborlist *nl = neighborlist[0];
     // the reference's own rebuild trigger (neighborlist.cpp:91-139)
     check(cvr_set_neighborlist(ctx, nl->cutoff, nl->cutoff_extra_coef, ad->ghost_cutoff, CVR_REBUILD_REFERENCE));
+    if (NeighborlistSettings::all_atom_test_of(nl)) // neighborlist.cpp:161-191
+      check(cvr_set_all_atom_test(ctx, 1));
     for (auto *f : force_field)
     {
       if (auto *lj = dynamic_cast<force_field::Lj *>(f))
@@ -125,13 +134,13 @@ namespace md_simulator
           lj->verify_settings();
           lj->settings_verified = true;
         }
-        if (lj->jump_fix || lj->monitor_jump)
-          error->all(FC_FILE_LINE_FUNC, "md_simulator b200: lj jump_tol / monitor_jump are not on this path");
         const std::vector<double> eps = flat(lj->epsilon, T), sig = flat(lj->sigma, T);
         const bool cl = lj->wca || lj->cutoff_list_activated;
         const std::vector<double> cut = cl ? flat(lj->cutoff_list, T) : std::vector<double>();
         check(cvr_set_lj(ctx, lj->cutoff, eps.data(), sig.data(), cl ? cut.data() : nullptr,
                          lj->ignore_intra_molecule ? 1 : 0));
+        if (lj->jump_fix) // lj.cpp:118-127, 423-432 (monitor_jump's per-pair print is not made)
+          check(cvr_set_lj_jump_tol(ctx, lj->jump_tol));
       }
       else if (auto *er = dynamic_cast<force_field::Electrostatic_ewald_r *>(f))
       {

@@ -77,6 +77,24 @@ int cvr_set_neighborlist(cvr_ctx *ctx, double cutoff, double cutoff_extra_coef, 
 int cvr_set_lj(cvr_ctx *ctx, double cutoff, const double *epsilon, const double *sigma,
                const double *cutoff_list, int ignore_intra_molecule);
 
+/* Neighborlist all_atom_test (neighborlist.cpp:161-191, 233-235, 517-519): a
+ * debugging mode of the reference whose list holds every owned pair once and
+ * every owned atom with every ghost image, with no distance test (LJ keeps
+ * its cutoff test; the Ewald real-space sum, which has none, runs over all of
+ * them).  Forces come from an all-pairs kernel over the direct displacements
+ * and the ghost images of this step's wrapped positions (rebuilt every
+ * step); cvr_get_pairs returns that pair set.  At most CVR_ALL_ATOM_MAX atoms
+ * (O(n^2) work).  on = 0 returns to the Verlet list. */
+#define CVR_ALL_ATOM_MAX 65536
+int cvr_set_all_atom_test(cvr_ctx *ctx, int on);
+
+/* force_field lj jump_tol v (lj.cpp:118-127, 423-432): a debugging clamp of
+ * the reference; after the cutoff test, a pair closer than sqrt(jump_tol)
+ * gets the LJ force coefficient (and LJ virial and energy) of r^2 = jump_tol,
+ * applied to its true displacement.  0 turns it off (the default).
+ * Replaces: Lj::read jump_tol and the clamp in Lj::calculate_acceleration. */
+int cvr_set_lj_jump_tol(cvr_ctx *ctx, double jump_tol);
+
 /* force_field electrostatic_ewald_r: alpha, k_electrostatic; lambda: n_types^2
  * same-molecule scaling or NULL; cutoff < 0 keeps the reference's behaviour of
  * summing every list pair (electrostatic_ewald_r.cpp:142-226 has no cutoff test).

@@ -87,7 +87,7 @@ def _d(a):
 class Oracle:
     """The FP64 restatement for one periodic system."""
 
-    def __init__(self, system, policy: int = POLICY_DISPLACEMENT):
+    def __init__(self, system, policy: int = POLICY_DISPLACEMENT, all_atom_test: bool = False):
         L = lib()
         self._keep = []
         s = system
@@ -99,7 +99,7 @@ class Oracle:
         self.h = L.orc_create(_d(lo), _d(hi), bc, s.n_types, _d(mass), _d(charge))
         self.n = s.n
         self.set_atoms(s.pos, s.vel, s.type, s.mol)
-        L.orc_set_neighborlist(self.h, s.cutoff, s.coef, s.ghost_cutoff, 0)
+        L.orc_set_neighborlist(self.h, s.cutoff, s.coef, s.ghost_cutoff, int(all_atom_test))
         if s.lj is not None:
             eps = np.ascontiguousarray(s.lj.epsilon, np.float64)
             sig = np.ascontiguousarray(s.lj.sigma, np.float64)
@@ -319,6 +319,8 @@ def casl_script(system, nsteps: int = 1, rebuild_test: bool = False, extra: str 
                 lines.append(f"f_lj sigma {i} {j} {r(float(s.lj.sigma[i][j]))}")
                 if s.lj.cutoff_list is not None:
                     lines.append(f"f_lj cutoff_list {i} {j} {r(float(s.lj.cutoff_list[i][j]))}")
+        if getattr(s.lj, "jump_tol", 0.0) > 0:
+            lines.append(f"f_lj jump_tol {r(float(s.lj.jump_tol))}")
         lines += ["f_lj set_neighborlist neigh", "f_lj set_atom_data adata", "f_lj set_domain dom"]
     if s.ewald_r is not None:
         ffs.append("f_er")

@@ -72,7 +72,17 @@ GPU tests never need the reference at run time).
    Ewald real-space sum then covers the minimum-image pairs within L/2):
    accelerations, virial, kinetic energy, k-space and self energies.
 
-Usage:  python tests/golden/make_golden.py [/path/to/reference] [--bench-only | --replicas-only | --nve-only]
+11. ref_ljjump500.npz -- the reference's forces and virial with `f_lj
+   jump_tol 0.9` on a 500-atom fluid in which twenty atoms were moved to
+   0.85-0.93 sigma from their nearest neighbour (jump_system()).
+
+12. ref_allatom300.npz -- the reference with `neigh all_atom_test` on 300
+   ions (all_atom_system()): forces, virial, S(k), k-space energy, the
+   SHA-256 and size of its pair set (every owned pair and every ghost image)
+   and a 10-step run.
+
+Usage:  python tests/golden/make_golden.py [/path/to/reference]
+        [--bench-only | --replicas-only | --nve-only | --jump-only]
 The reference root defaults to $CAVIAR_REFERENCE_ROOT, else to a directory
 named `reference` beside this repository.
 """
@@ -385,6 +395,56 @@ def replicas() -> None:
     np.savez_compressed(os.path.join(HERE, "ref_replicas.npz"), **out)
 
 
+def jump_system():
+    """500-atom LJ fluid with twenty atoms moved towards their nearest
+    neighbour (to 0.85-0.93 sigma) and the reference's lj jump_tol 0.9
+    (pairs closer than sqrt(0.9) get the coefficient of r^2 = 0.9)."""
+    s = W.fcc_lattice(5, 0.8442, 0.72, seed=17, jitter=0.05)
+    rng = np.random.default_rng(17)
+    L = float(s.box[0])
+    pos = s.pos.copy()
+    for i in rng.choice(s.n, size=20, replace=False):
+        d = pos - pos[i]
+        d -= L * np.round(d / L)
+        r = np.linalg.norm(d, axis=1)
+        r[i] = np.inf
+        j = int(np.argmin(r))
+        target = rng.uniform(0.85, 0.93)
+        pos[i] = pos[i] + d[j] / r[j] * (r[j] - target)
+    s.pos = pos % L
+    s.lj.jump_tol = 0.9
+    return s
+
+
+def jump500() -> None:
+    s = jump_system()
+    f = O.run_reference(s, "forces")
+    order = np.argsort(f["id"].astype(np.int64))
+    np.savez_compressed(os.path.join(HERE, "ref_ljjump500.npz"), pos=s.pos, acc=f["acc"].reshape(-1, 3)[order],
+                        virial=f["virial"], jump_tol=s.lj.jump_tol)
+
+
+def all_atom_system():
+    """300 ions (+-1) in a 10^3 box, LJ rc 2.5, Ewald alpha 0.8, k_max 3,
+    list radius 3.09 (ghost cutoff the same)."""
+    return W.random_ions(300, 10.0, seed=23, rc=3.0, coef=1.03, kmax=3, alpha=0.8)
+
+
+def all_atom300(nsteps: int = 10) -> None:
+    """The reference with `neigh all_atom_test`: forces, virial, its pair
+    set (every owned pair and ghost image) and a 10-step run."""
+    s = all_atom_system()
+    extra = "neigh all_atom_test\n"
+    f = O.run_reference(s, "forces", extra=extra)
+    order = np.argsort(f["id"].astype(np.int64))
+    r = O.run_reference(s, "run", nsteps=nsteps, extra=extra)
+    orr = np.argsort(r["id"].astype(np.int64))
+    np.savez_compressed(os.path.join(HERE, "ref_allatom300.npz"), acc=f["acc"].reshape(-1, 3)[order],
+                        virial=f["virial"], pairs_sha256=pair_digest(f["pairs"].reshape(-1, 5)),
+                        npairs=f["pairs"].size // 5, sk=f["sk"], ek=f["ek_kspace"],
+                        run_steps=nsteps, run_pos=r["pos"].reshape(-1, 3)[orr], run_vel=r["vel"].reshape(-1, 3)[orr])
+
+
 def pair_digest(pairs: np.ndarray) -> str:
     """SHA-256 of a canonical pair set (n x 5 int32, little endian, row major)."""
     return hashlib.sha256(np.ascontiguousarray(pairs, dtype="<i4").tobytes()).hexdigest()
@@ -446,6 +506,11 @@ def main():
             with open(os.path.join(HERE, f"nve_{name}.json"), "w") as f:
                 json.dump(nve(name, equilibrate=NVE_EQUILIBRATE[name]), f)
         return
+    if "--jump-only" in sys.argv:
+        O.build(ref_root)
+        jump500()
+        all_atom300()
+        return
     if "--replicas-only" in sys.argv:
         O.build(ref_root)
         replicas()
@@ -467,6 +532,8 @@ def main():
     random_velocity500()
     bench_systems()
     replicas()
+    jump500()
+    all_atom300()
     print("golden fixtures written to", HERE)
 
 

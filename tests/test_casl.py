@@ -46,10 +46,10 @@ def test_rejects_off_path_objects(cuda_lib, tmp_path):
 
 def test_rejects_unknown_keyword(cuda_lib, tmp_path):
     p = tmp_path / "bad.casl"
-    p.write_text("real rc 2.5\nneighborlist basic nl\nnl cutoff rc\nnl all_atom_test\n")
+    p.write_text("real rc 2.5\nneighborlist basic nl\nnl cutoff rc\nnl bin_resize\n")
     with pytest.raises(cuda_lib.CvrError) as e:
         cuda_lib.run_casl(str(p))
-    assert "all_atom_test" in str(e.value)
+    assert "bin_resize" in str(e.value)
 
 
 def test_requires_integrator_type(cuda_lib, tmp_path):

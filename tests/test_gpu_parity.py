@@ -365,3 +365,59 @@ def test_changed_dt_reaches_the_step_graphs(cuda_lib):
     c.set_integrator(0.5 * s.dt, 2.0)
     th_c = c.run(20, 10)
     assert np.array_equal(th_a, th_c)
+
+
+@pytest.mark.parametrize("prec", PRECS)
+def test_lj_jump_tol_vs_reference(cuda_lib, prec):
+    """cvr_set_lj_jump_tol (lj.cpp:118-127, 423-432) against the unmodified
+    reference's forces and virial on a fluid with pairs closer than
+    sqrt(jump_tol) (tests/golden/ref_ljjump500.npz); the clamp takes the
+    multi-type pair kernel."""
+    import importlib.util
+    import os
+    from helpers import GOLDEN
+    spec = importlib.util.spec_from_file_location("make_golden", os.path.join(GOLDEN, "make_golden.py"))
+    mg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mg)
+    d = np.load(os.path.join(GOLDEN, "ref_ljjump500.npz"))
+    s = mg.jump_system()
+    assert np.array_equal(s.pos, d["pos"])
+    sim = sim_for(cuda_lib, s, prec)
+    acc, th = sim.compute_forces()
+    check_forces(acc, d["acc"], prec)
+    tol = 1e-11 if prec == "fp64" else 1e-5
+    assert abs(th["virial"] - float(d["virial"])) <= tol * abs(float(d["virial"]))
+
+
+@pytest.mark.parametrize("prec", PRECS)
+def test_all_atom_test_vs_reference(cuda_lib, prec):
+    """cvr_set_all_atom_test (neighborlist.cpp:161-191): the pair set of every
+    owned pair and ghost image, forces, virial, S(k) and a 10-step run under
+    the reference's rebuild trigger against the unmodified reference with
+    `neigh all_atom_test` (tests/golden/ref_allatom300.npz)."""
+    import hashlib
+    import importlib.util
+    import os
+    from helpers import GOLDEN
+    spec = importlib.util.spec_from_file_location("make_golden", os.path.join(GOLDEN, "make_golden.py"))
+    mg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mg)
+    d = np.load(os.path.join(GOLDEN, "ref_allatom300.npz"))
+    s = mg.all_atom_system()
+    sim = sim_for(cuda_lib, s, prec, policy=cuda_lib.REBUILD_REFERENCE)
+    sim.set_all_atom_test(True)
+    acc, th = sim.compute_forces()
+    p = sim.pairs()
+    assert p.shape[0] == int(d["npairs"])
+    assert hashlib.sha256(np.ascontiguousarray(p, dtype="<i4").tobytes()).hexdigest() == str(d["pairs_sha256"])
+    check_forces(acc, d["acc"], prec)
+    tol = 1e-11 if prec == "fp64" else 1e-5
+    assert abs(th["virial"] - float(d["virial"])) <= tol * abs(float(d["virial"]))
+    sk = sim.sk()
+    ref_sk = d["sk"][0::2] + 1j * d["sk"][1::2]
+    assert np.abs(sk - ref_sk).max() <= (1e-11 if prec == "fp64" else 1e-5) * np.abs(ref_sk).max()
+    sim.run(int(d["run_steps"]))
+    pos, _, _ = sim.state()
+    dp = pos - d["run_pos"]
+    dp -= s.box * np.round(dp / s.box)
+    assert np.abs(dp).max() < (1e-9 if prec == "fp64" else 1e-5), np.abs(dp).max()

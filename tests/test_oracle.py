@@ -7,9 +7,12 @@
   and self energies, and a 20-step trajectory under the reference's rebuild
   policy.
 """
+import os
+
 import numpy as np
 import pytest
 
+from helpers import GOLDEN as GOLDEN_DIR
 from helpers import ewald_golden, load_ref_fixture
 
 FIXTURES = ["lj500", "ljmix500", "ions500"]
@@ -119,3 +122,48 @@ def test_live_reference_matches_oracle(oracle_lib):
     o.setup()
     assert np.array_equal(o.state()[2], ref["acc"])
     assert np.array_equal(o.pairs(), ref["pairs"])
+
+
+def _jump_system():
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("make_golden", os.path.join(GOLDEN_DIR, "make_golden.py"))
+    mg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mg)
+    return mg.jump_system()
+
+
+def test_jump_tol_matches_reference(oracle_lib):
+    """lj jump_tol (lj.cpp:118-127, 423-432): the restatement's clamp gives the
+    unmodified reference's forces and virial bit for bit on a fluid with close
+    pairs (tests/golden/ref_ljjump500.npz)."""
+    d = np.load(os.path.join(GOLDEN_DIR, "ref_ljjump500.npz"))
+    s = _jump_system()
+    assert np.array_equal(s.pos, d["pos"]) and s.lj.jump_tol == float(d["jump_tol"])
+    o = oracle_lib.Oracle(s)
+    o.setup()
+    assert np.array_equal(o.state()[2], d["acc"])
+    assert o.energy()["virial"] == float(d["virial"])
+
+
+def test_all_atom_test_matches_reference(oracle_lib):
+    """neighborlist all_atom_test (neighborlist.cpp:161-191): the restatement's
+    list (every owned pair, every ghost image) and forces equal the unmodified
+    reference's (tests/golden/ref_allatom300.npz), and so does a 10-step run
+    under the reference's rebuild trigger."""
+    import hashlib
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("make_golden", os.path.join(GOLDEN_DIR, "make_golden.py"))
+    mg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mg)
+    d = np.load(os.path.join(GOLDEN_DIR, "ref_allatom300.npz"))
+    s = mg.all_atom_system()
+    o = oracle_lib.Oracle(s, all_atom_test=True)
+    o.setup()
+    p = o.pairs()
+    assert p.shape[0] == int(d["npairs"])
+    assert hashlib.sha256(np.ascontiguousarray(p, dtype="<i4").tobytes()).hexdigest() == str(d["pairs_sha256"])
+    assert np.array_equal(o.state()[2], d["acc"])
+    o = oracle_lib.Oracle(s, all_atom_test=True, policy=oracle_lib.POLICY_REFERENCE)
+    o.setup()
+    o.step(int(d["run_steps"]))
+    assert np.array_equal(o.state()[0], d["run_pos"])
