@@ -1830,7 +1830,10 @@ int cvr_set_state(cvr_ctx *c, int64_t n, const double *pos, const double *vel, c
     c->list_valid = false;
     c->setup_done = false;
   }
-  cudaError_t e = cudaGetLastError();
+  // the host arrays are borrowed for this call only: the copies from them
+  // (asynchronous when they are pinned) end before it returns
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  if (e == cudaSuccess) e = cudaGetLastError();
   if (e != cudaSuccess) return fail(c, CVR_ERR_CUDA, cudaGetErrorString(e));
   return CVR_OK;
 }
