@@ -2,10 +2,10 @@
 // together: one persistent CTA per replica for all steps, all replicas in one
 // CUDA graph launch.
 //
-// No reference counterpart: the reference runs one system per process, and
-// its one-ghost-image scheme cannot hold boxes smaller than twice the list
-// radius (exchange_ghost_single_md_domain.cpp:59-99), which is where most of
-// these replicas sit (L = 4.3 .. 13.7 sigma).  Physics per replica: LJ with
+// No reference counterpart for the batching: the reference runs one system
+// per process (each replica as its own system needs its list radius and ghost
+// cutoff at L/2, the largest its one-ghost-image scheme allows,
+// exchange_ghost_single_md_domain.cpp:59-99).  Physics per replica: LJ with
 // the reference's linear force shift (lj.cpp:439-448) up to rc_lj, Ewald real
 // space (electrostatic_ewald_r.cpp:196-198) up to rc_r <= L/2 under the
 // minimum image (all pairs: at rc = L/2 half of all pairs are inside, so a
@@ -13,10 +13,14 @@
 // (initialize.cpp:184-222) and force (electrostatic_ewald_k.cpp:197-234).
 //
 // Layout: FP64 positions/velocities in global memory (concatenated, SoA);
-// each CTA keeps its replica's positions in shared memory as box-centred
-// FP32 hi/lo pairs (x = hi + lo), so the minimum-image displacement is
-// formed to ~1e-7 absolute from FP32 arithmetic; the k-space accumulation
-// S(k) is FP64; energies and virial are FP64 block sums.
+// each CTA keeps its replica's positions in shared memory as 32-bit
+// fixed-point coordinates u = round(x 2^32 / L) mod 2^32, so the minimum-image
+// displacement of a pair is the wrapping int32 difference (one integer
+// subtraction and one conversion per axis; resolution L / 2^32), the pair
+// constants are scaled to those units (h = L / 2^32) and the summed pair
+// forces are multiplied by 1/h once per atom; the k-space phases take their
+// argument m u mod 2^32 exactly in integer arithmetic.  The k-space
+// accumulation S(k) is FP64; energies and virial are FP64 block sums.
 //
 // Launch shape (threads per CTA) per replica size class is chosen by timing
 // candidates on the state itself (the autotuner below), replicas start in
@@ -76,6 +80,15 @@ __device__ __forceinline__ float2 conjf_if(float2 a, bool c) {
 
 using cvr::erfc_as;  // Abramowitz & Stegun 7.1.26 (cvr_device.cuh)
 
+// e^{i 2 pi m x / L} for the fixed-point coordinate u of x: m x / L = m u / 2^32,
+// reduced mod 1 exactly by the wrapping product, then sincospi of the signed
+// residue over 2^31 (in [-1, 1)).
+__device__ __forceinline__ float2 fixed_phase(uint32_t u, int m) {
+  float sn, cs;
+  sincospif((float)(int)((uint32_t)m * u) * 4.656612873077393e-10f, &sn, &cs);
+  return make_float2(cs, sn);
+}
+
 template <int TPB, int NV>
 __device__ __forceinline__ void block_sum(double (&v)[NV], double *red, double *out) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -100,7 +113,7 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double *red, double *
 struct Smem {
   float4 *ljc;      // per type pair: sig2, eps24, eps48, K (this replica's LJ cutoff)
   float4 *lje;      // per type pair: e4, C0, C1, k_e q_i q_j
-  float4 *xh, *xl;  // hi, lo of the box-centred position; type in xh.w, charge in xl.w
+  float4 *xh, *xl;  // xh: fixed-point coordinates (uint32 bits) and type; xl.w: charge
   double2 *skd;     // FP64 S(k) accumulators
   double *red;
   float2 *ak;   // (4 pi / V) f_k conj(S_k) for the k-force
@@ -138,9 +151,11 @@ __device__ inline Smem carve(unsigned char *raw, int nk, int np, int G) {
   return S;
 }
 
-// Per-replica pair constants and cutoffs.
+// Per-replica pair constants and cutoffs, in units of h = L / 2^32 (lengths
+// / h: rc2, rr2 / h^2, alpha * h, 2 alpha / sqrt(pi) * h, k_e / h; the LJ
+// tables likewise), so that a pair term takes the fixed-point displacement.
 struct PairK {
-  float Lh, Ll, iL, rc2, rr2, alpha2, alpha, tas, ke;
+  float rc2, rr2, alpha2, alpha, tas, ke;
   float4 lc, le;  // uniform LJ constants (UNI)
 };
 
@@ -149,13 +164,10 @@ struct PairK {
 template <bool UNI, bool EWR, bool EV>
 __device__ __forceinline__ float pair_c(const Smem &S, const PairK &K, const float4 &ih, const float4 &il,
                                         const float4 &jh, const float4 &jl, float (&d)[3], double (&e)[3], double w) {
-  const float hh[3] = {jh.x - ih.x, jh.y - ih.y, jh.z - ih.z};
-  const float ll[3] = {jl.x - il.x, jl.y - il.y, jl.z - il.z};
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    const float k = rintf(hh[a] * K.iL);
-    d[a] = fmaf(-k, K.Lh, hh[a]) + fmaf(-k, K.Ll, ll[a]);
-  }
+  // minimum image: the wrapping difference of the fixed-point coordinates
+  d[0] = (float)(int)(__float_as_uint(jh.x) - __float_as_uint(ih.x));
+  d[1] = (float)(int)(__float_as_uint(jh.y) - __float_as_uint(ih.y));
+  d[2] = (float)(int)(__float_as_uint(jh.z) - __float_as_uint(ih.z));
   const float r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
   float4 lc, le;
   if (UNI) {
@@ -253,16 +265,14 @@ __device__ void batch_forces(const BatchDev &p, const Smem &S, int r, int n, int
                              double (&ev)[5]) {
   constexpr int W = TPB / 32;
   const int warp = threadIdx.x >> 5;
+  const double h = L * 2.3283064365386963e-10;  // L / 2^32
   PairK K;
-  K.Lh = (float)L;
-  K.Ll = (float)(L - (double)K.Lh);
-  K.iL = (float)(1.0 / L);
-  K.rc2 = (float)(p.rc_lj[r] * p.rc_lj[r]);
-  K.rr2 = (float)(p.rc_r[r] * p.rc_r[r]);
-  K.alpha = (float)p.alpha;
+  K.rc2 = (float)(p.rc_lj[r] * p.rc_lj[r] / (h * h));
+  K.rr2 = (float)(p.rc_r[r] * p.rc_r[r] / (h * h));
+  K.alpha = (float)(p.alpha * h);
   K.alpha2 = K.alpha * K.alpha;
-  K.tas = (float)(2.0 * p.alpha * 0.56418958354775628695);
-  K.ke = (float)p.k_e;
+  K.tas = (float)(2.0 * p.alpha * 0.56418958354775628695 * h);
+  K.ke = (float)(p.k_e / h);
   K.lc = S.ljc[0];
   K.le = S.lje[0];
   const int nb = (n + 31) >> 5;
@@ -297,6 +307,16 @@ __device__ void batch_forces(const BatchDev &p, const Smem &S, int r, int n, int
     else
       tile_diag<UNI, false, EV>(S, K, I, n, e);
   }
+  __syncthreads();
+  // pair forces from units of h back to length units
+  {
+    const float inv_h = (float)(4294967296.0 / L);
+    for (int i = threadIdx.x; i < nb * 32; i += TPB) {
+      S.fsx[i] *= inv_h;
+      S.fsy[i] *= inv_h;
+      S.fsz[i] *= inv_h;
+    }
+  }
   if (EV) {
     ev[0] += e[0];
     ev[1] += e[1];
@@ -314,18 +334,9 @@ __device__ void batch_forces(const BatchDev &p, const Smem &S, int r, int n, int
       const int at = t / (3 * KP), rem = t % (3 * KP), dd = rem / KP, mm = rem % KP;
       float2 v = make_float2(0.f, 0.f);
       if (mm <= kmax) {
-        const float4 h = S.xh[a0 + at], lo = S.xl[a0 + at];
-        const float hx = dd == 0 ? h.x : (dd == 1 ? h.y : h.z);
-        const float lx = dd == 0 ? lo.x : (dd == 1 ? lo.y : lo.z);
-        // phase of the box-centred coordinate; e^{ik.(x - L/2)} = e^{ik.x} (-1)^m
-        const double u = (double)mm * (((double)hx + (double)lx) / L);
-        float sn, cs;
-        sincospif((float)(2.0 * (u - rint(u))), &sn, &cs);
-        if (mm & 1) {
-          sn = -sn;
-          cs = -cs;
-        }
-        v = make_float2(cs, sn);
+        const float4 h = S.xh[a0 + at];
+        const uint32_t u = __float_as_uint(dd == 0 ? h.x : (dd == 1 ? h.y : h.z));
+        v = fixed_phase(u, mm);
       }
       S.tab[t] = v;
     }
@@ -383,24 +394,12 @@ __device__ void batch_forces(const BatchDev &p, const Smem &S, int r, int n, int
   for (int i = threadIdx.x; i < nq; i += TPB) {
     float2 tx[KP], ty[KP], tz[KP];
     const float4 h = S.xh[i], lo = S.xl[i];
-    const double pc[3] = {(double)h.x + lo.x, (double)h.y + lo.y, (double)h.z + lo.z};
+    const uint32_t uc[3] = {__float_as_uint(h.x), __float_as_uint(h.y), __float_as_uint(h.z)};
 #pragma unroll
     for (int mm = 0; mm < KP; ++mm) {
-      float2 e3[3];
-#pragma unroll
-      for (int dd = 0; dd < 3; ++dd) {
-        const double u = (double)mm * (pc[dd] / L);
-        float sn, cs;
-        sincospif((float)(2.0 * (u - rint(u))), &sn, &cs);
-        if (mm & 1) {
-          sn = -sn;
-          cs = -cs;
-        }
-        e3[dd] = make_float2(cs, sn);
-      }
-      tx[mm] = e3[0];
-      ty[mm] = e3[1];
-      tz[mm] = e3[2];
+      tx[mm] = fixed_phase(uc[0], mm);
+      ty[mm] = fixed_phase(uc[1], mm);
+      tz[mm] = fixed_phase(uc[2], mm);
     }
     float fx = 0, fy = 0, fz = 0;
     for (int rr = 0; rr < p.nruns; ++rr) {
@@ -433,19 +432,17 @@ __device__ void batch_forces(const BatchDev &p, const Smem &S, int r, int n, int
   }
 }
 
-// Box-centred hi/lo FP32 copy of one atom's FP64 position (wrapped into [0, L)).
+// Fixed-point copy u = round(x 2^32 / L) mod 2^32 of one atom's FP64
+// position (the bits of u in xh.x-z, the type in xh.w, the charge in xl.w).
 __device__ __forceinline__ void to_smem(const BatchDev &p, const Smem &S, int i, long long gi, double L) {
-  double c[3] = {p.x[gi], p.y[gi], p.z[gi]};
-  float hv[3], lv[3];
+  const double sc = 4294967296.0 / L;
+  const double c[3] = {p.x[gi], p.y[gi], p.z[gi]};
+  uint32_t u[3];
 #pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    const double v = c[a] - 0.5 * L;
-    hv[a] = (float)v;
-    lv[a] = (float)(v - (double)hv[a]);
-  }
+  for (int a = 0; a < 3; ++a) u[a] = (uint32_t)(unsigned long long)llrint(c[a] * sc);  // 2^32 wraps to 0
   const int t = p.type[gi];
-  S.xh[i] = make_float4(hv[0], hv[1], hv[2], __int_as_float(t));
-  S.xl[i] = make_float4(lv[0], lv[1], lv[2], p.charge[t]);
+  S.xh[i] = make_float4(__uint_as_float(u[0]), __uint_as_float(u[1]), __uint_as_float(u[2]), __int_as_float(t));
+  S.xl[i] = make_float4(0.f, 0.f, 0.f, p.charge[t]);
 }
 
 // One launch: nsteps velocity-Verlet steps of replica order[first + blockIdx.x].
@@ -469,13 +466,17 @@ __global__ void __launch_bounds__(TPB, 1) k_batch(BatchDev p, int first, int nst
   if (threadIdx.x < TMAX * TMAX) {
     const int a = threadIdx.x / TMAX, b = threadIdx.x % TMAX, T = p.n_types;
     const bool ok = a < T && b < T;
-    const float rc2 = (float)(p.rc_lj[r] * p.rc_lj[r]);
-    const float e = ok ? p.eps[a * T + b] : 0.f, sg = ok ? p.sig[a * T + b] : 0.f;
-    const float rcinv = 1.f / rc2, c2 = sg * sg * rcinv, c6 = c2 * c2 * c2, c12 = c6 * c6;
-    const float g = 4.f * e * (12.f * c12 - 6.f * c6);
-    S.ljc[threadIdx.x] = make_float4(sg * sg, 24.f * e, 48.f * e, 4.f * e * (12.f * c12 * rcinv - 6.f * c6 * rcinv));
-    S.lje[threadIdx.x] = make_float4(4.f * e, -4.f * e * (c12 - c6) - 0.5f * g, g / (2.f * rc2),
-                                     ok ? (float)(p.k_e * p.chargeD[a] * p.chargeD[b]) : 0.f);
+    // in units of h = L / 2^32 (see PairK): sigma^2 / h^2, K h^2, C1 h^2, k_e q q / h
+    const double hh = L * 2.3283064365386963e-10, h2 = hh * hh;
+    const double rc2 = p.rc_lj[r] * p.rc_lj[r];
+    const double e = ok ? p.eps[a * T + b] : 0.0, sg = ok ? p.sig[a * T + b] : 0.0;
+    const double rcinv = 1.0 / rc2, c2 = sg * sg * rcinv, c6 = c2 * c2 * c2, c12 = c6 * c6;
+    const double g = 4.0 * e * (12.0 * c12 - 6.0 * c6);
+    S.ljc[threadIdx.x] = make_float4((float)(sg * sg / h2), (float)(24.0 * e), (float)(48.0 * e),
+                                     (float)(4.0 * e * (12.0 * c12 * rcinv - 6.0 * c6 * rcinv) * h2));
+    S.lje[threadIdx.x] = make_float4((float)(4.0 * e), (float)(-4.0 * e * (c12 - c6) - 0.5 * g),
+                                     (float)(g / (2.0 * rc2) * h2),
+                                     ok ? (float)(p.k_e * p.chargeD[a] * p.chargeD[b] / hh) : 0.f);
   }
   // f_k = exp(-k^2 / 4 alpha^2) / k^2 for this box (initialize.cpp:201-221)
   const double tpl = 6.28318530717958647692 / L, fa = 1.0 / (4.0 * p.alpha * p.alpha);

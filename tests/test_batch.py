@@ -19,10 +19,9 @@ from helpers import force_errors, golden_path
 
 # Mixed precision: FP32 pair / k-space terms on hi/lo FP32 coordinates, FP64 sums.
 FORCE_TOL = 1e-5  # global ||dF|| / ||F||
-# per atom, max_i |dF_i| / rms|F|: the all-pairs kernel sums up to 2047
-# partners and 1728 k-vectors per atom in FP32 (measured 1.5e-5 on a
-# 777-atom replica whose global error is 2.6e-6)
-MAX_TOL = 2e-5
+# per atom, max_i |dF_i| / rms|F| (measured <= 3.5e-6 over the twelve
+# replicas with fixed-point displacements; global errors ~1e-6)
+MAX_TOL = 1e-5
 ENERGY_TOL = 1e-5  # relative, per energy term
 
 
@@ -139,6 +138,7 @@ def test_batch_forces_and_energies(cuda_lib, oracle_lib):
     for r in range(len(SIZES)):
         ref, en = oracle_forces(oracle_lib, b, r)
         g, m, _ = force_errors(acc[replica(b, r)], ref)
+        print("replica", SIZES[r], "force error", g, m)
         assert g < FORCE_TOL and m < MAX_TOL, (SIZES[r], g, m)
         got = dict(zip(bt.OUT_KEYS, out[r]))
         for k in ("e_lj", "e_ewald_r", "e_ewald_k", "virial"):
