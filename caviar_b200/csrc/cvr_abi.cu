@@ -144,6 +144,7 @@ struct cvr_ctx {
   std::vector<size_t> snap_bytes;
   // cells
   int *cell_count{}, *cell_start{}, *cell_fill{}, *block_sums{};
+  unsigned long long *d_type_hist{};  // atoms per type of the last cvr_set_state (+ out-of-range count)
   // list
   uint32_t *nlist{};
   size_t nlist_bytes = 0;
@@ -1496,7 +1497,8 @@ int cvr_create(cvr_ctx **out, const double lo[3], const double hi[3], const int 
     delete c;
     return CVR_ERR_CUDA;
   }
-  if (dalloc(c, &c->flags, 4) != CVR_OK || dalloc(c, &c->counters, 2) != CVR_OK) {
+  if (dalloc(c, &c->flags, 4) != CVR_OK || dalloc(c, &c->counters, 2) != CVR_OK ||
+      dalloc(c, &c->d_type_hist, MAX_TYPES + 1) != CVR_OK) {
     cudaEventDestroy(c->k_fork);
     cudaEventDestroy(c->k_join);
     cudaStreamDestroy(c->kstream);
@@ -1769,19 +1771,6 @@ int cvr_set_state(cvr_ctx *c, int64_t n, const double *pos, const double *vel, c
   if (!c) return CVR_ERR_INVALID;
   if (n <= 0 || n > (int64_t)INDEX_MASK || !pos || !type) return fail(c, CVR_ERR_INVALID, "bad atom arrays");
   if (c->all_atom && n > CVR_ALL_ATOM_MAX) return fail(c, CVR_ERR_INVALID, "all_atom_test is for small systems");
-  // atoms per type (validates every type; the charge and mass sums below
-  // then cost one term per type instead of a dependent chain over atoms)
-  std::vector<int64_t> per_type((size_t)c->n_types, 0);
-  {
-    const uint32_t nt = (uint32_t)c->n_types;
-    bool bad = false;
-    for (int64_t i = 0; i < n; ++i) {
-      const uint32_t t = (uint32_t)type[i];
-      bad |= t >= nt;
-      per_type[t < nt ? t : 0]++;
-    }
-    if (bad) return fail(c, CVR_ERR_INVALID, "atom type out of range");
-  }
   cudaSetDevice(c->device);
   if (n != c->n || !c->x) {
     c->refreshed = false;
@@ -1792,18 +1781,29 @@ int cvr_set_state(cvr_ctx *c, int64_t n, const double *pos, const double *vel, c
     // list interleave: TPA lanes per atom, or quads of four entries when one lane per atom
     c->log2_tpa = (c->tpa == 32) ? 5 : (c->tpa == 8 ? 3 : 2);
   }
+  // Types first: atoms per type on the GPU (the range check of every type,
+  // and the charge and mass sums at one term per type), read back before
+  // the positions and velocities are sent.
+  CVR_CUDA(c, cudaMemcpyAsync(c->stage_i, type, (size_t)n * sizeof(int32_t), cudaMemcpyHostToDevice, c->stream));
+  CVR_CUDA(c, cudaMemsetAsync(c->d_type_hist, 0, (MAX_TYPES + 1) * sizeof(unsigned long long), c->stream));
+  k_type_hist<<<std::min<int64_t>(grid_for(n, 256), 4 * 148), 256, 0, c->stream>>>(c->stage_i, (int)n, c->n_types,
+                                                                                  c->d_type_hist);
+  c->launches++;
+  unsigned long long per_type[MAX_TYPES + 1];
+  CVR_CUDA(c, cudaMemcpyAsync(per_type, c->d_type_hist, sizeof(per_type), cudaMemcpyDeviceToHost, c->stream));
+  CVR_CUDA(c, cudaStreamSynchronize(c->stream));
+  if (per_type[MAX_TYPES] != 0) return fail(c, CVR_ERR_INVALID, "atom type out of range");
   CVR_CUDA(c, cudaMemcpyAsync(c->stage, pos, (size_t)n * 3 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   if (vel)
     CVR_CUDA(c, cudaMemcpyAsync(c->stage + 3 * n, vel, (size_t)n * 3 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-  CVR_CUDA(c, cudaMemcpyAsync(c->stage_i, type, (size_t)n * sizeof(int32_t), cudaMemcpyHostToDevice, c->stream));
   if (mol) CVR_CUDA(c, cudaMemcpyAsync(c->stage_i + n, mol, (size_t)n * sizeof(int32_t), cudaMemcpyHostToDevice, c->stream));
   c->have_state = true;
   const bool mol_changed = (mol != nullptr) != c->use_mol;
   c->use_mol = mol != nullptr;
   double q2 = 0, mt = 0;
   for (int t = 0; t < c->n_types; ++t) {
-    q2 += (double)per_type[(size_t)t] * (c->charge[t] * c->charge[t]);
-    mt += (double)per_type[(size_t)t] * c->mass[t];
+    q2 += (double)per_type[t] * (c->charge[t] * c->charge[t]);
+    mt += (double)per_type[t] * c->mass[t];
   }
   // the step graphs bake these in (thermo kernel, pair-kernel choice)
   if (mol_changed || mt != c->total_mass || q2 != c->q2_sum) c->epoch++;

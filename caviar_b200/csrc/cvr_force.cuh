@@ -1521,6 +1521,23 @@ __global__ void k_gather_state(DevState<real> s, double *__restrict__ pos, doubl
 }
 
 // Scatter the caller's AoS state (id order) into the SoA arrays.
+// Atoms per type (and, in hist[MAX_TYPES], atoms whose type is out of
+// [0, nt)) of the caller's type array: shared-memory counters per block,
+// one global add per counter and block (integer sums: order-free).
+__global__ void __launch_bounds__(256) k_type_hist(const int *__restrict__ type, int n, int nt,
+                                                   unsigned long long *__restrict__ hist) {
+  __shared__ unsigned int h[MAX_TYPES + 1];
+  for (int t = threadIdx.x; t <= MAX_TYPES; t += blockDim.x) h[t] = 0;
+  __syncthreads();
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const unsigned t = (unsigned)type[i];
+    atomicAdd(&h[t < (unsigned)nt ? t : MAX_TYPES], 1u);
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t <= MAX_TYPES; t += blockDim.x)
+    if (h[t]) atomicAdd(&hist[t], (unsigned long long)h[t]);
+}
+
 template <typename real>
 __global__ void k_scatter_state(DevState<real> s, const double *__restrict__ pos, const double *__restrict__ vel,
                                 const int *__restrict__ typ, const int *__restrict__ mol) {

@@ -421,3 +421,23 @@ def test_all_atom_test_vs_reference(cuda_lib, prec):
     dp = pos - d["run_pos"]
     dp -= s.box * np.round(dp / s.box)
     assert np.abs(dp).max() < (1e-9 if prec == "fp64" else 1e-5), np.abs(dp).max()
+
+
+def test_type_out_of_range_rejected_and_state_kept(cuda_lib):
+    """cvr_set_state checks every type on the GPU (atoms per type) before it
+    sends the positions: a type outside [0, n_types) is CVR_ERR_INVALID and
+    the context keeps its previous state (a run continues from it)."""
+    s, _ = load_ref_fixture("lj500")
+    sim = sim_for(cuda_lib, s, "fp64")
+    p0, v0, _ = sim.state()
+    bad = np.array(s.type, np.int32).copy()
+    bad[123] = s.n_types + 2
+    with pytest.raises(cuda_lib.CvrError) as e:
+        sim.set_state(s.pos + 0.01, s.vel, bad)
+    assert "type out of range" in str(e.value)
+    p1, v1, _ = sim.state()
+    assert np.array_equal(p0, p1) and np.array_equal(v0, v1)
+    ref = sim_for(cuda_lib, s, "fp64")
+    sim.run(5)
+    ref.run(5)
+    assert np.array_equal(sim.state()[0], ref.state()[0])
