@@ -1379,6 +1379,8 @@ int refresh(cvr_ctx *c) {
 // classes (the reference's list, neighborlist.cpp:161-191).
 int pairs_all_atom(cvr_ctx *c, std::vector<std::array<int32_t, 5>> &out) {
   const int64_t n = c->n;
+  // n (n - 1) / 2 owned pairs plus n per ghost image: host memory grows as n^2
+  if (n > 4096) return fail(c, CVR_ERR_CAPACITY, "the all_atom_test pair set is exported for at most 4096 atoms");
   std::vector<int> ids(n);
   std::vector<int8_t> g(n);
   CVR_CUDA(c, cudaMemcpyAsync(ids.data(), c->id, n * 4, cudaMemcpyDeviceToHost, c->stream));

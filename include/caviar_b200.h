@@ -83,8 +83,9 @@ int cvr_set_lj(cvr_ctx *ctx, double cutoff, const double *epsilon, const double 
  * its cutoff test; the Ewald real-space sum, which has none, runs over all of
  * them).  Forces come from an all-pairs kernel over the direct displacements
  * and the ghost images of this step's wrapped positions (rebuilt every
- * step); cvr_get_pairs returns that pair set.  At most CVR_ALL_ATOM_MAX atoms
- * (O(n^2) work).  on = 0 returns to the Verlet list. */
+ * step); cvr_get_pairs returns that pair set (for at most 4096 atoms, else
+ * CVR_ERR_CAPACITY).  At most CVR_ALL_ATOM_MAX atoms (O(n^2) work).  on = 0
+ * returns to the Verlet list. */
 #define CVR_ALL_ATOM_MAX 65536
 int cvr_set_all_atom_test(cvr_ctx *ctx, int on);
 
