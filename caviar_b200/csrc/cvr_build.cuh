@@ -341,12 +341,19 @@ __global__ void __launch_bounds__(128) k_build_list_warp(DevState<real> s, int c
     // cell-by-cell sweep below).
     constexpr int KP = (3 * (2 * MAX_STENCIL_R + 1) * (2 * MAX_STENCIL_R + 1) + 31) / 32;
     const int P = 3 * S * S;
+    // per piece: first candidate, length, and the list-entry bits of the
+    // piece (dy, dz fields and cell_x(j) + dxc + R in the dx field, less
+    // cell_x(j); wrapping 32-bit arithmetic, exact once cell_x(j) is added)
+    // with the image shift (sx + 1) | (sy + 1) << 2 | (sz + 1) << 4 in the
+    // low bits (the j field, zero in the entry bits)
     int pst[KP], plen[KP];
+    uint32_t pcode[KP];
 #pragma unroll
     for (int k = 0; k < KP; ++k) {
       const int p = 32 * k + lane;
       pst[k] = 0;
       plen[k] = 0;
+      pcode[k] = 0;
       if (p < P) {
         const int r = p / 3, sx = p % 3 - 1;
         const int dz = r / S - R, dy = r % S - R;
@@ -363,25 +370,38 @@ __global__ void __launch_bounds__(128) k_build_list_warp(DevState<real> s, int c
           const int rowbase = nc0 * (cy + dy - sy * nc1 + nc1 * (cz + dz - sz * nc2));
           pst[k] = s.cell_start[rowbase + ua - sx * nc0];
           plen[k] = s.cell_start[rowbase + ub - sx * nc0 + 1] - pst[k];
+          const int dxc = sx * nc0 - cx;  // dx = cell_x(j) + dxc
+          pcode[k] = (list_entry(0, 0, dy, dz, R, S) + (uint32_t)dxc * (1u << CODE_SHIFT)) |
+                     (uint32_t)((sx + 1) | ((sy + 1) << 2) | ((sz + 1) << 4));
         }
       }
     }
-#pragma unroll
+    constexpr uint32_t kUnshifted = 1u | (1u << 2) | (1u << 4);
     for (int k = 0; k < KP; ++k) {
-      for (int src = 0; src < 32; ++src) {
-        const int p = 32 * k + src;
-        if (p >= P) break;
-        const int len = __shfl_sync(0xffffffffu, plen[k], src);
-        if (len == 0) continue;
-        const int jb = __shfl_sync(0xffffffffu, pst[k], src);
-        const int r = p / 3, sx = p % 3 - 1;
-        const int dz = r / S - R, dy = r % S - R;
-        const int sz = floor_div(cz + dz, nc2), sy = floor_div(cy + dy, nc1);
+      // this round's pieces, selected with static indices (the arrays stay in registers)
+      int kst = pst[0], klen = plen[0];
+      uint32_t kcode = pcode[0];
+#pragma unroll
+      for (int t = 1; t < KP; ++t)
+        if (k == t) {
+          kst = pst[t];
+          klen = plen[t];
+          kcode = pcode[t];
+        }
+      unsigned todo = __ballot_sync(0xffffffffu, klen > 0);  // live pieces, in stencil order
+      while (todo) {
+        const int src = __ffs(todo) - 1;
+        todo &= todo - 1;
+        const int len = __shfl_sync(0xffffffffu, klen, src);
+        const int jb = __shfl_sync(0xffffffffu, kst, src);
+        const uint32_t pc = __shfl_sync(0xffffffffu, kcode, src);
+        const uint32_t code = pc & 63u;
+        const uint32_t ebase = pc & ~((1u << CODE_SHIFT) - 1u);
+        const int sx = (int)(code & 3u) - 1, sy = (int)((code >> 2) & 3u) - 1, sz = (int)(code >> 4) - 1;
         const float bx = sx * s.box.Lf[0] - xi.x, by = sy * s.box.Lf[1] - xi.y, bz = sz * s.box.Lf[2] - xi.z;
-        const bool shifted = (sx | sy | sz) != 0;
+        const bool shifted = code != kUnshifted;
         const bool fast_ok = !shifted || s.regular_images;
         const int self = shifted ? -1 : i;
-        const int dxc = sx * nc0 - cx;  // dx = cell_x(j) + dxc
         for (int base = 0; base < len; base += 32) {
           const int j = jb + base + lane;
           bool ok = false;
@@ -395,7 +415,8 @@ __global__ void __launch_bounds__(128) k_build_list_warp(DevState<real> s, int c
           const unsigned m = __ballot_sync(0xffffffffu, ok);
           if (ok && !count_only) {
             const int k2 = cnt + __popc(m & lt);
-            if (k2 < s.cap) row[list_slot(k2, log2_tpa, stride)] = list_entry(j, __float_as_int(q.w) + dxc, dy, dz, R, S);
+            if (k2 < s.cap)
+              row[list_slot(k2, log2_tpa, stride)] = (uint32_t)j | (ebase + ((uint32_t)__float_as_int(q.w) << CODE_SHIFT));
           }
           cnt += __popc(m);
         }

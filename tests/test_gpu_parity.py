@@ -184,12 +184,13 @@ def _lattice(nc, bc=(1, 1, 1), seed=5):
     return s
 
 
-@pytest.mark.parametrize("bc", [(1, 1, 1), (1, 0, 1)])
-def test_list_kernels_same_pair_set(cuda_lib, oracle_lib, bc):
+@pytest.mark.parametrize("nc,bc", [(10, (1, 1, 1)), (10, (1, 0, 1)), (3, (1, 1, 1)), (3, (0, 1, 1))])
+def test_list_kernels_same_pair_set(cuda_lib, oracle_lib, nc, bc):
     """Both list-search kernels (one thread per atom, one warp per atom)
     build the reference's pair set, and the FP64 forces from their lists
-    agree to rounding."""
-    s = _lattice(10, bc)
+    agree to rounding (the 108-atom box has fewer than 2R + 1 cells per
+    axis, so every stencil cell is searched as its own piece, with images)."""
+    s = _lattice(nc, bc)
     o = oracle_lib.Oracle(s)
     o.setup()
     ref = o.pairs()
