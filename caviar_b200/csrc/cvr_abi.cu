@@ -148,7 +148,7 @@ struct cvr_ctx {
   // list
   uint32_t *nlist{};
   size_t nlist_bytes = 0;
-  // flags: [flag, err, max_count, n_builds]
+  // flags: [flag, err, max_count, n_builds, build_epoch, clamp_mark]
   int *flags{};
   double *d_mass_inv{}, *d_mass{}, *d_charge{};
   void *d_coef{};
@@ -315,6 +315,8 @@ DevState<real> dev_state(cvr_ctx *c) {
   s.err = c->flags + 1;
   s.max_count = c->flags + 2;
   s.n_builds = c->flags + 3;
+  s.build_epoch = c->flags + 4;
+  s.clamp_mark = c->flags + 5;
   s.mass_inv = c->d_mass_inv;
   s.mass = c->d_mass;
   return s;
@@ -608,7 +610,7 @@ void launch_build(cvr_ctx *c, int count_only) {
   const int nb_scan = grid_for(c->ncells, 1024);
   k_bin_count<real><<<grid_for(n, 256), 256, 0, c->stream>>>(s);
   k_scan_local<<<nb_scan, 1024, 0, c->stream>>>(s.flag, c->cell_count, c->cell_start, c->block_sums, c->ncells);
-  k_scan_sums<<<1, 1024, 0, c->stream>>>(s.flag, c->block_sums, nb_scan, c->cell_start + c->ncells);
+  k_scan_sums<<<1, 1024, 0, c->stream>>>(s.flag, c->block_sums, nb_scan, c->cell_start + c->ncells, s.build_epoch);
   k_scan_add<<<nb_scan, 1024, 0, c->stream>>>(s.flag, c->cell_start, c->block_sums, c->ncells);
   k_bin_scatter<real><<<grid_for(n, 256), 256, 0, c->stream>>>(s);
   k_rank<real><<<grid_for(n, 256), 256, 0, c->stream>>>(s);
@@ -1499,7 +1501,7 @@ int cvr_create(cvr_ctx **out, const double lo[3], const double hi[3], const int 
     delete c;
     return CVR_ERR_CUDA;
   }
-  if (dalloc(c, &c->flags, 4) != CVR_OK || dalloc(c, &c->counters, 2) != CVR_OK ||
+  if (dalloc(c, &c->flags, 6) != CVR_OK || dalloc(c, &c->counters, 2) != CVR_OK ||
       dalloc(c, &c->d_type_hist, MAX_TYPES + 1) != CVR_OK) {
     cudaEventDestroy(c->k_fork);
     cudaEventDestroy(c->k_join);

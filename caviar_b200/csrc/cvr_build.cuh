@@ -67,6 +67,7 @@ __global__ void k_bin_count(DevState<real> s) {
   if (i >= s.n) return;
   double p[3] = {s.x[i], s.y[i], s.z[i]};
   int c[3];
+  bool clamped = false;
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
     if (s.box.bc[d] == 1) {
@@ -77,9 +78,12 @@ __global__ void k_bin_count(DevState<real> s) {
     }
     const double u = (p[d] - s.box.lo[d]) * s.cells.inv_w[d];
     int ci = (u >= 0.0) ? (int)fmin(u, 2.0e9) : -1;  // floor for u >= 0; NaN lands in cell 0
+    clamped = clamped || ci < 0 || ci >= s.cells.nc[d];
     ci = min(max(ci, 0), s.cells.nc[d] - 1);
     c[d] = ci;
   }
+  // an atom outside its cell's slab: the search must not clip rows by cell geometry
+  if (clamped) *s.clamp_mark = *s.build_epoch + 1;
   const int cell = c[0] + s.cells.nc[0] * (c[1] + s.cells.nc[1] * c[2]);
   s.tx[i] = p[0];
   s.ty[i] = p[1];
@@ -134,8 +138,9 @@ __global__ void __launch_bounds__(1024) k_scan_local(const int *__restrict__ fla
 }
 
 __global__ void __launch_bounds__(1024) k_scan_sums(const int *__restrict__ flag, int *__restrict__ block_sums, int nb,
-                                                     int *__restrict__ total_out) {
+                                                     int *__restrict__ total_out, int *__restrict__ build_epoch) {
   if (*flag == 0) return;
+  if (threadIdx.x == 0) *build_epoch += 1;  // after k_bin_count, before the list search
   __shared__ int wt[32];
   __shared__ int carry;
   if (threadIdx.x == 0) carry = 0;
@@ -341,6 +346,25 @@ __global__ void __launch_bounds__(128) k_build_list_warp(DevState<real> s, int c
     // cell-by-cell sweep below).
     constexpr int KP = (3 * (2 * MAX_STENCIL_R + 1) * (2 * MAX_STENCIL_R + 1) + 31) / 32;
     const int P = 3 * S * S;
+    // Each row is clipped to the cells that meet the rl sphere around atom i:
+    // with g_y, g_z the atom's distances to the row's y and z slabs, only
+    // cells within h = sqrt(rl^2 - g_y^2 - g_z^2) of it in x can hold a
+    // listed candidate.  Widened by a margin far above the FP32 rounding of
+    // these few operations (gaps shrunk and h grown by 1e-3 of a cell, rl^2
+    // taken at the top of the prefilter band), the clip only drops cells
+    // from the two ends of a row range, so every atom keeps the same entries
+    // in the same order.  f = the atom's place in its cell.  The clip needs
+    // every atom inside its cell's slab, which binning breaks only when it
+    // clamps a coordinate outside the box into an edge cell; such a build
+    // searches whole rows.
+    const float wx = (float)s.cells.w[0], wy = (float)s.cells.w[1], wz = (float)s.cells.w[2];
+    const float ivx = (float)s.cells.inv_w[0];
+    const float fx = (float)(pi[0] - s.box.lo[0] - cx * s.cells.w[0]);
+    const float fy = (float)(pi[1] - s.box.lo[1] - cy * s.cells.w[1]);
+    const float fz = (float)(pi[2] - s.box.lo[2] - cz * s.cells.w[2]);
+    const float dlt = 1e-3f * fminf(wx, fminf(wy, wz));
+    const float rc2 = s.rl_sq_hi;
+    const bool clip = *s.clamp_mark != *s.build_epoch;
     // per piece: first candidate, length, and the list-entry bits of the
     // piece (dy, dz fields and cell_x(j) + dxc + R in the dx field, less
     // cell_x(j); wrapping 32-bit arithmetic, exact once cell_x(j) is added)
@@ -358,7 +382,18 @@ __global__ void __launch_bounds__(128) k_build_list_warp(DevState<real> s, int c
         const int r = p / 3, sx = p % 3 - 1;
         const int dz = r / S - R, dy = r % S - R;
         const int sz = floor_div(cz + dz, nc2), sy = floor_div(cy + dy, nc1);
+        const float gy = fmaxf(fmaxf(dy * wy - fy, fy - (dy + 1) * wy) - dlt, 0.f);
+        const float gz = fmaxf(fmaxf(dz * wz - fz, fz - (dz + 1) * wz) - dlt, 0.f);
+        const float h2 = rc2 - gy * gy - gz * gz;
         int ua = cx - R, ub = cx + R;
+        if (clip && !(h2 >= 0.f)) {
+          ua = 1;  // the row misses the sphere
+          ub = 0;
+        } else if (clip) {
+          const float hx = sqrtf(h2) + dlt;
+          ua = cx + max(-R, min(R + 1, __float2int_rd((fx - hx) * ivx)));
+          ub = cx + min(R, max(-R - 1, __float2int_rd((fx + hx) * ivx)));
+        }
         if (sx < 0) ub = min(ub, -1);
         if (sx == 0) {
           ua = max(ua, 0);

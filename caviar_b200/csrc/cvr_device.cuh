@@ -87,6 +87,8 @@ template <typename real> struct DevState {
   int *err;        // sticky ERR_* bits
   int *max_count;  // largest neighbour count at the last build
   int *n_builds;
+  int *build_epoch;  // advanced once per build (k_scan_sums)
+  int *clamp_mark;   // build_epoch + 1 when that build's binning clamped a coordinate into an edge cell
   double *mass_inv;  // per type (device)
   double *mass;      // per type (device)
 };

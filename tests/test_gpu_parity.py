@@ -206,6 +206,27 @@ def test_list_kernels_same_pair_set(cuda_lib, oracle_lib, nc, bc):
         assert force_errors(acc[name], acc["thread"])[0] < 1e-13
 
 
+def test_list_kernels_atoms_outside_open_face(cuda_lib, oracle_lib):
+    """Atoms beyond a non-periodic face are binned into the edge cells; the
+    warp kernel's per-row clipping assumes every atom inside its cell, so a
+    build that clamps one searches whole rows: both kernels keep the pair of
+    two atoms outside the face, and the reference's pair set."""
+    s = _lattice(10, (1, 0, 1))
+    L = s.box
+    s.pos[0] = [3.0, L[1] + 0.6, 4.0]
+    s.pos[1] = [3.5, L[1] + 0.9, 4.2]
+    s.pos[2] = [8.0, -0.4, 8.0]
+    o = oracle_lib.Oracle(s)
+    o.setup()
+    ref = o.pairs()
+    assert ((ref[:, 0] == 0) & (ref[:, 1] == 1)).any() or ((ref[:, 0] == 1) & (ref[:, 1] == 0)).any()
+    for name in LIST_KERNELS:
+        sim = cuda_lib.Simulation(s, precision=cuda_lib.PREC_FP64, list_kernel=getattr(cuda_lib, "LIST_" + name.upper()))
+        sim.build_neighbors(True)
+        assert np.array_equal(sim.pairs(), ref), name
+        sim.close()
+
+
 def test_list_kernels_large_system_and_run(cuda_lib):
     """186,624 atoms (the size class where one thread per atom is the
     default): the warp kernel gives the same pair set at setup, and after a
