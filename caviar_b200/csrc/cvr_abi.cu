@@ -1156,7 +1156,7 @@ int build_graphs(cvr_ctx *c) {
     CVR_CUDA(c, cudaStreamEndCapture(c->stream, &post));
     if (r) return r;
     CVR_CUDA(c, cudaGraphAddChildGraphNode(&n_post, g, &n_cond, 1, post));
-    CVR_CUDA(c, cudaGraphInstantiate(&c->g_step[th], g, 0));
+    CVR_CUDA(c, cudaGraphInstantiate(&c->g_step[th], g, cudaGraphInstantiateFlagUseNodePriority));
     cudaGraphDestroy(pre);
     cudaGraphDestroy(post);
     cudaGraphDestroy(g);
@@ -1492,7 +1492,12 @@ int cvr_create(cvr_ctx **out, const double lo[3], const double hi[3], const int 
     delete c;
     return CVR_ERR_CUDA;
   }
-  if (cudaStreamCreateWithFlags(&c->kstream, cudaStreamNonBlocking) != cudaSuccess ||
+  // the S(k) side stream at the highest priority: its chain (phases, partials,
+  // reduction) gates the k-space force, while the pair kernel beside it has
+  // slack; step graphs keep the captured priorities (UseNodePriority)
+  int prio_least = 0, prio_greatest = 0;
+  cudaDeviceGetStreamPriorityRange(&prio_least, &prio_greatest);
+  if (cudaStreamCreateWithPriority(&c->kstream, cudaStreamNonBlocking, prio_greatest) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->k_fork, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->k_join, cudaEventDisableTiming) != cudaSuccess) {
     if (c->kstream) cudaStreamDestroy(c->kstream);
