@@ -602,6 +602,10 @@ int list_kernel_kind(const cvr_ctx *c) {
   return (c->n * 32 <= 4 * 1024 * 1024) ? CVR_LIST_WARP : CVR_LIST_THREAD;
 }
 
+bool phase_in_drift(const cvr_ctx *c);
+template <typename real>
+KArgs<real> kargs(cvr_ctx *c);
+
 template <typename real>
 void launch_build(cvr_ctx *c, int count_only) {
   Bracket br(c, CVR_KT_BUILD);
@@ -622,6 +626,10 @@ void launch_build(cvr_ctx *c, int count_only) {
     k_build_list<real><<<grid_for(n, 128), 128, 0, c->stream>>>(s, count_only, c->log2_tpa);
   }
   c->launches += 8;
+  if (phase_in_drift(c)) {  // the atoms moved in memory: the step's phase tables follow them
+    k_phase<real><<<grid_for(3 * c->n, 256), 256, 0, c->stream>>>(s, kargs<real>(c), s.flag);
+    c->launches++;
+  }
 }
 
 template <typename real, int TPA, bool LJ, bool EWR, bool EV, bool ONE_TYPE, bool FIXED>
@@ -759,11 +767,12 @@ size_t kf_smem(const cvr_ctx *c) {
 // M = 1..KMZ (one instance per M), else from shared memory.
 template <typename real, int MZ>
 struct KForceTable {
-  static void launch(cvr_ctx *c, const DevState<real> &s, const KArgs<real> &a) {
+  static void launch(cvr_ctx *c, const DevState<real> &s, const KArgs<real> &a, double kick_h) {
     if (c->kM == MZ)
-      k_kforce<real, MZ><<<grid_for(c->n, 32), dim3(32, c->kf_warps), kf_smem<real>(c), c->stream>>>(s, a, c->kf_tc);
+      k_kforce<real, MZ><<<grid_for(c->n, 32), dim3(32, c->kf_warps), kf_smem<real>(c), c->stream>>>(
+          s, a, c->kf_tc, kick_h, c->counters);
     else
-      KForceTable<real, MZ - 1>::launch(c, s, a);
+      KForceTable<real, MZ - 1>::launch(c, s, a, kick_h);
   }
   static void attrs(cvr_ctx *c) {
     cudaFuncSetAttribute(k_kforce<real, MZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -773,30 +782,50 @@ struct KForceTable {
 };
 template <typename real>
 struct KForceTable<real, 0> {
-  static void launch(cvr_ctx *c, const DevState<real> &s, const KArgs<real> &a) {
-    k_kforce<real, 0><<<grid_for(c->n, 32), dim3(32, c->kf_warps), kf_smem<real>(c), c->stream>>>(s, a, c->kf_tc);
+  static void launch(cvr_ctx *c, const DevState<real> &s, const KArgs<real> &a, double kick_h) {
+    k_kforce<real, 0><<<grid_for(c->n, 32), dim3(32, c->kf_warps), kf_smem<real>(c), c->stream>>>(
+        s, a, c->kf_tc, kick_h, c->counters);
   }
   static void attrs(cvr_ctx *c) {
     cudaFuncSetAttribute(k_kforce<real, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)std::max<size_t>(kf_smem<real>(c), 48 * 1024));
   }
 };
+// kick_h != 0: with the step's second half kick (v += kick_h a) fused.
 template <typename real>
-void launch_kforce(cvr_ctx *c, const DevState<real> &s, const KArgs<real> &a) {
-  KForceTable<real, KMZ>::launch(c, s, a);
+void launch_kforce(cvr_ctx *c, const DevState<real> &s, const KArgs<real> &a, double kick_h = 0.0) {
+  KForceTable<real, KMZ>::launch(c, s, a, kick_h);
 }
 
-// S(k) of the current positions: phase tables, chunk partials, reduction
-// (S(k), energy partials, force coefficients), on stream st.
+// S(k) of the current positions: phase tables (unless the position update
+// already wrote them), chunk partials, reduction (S(k), energy partials,
+// force coefficients), on stream st.
 template <typename real>
-void launch_sk(cvr_ctx *c, cudaStream_t st) {
+void launch_sk(cvr_ctx *c, cudaStream_t st, bool tables_fresh = false) {
   DevState<real> s = dev_state<real>(c);
   KArgs<real> a = kargs<real>(c);
-  k_phase<real><<<grid_for(3 * c->n, 256), 256, 0, st>>>(s, a);
+  if (!tables_fresh) {
+    k_phase<real><<<grid_for(3 * c->n, 256), 256, 0, st>>>(s, a, nullptr);
+    c->launches++;
+  }
   dim3 g1(grid_for(((c->kM + KMG - 1) / KMG) * c->nxy, 128), c->nchunks);
   k_sk_partial<real, KMG, KCH><<<g1, 128, sk_smem<real>(c), st>>>(s, a);
   k_sk_reduce<real, KRW><<<c->n_ek_blocks, KRW * 32, 0, st>>>(s, a);
-  c->launches += 3;
+  c->launches += 2;
+}
+
+// Whether the velocity-Verlet position update writes the S(k) phase tables
+// (k space on): then every list build rewrites them after reordering atoms,
+// and a step's S(k) chain starts at the chunk partials.
+bool phase_in_drift(const cvr_ctx *c) { return c->ewk_on && c->nk > 0 && c->integrator == 0 && c->d_ptab; }
+
+// Whether a plain (no thermo record) velocity-Verlet step fuses its second
+// half kick into the k-space force kernel: nothing else may touch the
+// accelerations or velocities after that kernel (slab correction, dipole
+// term, thermostat), and per-kernel timing keeps the kick separate.
+bool kick_in_kforce(const cvr_ctx *c, bool th) {
+  return !th && c->ewk_on && c->nk > 0 && c->integrator == 0 && !c->tstat.kind && !c->sc_on &&
+         !c->dipole_mode && !c->timing;
 }
 
 template <typename real>
@@ -936,7 +965,7 @@ int launch_slab(cvr_ctx *c) {
 }
 
 template <typename real>
-int forces_now(cvr_ctx *c, bool ev) {
+int forces_now(cvr_ctx *c, bool ev, bool tables_fresh = false, double kick_h = 0.0) {
   if (c->ewk_on && c->nk > 0 && !c->timing) {
     // The S(k) chain reads only positions and charges and the pair kernel
     // writes only the accelerations and its energy partials, so the chain
@@ -947,13 +976,13 @@ int forces_now(cvr_ctx *c, bool ev) {
     // event bracket.
     CVR_CUDA(c, cudaEventRecord(c->k_fork, c->stream));
     CVR_CUDA(c, cudaStreamWaitEvent(c->kstream, c->k_fork, 0));
-    launch_sk<real>(c, c->kstream);
+    launch_sk<real>(c, c->kstream, tables_fresh);
     CVR_CUDA(c, cudaEventRecord(c->k_join, c->kstream));
     launch_pair<real>(c, ev);
     CVR_CUDA(c, cudaStreamWaitEvent(c->stream, c->k_join, 0));
     DevState<real> s = dev_state<real>(c);
     KArgs<real> a = kargs<real>(c);
-    launch_kforce<real>(c, s, a);
+    launch_kforce<real>(c, s, a, kick_h);
     c->launches += 1;
   } else {
     launch_pair<real>(c, ev);
@@ -1041,9 +1070,10 @@ LangevinArgs langevin_args(cvr_ctx *c) {
 template <typename real>
 int launch_step_tail(cvr_ctx *c, bool th) {
   DevState<real> s = dev_state<real>(c);
-  if (int r = forces_now<real>(c, th)) return r;
+  const bool fused_kick = kick_in_kforce(c, th);
+  if (int r = forces_now<real>(c, th, phase_in_drift(c), fused_kick ? 0.5 * c->dt : 0.0)) return r;
   const int nb = grid_for(c->n, 256);
-  {
+  if (!fused_kick) {
     Bracket br(c, CVR_KT_INTEGRATE);
     if (c->integrator == 1) {
       const LangevinArgs lg = langevin_args(c);
@@ -1075,8 +1105,8 @@ int launch_step_tail(cvr_ctx *c, bool th) {
         k_thermostat_apply<real, false><<<nb, 256, 0, c->stream>>>(s, t.kind, c->d_tscal, c->ke_part);
       c->launches += 2;
     }
+    c->launches++;
   }
-  c->launches++;
   if (th) launch_thermo<real>(c, c->d_thermo);
   return CVR_OK;
 }
@@ -1086,8 +1116,10 @@ void launch_kick_drift(cvr_ctx *c) {
   Bracket br(c, CVR_KT_INTEGRATE);
   if (c->integrator == 1)
     k_lgv_kick_drift<real><<<grid_for(c->n, 256), 256, 0, c->stream>>>(dev_state<real>(c), c->dt, langevin_args(c));
+  else if (phase_in_drift(c))
+    k_kick_drift<real, true><<<grid_for(c->n, 256), 256, 0, c->stream>>>(dev_state<real>(c), c->dt, kargs<real>(c));
   else
-    k_kick_drift<real><<<grid_for(c->n, 256), 256, 0, c->stream>>>(dev_state<real>(c), c->dt);
+    k_kick_drift<real, false><<<grid_for(c->n, 256), 256, 0, c->stream>>>(dev_state<real>(c), c->dt, KArgs<real>{});
   c->launches++;
 }
 
@@ -1241,11 +1273,15 @@ int run_impl(cvr_ctx *c, int64_t nsteps, int64_t every, double *thermo) {
     if (int r = read_flags(c, f)) return r;
     collect_timing(c);
     if (graphs) {
-      // kernel nodes executed: per step kick_drift + condition + tail; 8 per rebuild
-      const int tail = 1 + (c->lj_on || c->ewr_on ? 1 : 0) + ((c->ewk_on && c->nk > 0) ? 4 : 0) +
-                       ((c->tstat.kind && c->integrator == 0) ? 2 : 0) + (c->sc_on ? 4 : 0) +
-                       ((c->ewk_on && c->dipole_mode) ? 3 : 0);
-      c->launches = launches0 + nsteps * (2 + tail) + nrec + 8 * (int64_t)(f[3] - f0[3]);
+      // kernel nodes executed: per step kick_drift + condition + forces +
+      // kick (fused into the k-space force on plain steps when possible) +
+      // thermo record; 8 per rebuild (9 when the build rewrites phase tables)
+      const int ks = (c->ewk_on && c->nk > 0) ? (phase_in_drift(c) ? 3 : 4) : 0;
+      const int tail = (c->lj_on || c->ewr_on ? 1 : 0) + ks + ((c->tstat.kind && c->integrator == 0) ? 2 : 0) +
+                       (c->sc_on ? 4 : 0) + ((c->ewk_on && c->dipole_mode) ? 3 : 0);
+      const int kick_plain = kick_in_kforce(c, false) ? 0 : 1;
+      c->launches = launches0 + nsteps * (2 + tail) + (nsteps - nrec) * kick_plain + nrec * 2 +
+                    (8 + (phase_in_drift(c) ? 1 : 0)) * (int64_t)(f[3] - f0[3]);
     }
     if (f[1] & ERR_NAN) return fail(c, CVR_ERR_NAN, "NaN acceleration");
     if (f[1] & ERR_OVERFLOW) {

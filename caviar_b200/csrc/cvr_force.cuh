@@ -470,8 +470,12 @@ __device__ __forceinline__ T conj_if(T a, bool c) {
 // Phase tables of every atom, once per force evaluation:
 // ptab[(d * kp + m) * n + i] = e^{i 2 pi m x_d / L_d}, m = 0..kmax_d
 // (row-major by (d, m), so 32 consecutive atoms are 32 consecutive words).
+// gate: when set, the launch belongs to a list build and returns unless the
+// build's flag is raised (the build reorders atoms: the step's tables, made
+// by the position update, are rewritten in the new order).
 template <typename real>
-__global__ void __launch_bounds__(256) k_phase(DevState<real> s, KArgs<real> a) {
+__global__ void __launch_bounds__(256) k_phase(DevState<real> s, KArgs<real> a, const int *__restrict__ gate) {
+  if (gate && *gate == 0) return;
   if (*s.err) return;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= 3 * s.n) return;
@@ -701,9 +705,17 @@ __device__ __forceinline__ void kf_term(const real (&q)[8], real zx, real zy, re
 // D = sum_m m (A+ z - A- conj z), then Im(P C) feeds F_x, F_y and Im(P D)
 // feeds F_z, P = X[nx] Y[ny].  The W partial forces of an atom are added in
 // warp order (deterministic).
+// kick_h != 0: the step's second half kick follows in the epilogue (v +=
+// kick_h a with the atom's final acceleration, as k_kick<real, false>, whose
+// flag reset and step count block 0 also takes over).
 template <typename real, int MZ>
 __global__ void __launch_bounds__(512, sizeof(real) == 4 ? CVR_KF_MINB : 1) k_kforce(DevState<real> s, KArgs<real> a,
-                                                                                  int TC) {
+                                                                                  int TC, double kick_h,
+                                                                                  long long *__restrict__ counters) {
+  if (kick_h != 0.0 && blockIdx.x == 0 && threadIdx.x == 0 && threadIdx.y == 0) {
+    *s.flag = 0;
+    if (counters) counters[0]++;
+  }
   using c2 = typename R2<real>::t;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x, w = threadIdx.y, W = blockDim.y;
@@ -802,6 +814,11 @@ __global__ void __launch_bounds__(512, sizeof(real) == 4 ? CVR_KF_MINB : 1) k_kf
   s.ax[i] += qm * a.two_pi_over_L[0] * fx;
   s.ay[i] += qm * a.two_pi_over_L[1] * fy;
   s.az[i] += qm * a.two_pi_over_L[2] * fz;
+  if (kick_h != 0.0) {
+    s.vx[i] = s.vx[i] + kick_h * (double)s.ax[i];
+    s.vy[i] = s.vy[i] + kick_h * (double)s.ay[i];
+    s.vz[i] = s.vz[i] + kick_h * (double)s.az[i];
+  }
 }
 
 // ------------------------------------------------------------- integrator
@@ -853,8 +870,10 @@ __device__ __forceinline__ bool update_local(DevState<real> &s, int i, const dou
   return need;
 }
 
-template <typename real>
-__global__ void __launch_bounds__(256) k_kick_drift(DevState<real> s, double dt) {
+// PHASE: also the atom's S(k) phase tables at the new position (the values
+// k_phase writes), so the step's S(k) chain starts at the chunk partials.
+template <typename real, bool PHASE>
+__global__ void __launch_bounds__(256) k_kick_drift(DevState<real> s, double dt, KArgs<real> ka) {
   if (*s.err) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   bool need = false;
@@ -871,6 +890,13 @@ __global__ void __launch_bounds__(256) k_kick_drift(DevState<real> s, double dt)
     s.y[i] = p[1];
     s.z[i] = p[2];
     need = update_local(s, i, p);
+    if constexpr (PHASE) {
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        const double x = p[d] * ka.inv_L[d];
+        for (int m = 0; m <= ka.kmax[d]; ++m) ka.ptab[(size_t)(d * ka.kp + m) * s.n + i] = phase<real>(x, m);
+      }
+    }
   }
   if (__any_sync(0xffffffffu, need) && (threadIdx.x & 31) == 0) *s.flag = 1;
 }
