@@ -24,12 +24,13 @@ TH_KEYS = ["step", "ke", "temperature", "e_lj", "e_ewald_r", "e_ewald_k", "e_sel
 N_THERMO = len(TH_KEYS)
 KT_PAIR, KT_KSPACE, KT_INTEGRATE, KT_BUILD = 0, 1, 2, 3
 LIST_AUTO, LIST_THREAD, LIST_WARP = 0, 1, 2
+KFORCE_AUTO, KFORCE_CUDA_CORES = 0, 1
 
 # Every symbol declared in include/caviar_b200.h.
 EXPORTED = ["cvr_create", "cvr_destroy", "cvr_set_neighborlist", "cvr_set_lj", "cvr_set_ewald_r", "cvr_set_ewald_k",
             "cvr_set_integrator", "cvr_set_langevin", "cvr_set_berendsen", "cvr_set_nose_hoover",
             "cvr_clear_thermostat", "cvr_set_ewald_k_geometry",
-            "cvr_set_ewald_slab_correction", "cvr_set_precision", "cvr_set_list_kernel", "cvr_set_state", "cvr_build_neighbors", "cvr_compute_forces",
+            "cvr_set_ewald_slab_correction", "cvr_set_precision", "cvr_set_list_kernel", "cvr_set_kspace_force_kernel", "cvr_set_state", "cvr_build_neighbors", "cvr_compute_forces",
             "cvr_run", "cvr_get_state", "cvr_get_pairs", "cvr_get_sk", "cvr_get_scalars", "cvr_last_error",
             "cvr_launch_count", "cvr_get_stream", "cvr_get_info", "cvr_set_kernel_timing", "cvr_kernel_time",
             "cvr_structure_factor_noalloc", "cvr_casl_run_file", "cvr_batch_create", "cvr_batch_destroy",
@@ -72,6 +73,7 @@ def load(path: str = LIB_PATH):
                                    ctypes.c_uint64]
     L.cvr_set_precision.argtypes = [vp, ctypes.c_int]
     L.cvr_set_list_kernel.argtypes = [vp, ctypes.c_int]
+    L.cvr_set_kspace_force_kernel.argtypes = [vp, ctypes.c_int]
     L.cvr_set_berendsen.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                     ctypes.c_double, ctypes.c_double]
     L.cvr_set_nose_hoover.argtypes = [vp, ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_double,
@@ -317,6 +319,10 @@ class Simulation:
     @property
     def stream(self) -> int:
         return int(self.L.cvr_get_stream(self.h) or 0)
+
+    def set_kspace_force_kernel(self, kind: int):
+        """KFORCE_AUTO (tensor cores where they apply) or KFORCE_CUDA_CORES."""
+        self._check(self.L.cvr_set_kspace_force_kernel(self.h, kind))
 
     def set_kernel_timing(self, on: bool):
         self._check(self.L.cvr_set_kernel_timing(self.h, int(on)))

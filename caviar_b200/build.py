@@ -13,7 +13,7 @@ SOURCES = [os.path.join(HERE, "csrc", "cvr_abi.cu"), os.path.join(HERE, "csrc", 
            os.path.join(HERE, "csrc", "cvr_casl.cpp"), os.path.join(HERE, "csrc", "cvr_batch.cu"),
            os.path.join(HERE, "csrc", "cvr_adjoint.cu"), os.path.join(HERE, "csrc", "cvr_peaks.cu")]
 CLI = os.path.join(HERE, "caviar_b200_casl")
-DEPS = SOURCES + [os.path.join(HERE, "csrc", f) for f in ("cvr_device.cuh", "cvr_build.cuh", "cvr_force.cuh", "cvr_main.cpp")] + [
+DEPS = SOURCES + [os.path.join(HERE, "csrc", f) for f in ("cvr_device.cuh", "cvr_build.cuh", "cvr_force.cuh", "cvr_kforce_tc.cuh", "cvr_main.cpp")] + [
     os.path.join(ROOT, "include", "caviar_b200.h")]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -21,6 +21,7 @@
 #include "cvr_build.cuh"
 #include "cvr_device.cuh"
 #include "cvr_force.cuh"
+#include "cvr_kforce_tc.cuh"
 
 // Stencil radius in cells: cells are at least rl / R wide, so every pair
 // within rl is at most R cells apart on each axis (R = 1 was measured: the
@@ -165,6 +166,10 @@ struct cvr_ctx {
   int nchunks = 0;
   int kf_warps = 1;  // k-force warps per block of 32 atoms
   int kf_tc = 1;     // k-force columns per staged tile of one warp
+  // tensor-core k-space force (mixed form): coefficient image and its tiles
+  float *d_kimg{};
+  int kimg_tiles = 0;
+  int kforce_kind = CVR_KFORCE_AUTO;  // cvr_set_kspace_force_kernel
   // diagnostics
   std::string err;
   int64_t launches = 0;
@@ -533,7 +538,20 @@ int setup_kspace(cvr_ctx *c) {
   CVR_CUDA(c, cudaMemcpyAsync(c->d_kpm, c->kpm.data(), c->kpm.size() * sizeof(int2), cudaMemcpyHostToDevice, c->stream));
   c->n_ek_blocks = grid_for(c->kM * c->nxy, 32);
   if (int r = dalloc(c, &c->ek_part, c->n_ek_blocks)) return r;
+  // the tensor-core k-space force holds 2 M <= KTC_K z components and
+  // kmax + 1 <= KTC_KPMAX phase rows per axis; its coefficient image is
+  // zero wherever k_sk_reduce does not write (padding)
+  c->kimg_tiles = 0;
+  if (c->precision != CVR_PREC_FP64 && 2 * c->kM <= KTC_K && c->kp <= KTC_KPMAX && c->nxy <= KTC_MAXCOLS) {
+    c->kimg_tiles = grid_for(c->nxy, KTC_COLS);
+    if (int r = dalloc(c, &c->d_kimg, (size_t)c->kimg_tiles * 2 * KTC_TILE_FLOATS)) return r;
+  }
   return CVR_OK;
+}
+
+// Whether the k-space force runs on the tensor cores (mixed form).
+bool kforce_tc(const cvr_ctx *c) {
+  return c->precision != CVR_PREC_FP64 && c->kimg_tiles > 0 && c->d_kimg && c->kforce_kind == CVR_KFORCE_AUTO;
 }
 
 int alloc_atoms(cvr_ctx *c, int64_t n) {
@@ -745,6 +763,7 @@ KArgs<real> kargs(cvr_ctx *c) {
   a.charge = c->d_charge;
   a.k_e = c->ewk_ke;
   a.nchunks = c->nchunks;
+  a.kimg = (sizeof(real) == 4 && kforce_tc(c)) ? c->d_kimg : nullptr;
   return a;
 }
 
@@ -794,6 +813,14 @@ struct KForceTable<real, 0> {
 // kick_h != 0: with the step's second half kick (v += kick_h a) fused.
 template <typename real>
 void launch_kforce(cvr_ctx *c, const DevState<real> &s, const KArgs<real> &a, double kick_h = 0.0) {
+  if constexpr (sizeof(real) == 4) {
+    if (a.kimg) {
+      // two blocks (a cluster) per 128 atoms
+      k_kforce_tc<<<2 * grid_for(c->n, KTC_ATOMS), KTC_THREADS, KTC_SMEM, c->stream>>>(s, a, c->kimg_tiles, kick_h,
+                                                                                      c->counters);
+      return;
+    }
+  }
   KForceTable<real, KMZ>::launch(c, s, a, kick_h);
 }
 
@@ -842,6 +869,7 @@ int launch_kspace(cvr_ctx *c) {
 
 template <typename real>
 void set_smem_attrs(cvr_ctx *c) {
+  if (sizeof(real) == 4) cudaFuncSetAttribute(k_kforce_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, KTC_SMEM);
   cudaFuncSetAttribute(k_sk_partial<real, KMG, KCH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)std::max<size_t>(sk_smem<real>(c), 48 * 1024));
   KForceTable<real, KMZ>::attrs(c);
@@ -1018,6 +1046,7 @@ int setup_run(cvr_ctx *c) {
   int f[4];
   if (int r = read_flags(c, f)) return r;
   if (f[1] & ERR_OVERFLOW) return fail(c, CVR_ERR_CAPACITY, "neighbour list overflow at setup");
+  if (f[1] & ERR_KSPACE_TC) return fail(c, CVR_ERR_CUDA, "tensor-core k-space force: a wait ran out");
   c->list_valid = true;
   c->setup_done = true;
   return CVR_OK;
@@ -1284,6 +1313,7 @@ int run_impl(cvr_ctx *c, int64_t nsteps, int64_t every, double *thermo) {
                     (8 + (phase_in_drift(c) ? 1 : 0)) * (int64_t)(f[3] - f0[3]);
     }
     if (f[1] & ERR_NAN) return fail(c, CVR_ERR_NAN, "NaN acceleration");
+    if (f[1] & ERR_KSPACE_TC) return fail(c, CVR_ERR_CUDA, "tensor-core k-space force: a wait ran out");
     if (f[1] & ERR_OVERFLOW) {
       // replay the call from the snapshot with a larger list
       if (int r = snapshot(c, true)) return r;
@@ -1791,6 +1821,14 @@ int cvr_clear_thermostat(cvr_ctx *c) {
   if (!c) return CVR_ERR_INVALID;
   c->tstat = ThermostatArgs{};
   c->epoch++;
+  return CVR_OK;
+}
+
+int cvr_set_kspace_force_kernel(cvr_ctx *c, int kind) {
+  if (!c) return CVR_ERR_INVALID;
+  if (kind != CVR_KFORCE_AUTO && kind != CVR_KFORCE_CUDA_CORES) return fail(c, CVR_ERR_INVALID, "unknown k-space force kernel");
+  if (kind != c->kforce_kind) c->epoch++;  // the step graphs bake the kernel and its arguments in
+  c->kforce_kind = kind;
   return CVR_OK;
 }
 

@@ -20,7 +20,7 @@
 
 namespace cvr {
 
-enum : int { ERR_NAN = 1, ERR_OVERFLOW = 2, ERR_GEOMETRY = 4 };
+enum : int { ERR_NAN = 1, ERR_OVERFLOW = 2, ERR_GEOMETRY = 4, ERR_KSPACE_TC = 8 };
 constexpr int CODE_SHIFT = 23;  // first of the three 3-bit stencil-offset fields
 constexpr unsigned INDEX_MASK = (1u << CODE_SHIFT) - 1u;
 constexpr int MAX_STENCIL_R = 3;  // dx + R must fit in 3 bits

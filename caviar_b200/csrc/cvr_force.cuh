@@ -422,6 +422,30 @@ __global__ void __launch_bounds__(128) k_pair_all(DevState<real> s, const PairCo
 // it).  e^{i k.r} = X[nx] Y[ny] Z[+-m] with Z[-m] = conj(Z[m]), so one
 // complex product P = X Y serves a whole column and each +-m pair costs
 // eight FMAs in both the S(k) and the force kernel.
+// Tensor-core form of the k-space force (k_kforce_tc, mixed form): per
+// block of 128 atoms, D[atom][(column, c)] = sum_k Z[atom][k] B[(column, c)][k]
+// with k = (Re z_m, Im z_m) for m < M (zero padded to KTC_K) and c = the
+// four sums Cx, Cy, Dx, Dy of k_kforce, as TF32 hi/lo halves (3 products
+// per term: hi hi + hi lo + lo hi, FP32-level).  B comes from k_sk_reduce as
+// an image of KTC_COLS-column tiles in the MMA's canonical K-major layout
+// without swizzle: 8-row x 16-byte core matrices, adjacent in K every 128
+// bytes, 8-row groups every KTC_K / 4 * 128 bytes.
+constexpr int KTC_ATOMS = 128;                      // atoms per block = TMEM lanes = MMA M
+constexpr int KTC_COLS = 64;                        // (nx, ny) columns per N-tile
+constexpr int KTC_N = 4 * KTC_COLS;                 // MMA N
+constexpr int KTC_K = 24;                           // 2 M <= 24
+constexpr int KTC_KPMAX = 12;                       // kmax + 1 per axis held for the epilogue
+constexpr int KTC_TILE_FLOATS = KTC_N * KTC_K;      // one operand image (hi or lo) of an N-tile
+__host__ __device__ constexpr int ktc_off(int r, int k) {  // byte offset of (row, k) in an operand image
+  return (r & 7) * 16 + (k >> 2) * 128 + (r >> 3) * (KTC_K / 4 * 128) + (k & 3) * 4;
+}
+// TF32 rounding (round to nearest, ties away) of an FP32 value, kept as FP32.
+__device__ __forceinline__ float to_tf32(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return __uint_as_float(r);
+}
+
 template <typename real> struct KArgs {
   int nk, nxy, M, kmax[3], kp;  // M = kmax_z + 1 m-values; kp = max kmax + 1
   const int2 *xy;               // (nx, ny) per column
@@ -438,6 +462,7 @@ template <typename real> struct KArgs {
   double *charge;               // per type
   double k_e;
   int nchunks;
+  float *kimg;                  // tensor-core coefficient image (k_kforce_tc), else null
 };
 
 // Phase e^{i 2 pi m x / L} from the fractional part of m x / L in FP64 (so
@@ -644,6 +669,23 @@ __global__ void __launch_bounds__(RW * 32) k_sk_reduce(DevState<real> s, KArgs<r
     for (int c = 0; c < 4; ++c) {
       o[c] = (real)c4[c];
       o[4 + c] = (real)(m * c4[c]);
+    }
+    if (a.kimg) {
+      // B rows of this column for k = 2m, 2m + 1: Cx (q0, q1), Cy (q2, q3),
+      // Dx (q7, -q6), Dy (-q5, q4) with q4..q7 = m q0..q3 (see kf_term)
+      float *hi = a.kimg + (size_t)(col / KTC_COLS) * 2 * KTC_TILE_FLOATS, *lo = hi + KTC_TILE_FLOATS;
+      const int rb = 4 * (col % KTC_COLS);
+      const float v[4][2] = {{(float)c4[0], (float)c4[1]},
+                             {(float)c4[2], (float)c4[3]},
+                             {(float)(m * c4[3]), -(float)(m * c4[2])},
+                             {-(float)(m * c4[1]), (float)(m * c4[0])}};
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const int o2 = ktc_off(rb + r, 2 * m) / 4;
+        const float h0 = to_tf32(v[r][0]), h1 = to_tf32(v[r][1]);
+        *reinterpret_cast<float2 *>(hi + o2) = make_float2(h0, h1);
+        *reinterpret_cast<float2 *>(lo + o2) = make_float2(to_tf32(v[r][0] - h0), to_tf32(v[r][1] - h1));
+      }
     }
   }
   double ev[1] = {e};

@@ -157,6 +157,16 @@ int cvr_set_langevin(cvr_ctx *c, double temperature, double friction, double kb,
  * atom up to 131072 atoms, else a thread per atom), CVR_LIST_THREAD one
  * thread per atom, CVR_LIST_WARP one warp per atom.  Takes effect at the
  * next list build. */
+/* k-space force kernel of the mixed form (a tuning and testing knob; both
+ * compute the reference's k-space force, electrostatic_ewald_k.cpp:197-234):
+ * CVR_KFORCE_AUTO takes the tensor cores (tcgen05 TF32 MMAs with hi/lo
+ * split operands, FP32-level sums) when k_max_z <= 11 and k_max <= 11 on
+ * every axis, else the CUDA-core kernel; CVR_KFORCE_CUDA_CORES always the
+ * latter.  The FP64 form always uses the CUDA-core kernel. */
+#define CVR_KFORCE_AUTO 0
+#define CVR_KFORCE_CUDA_CORES 1
+int cvr_set_kspace_force_kernel(cvr_ctx *ctx, int kind);
+
 #define CVR_LIST_AUTO 0
 #define CVR_LIST_THREAD 1
 #define CVR_LIST_WARP 2
