@@ -21,7 +21,10 @@
 // the columns of quarter w / 4 of every tile, so four warps share an atom
 // and hide each other's latency; their partial forces are added in quarter
 // order at the end (deterministic).  Z (hi, lo), the atoms' X, Y phase
-// rows and the column list are built in shared memory; B tiles (hi + lo,
+// rows for m = -kmax .. kmax (conjugates included) and per column the two
+// row offsets and (nx, ny) as floats are built in shared memory, so a
+// column costs one broadcast load, two table loads and ten flops in the
+// epilogue; B tiles (hi + lo,
 // 48 KB) arrive by bulk copy from the image k_sk_reduce writes, two buffers
 // deep.  Thread 0 issues the MMAs of tile j + 1 into the second TMEM
 // accumulator (2 x 256 columns) while the warps read tile j (tcgen05.ld, 32
@@ -41,11 +44,12 @@ constexpr int KTC_OFF_AHI = 0;
 constexpr int KTC_OFF_ALO = KTC_A_BYTES;
 constexpr int KTC_OFF_B0 = 2 * KTC_A_BYTES;
 constexpr int KTC_OFF_B1 = KTC_OFF_B0 + KTC_B_BYTES;
+constexpr int KTC_PROWS = 2 * KTC_KPMAX - 1;              // phase rows m = -kmax .. kmax per axis
 constexpr int KTC_OFF_TAB = KTC_OFF_B1 + KTC_B_BYTES;    // X rows then Y rows, atom-minor
-constexpr int KTC_TAB_BYTES = 2 * KTC_KPMAX * KTC_ATOMS * 8;
-constexpr int KTC_MAXCOLS = (2 * KTC_KPMAX - 1) * (2 * KTC_KPMAX - 1);  // (nx, ny) columns at most
-constexpr int KTC_OFF_XY = KTC_OFF_TAB + KTC_TAB_BYTES;                 // the column list
-constexpr int KTC_OFF_RED = KTC_OFF_XY + KTC_MAXCOLS * 8;                // partial forces [3][3][128]
+constexpr int KTC_TAB_BYTES = 2 * KTC_PROWS * KTC_ATOMS * 8;
+constexpr int KTC_MAXCOLS = KTC_PROWS * KTC_PROWS;                      // (nx, ny) columns at most
+constexpr int KTC_OFF_XY = KTC_OFF_TAB + KTC_TAB_BYTES;                 // per column: X, Y row offsets, nx, ny
+constexpr int KTC_OFF_RED = KTC_OFF_XY + KTC_MAXCOLS * 16;               // partial forces [3][3][128]
 constexpr int KTC_OFF_PEER = KTC_OFF_RED + 9 * KTC_ATOMS * 4;           // rank 1's forces [3][128] (rank 0)
 constexpr int KTC_OFF_BAR = KTC_OFF_PEER + 3 * KTC_ATOMS * 4;           // 4 mbarriers, TMEM slot, error words
 constexpr int KTC_SMEM = KTC_OFF_BAR + 64;
@@ -189,8 +193,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(KTC_THREADS, 1)
         *reinterpret_cast<float2 *>(alo + o) = make_float2(to_tf32(z[m].x - hx), to_tf32(z[m].y - hy));
       }
     } else if (qtr < 3) {
-      const int d = qtr - 1;  // 0: X rows, 1: Y rows
-      float2 *tab = reinterpret_cast<float2 *>(sm + KTC_OFF_TAB) + d * KTC_KPMAX * KTC_ATOMS;
+      const int d = qtr - 1;  // 0: X rows, 1: Y rows; row KTC_KPMAX - 1 + m holds e^{i 2 pi m x_d / L_d}
+      float2 *tab = reinterpret_cast<float2 *>(sm + KTC_OFF_TAB) + d * KTC_PROWS * KTC_ATOMS;
       float2 x[KTC_KPMAX];
 #pragma unroll
       for (int m = 0; m < KTC_KPMAX; ++m) {
@@ -198,10 +202,17 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(KTC_THREADS, 1)
         if (valid && m <= a.kmax[d]) x[m] = a.ptab[(size_t)(d * a.kp + m) * s.n + i];
       }
 #pragma unroll
-      for (int m = 0; m < KTC_KPMAX; ++m) tab[m * KTC_ATOMS + al] = x[m];
+      for (int m = 0; m < KTC_KPMAX; ++m) {
+        tab[(KTC_KPMAX - 1 + m) * KTC_ATOMS + al] = x[m];
+        if (m > 0) tab[(KTC_KPMAX - 1 - m) * KTC_ATOMS + al] = make_float2(x[m].x, -x[m].y);
+      }
     } else {
-      int2 *xy = reinterpret_cast<int2 *>(sm + KTC_OFF_XY);
-      for (int c = t - 3 * KTC_ATOMS; c < a.nxy; c += KTC_ATOMS) xy[c] = a.xy[c];
+      float4 *xy = reinterpret_cast<float4 *>(sm + KTC_OFF_XY);
+      for (int c = t - 3 * KTC_ATOMS; c < a.nxy; c += KTC_ATOMS) {
+        const int2 nn = a.xy[c];
+        const int ox = (KTC_KPMAX - 1 + nn.x) * KTC_ATOMS * 8, oy = (KTC_PROWS + KTC_KPMAX - 1 + nn.y) * KTC_ATOMS * 8;
+        xy[c] = make_float4(__int_as_float(ox), __int_as_float(oy), (float)nn.x, (float)nn.y);
+      }
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // Z visible to the tensor core
     if (warp == 0) {
@@ -238,8 +249,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(KTC_THREADS, 1)
         bad = true;
       }
     }
-    const float2 *tab = reinterpret_cast<const float2 *>(sm + KTC_OFF_TAB);
-    const int2 *xy = reinterpret_cast<const int2 *>(sm + KTC_OFF_XY);
+    const unsigned char *tab_al = sm + KTC_OFF_TAB + 8 * al;  // this atom's column of the phase rows
+    const float4 *xy = reinterpret_cast<const float4 *>(sm + KTC_OFF_XY);
     for (int jj = 0; jj < nloc; ++jj) {
       if (t == 0 && !bad && jj + 1 < nloc) {
         if (ktc_mbar_wait(bar_full((jj + 1) & 1), ((jj + 1) >> 1) & 1)) {
@@ -276,16 +287,15 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(KTC_THREADS, 1)
         for (int u = 0; u < 8; ++u) {
           const int c = c0 + 8 * q + u;
           if (c < a.nxy) {
-            const int2 nn = xy[c];
-            float2 X = tab[abs(nn.x) * KTC_ATOMS + al], Y = tab[(KTC_KPMAX + abs(nn.y)) * KTC_ATOMS + al];
-            if (nn.x < 0) X.y = -X.y;
-            if (nn.y < 0) Y.y = -Y.y;
+            const float4 ci = xy[c];
+            const float2 X = *reinterpret_cast<const float2 *>(tab_al + __float_as_int(ci.x));
+            const float2 Y = *reinterpret_cast<const float2 *>(tab_al + __float_as_int(ci.y));
             const float2 P = cmul(X, Y);
             const float Cx = __uint_as_float(r[4 * u]), Cy = __uint_as_float(r[4 * u + 1]);
             const float Dx = __uint_as_float(r[4 * u + 2]), Dy = __uint_as_float(r[4 * u + 3]);
             const float tt = P.x * Cy + P.y * Cx;
-            fx += (float)nn.x * tt;
-            fy += (float)nn.y * tt;
+            fx += ci.z * tt;
+            fy += ci.w * tt;
             fz += P.x * Dy + P.y * Dx;
           }
         }
