@@ -262,8 +262,10 @@ def ions_line(abi, W, torch, steps: int, warmup: int, device: int = 0):
         kms, kn = si.kernel_time(abi.KT_KSPACE)
         pms, pn = si.kernel_time(abi.KT_PAIR)
         bms, _ = si.kernel_time(abi.KT_BUILD)
-        nk = si.info()["nk"]
+        info = si.info()
+        nk = info["nk"]
         ion[nm] = {"value": s_ion.n * steps / (msi / 1e3), "ms_per_step": msi / steps, "list_builds": nbuilds,
+                   "kspace_force": "tcgen05 TF32 hi/lo" if info["kspace_tensor_cores"] else "CUDA cores",
                    "kernel_window_ms_per_step": msk / steps, "kspace_ms_per_step": kms / max(kn, 1),
                    "pair_ms_per_step": pms / max(pn, 1), "build_ms_per_step": bms / steps,
                    # algorithmic flops of the k-space pass: S(k) and the force each 4 FMA

@@ -306,10 +306,10 @@ class Simulation:
         return dict(zip(TH_KEYS, th.tolist()))
 
     def info(self) -> dict:
-        v = (ctypes.c_int64 * 14)()
-        self._check(self.L.cvr_get_info(self.h, v, 14))
+        v = (ctypes.c_int64 * 15)()
+        self._check(self.L.cvr_get_info(self.h, v, 15))
         keys = ["n", "ncx", "ncy", "ncz", "cap", "builds", "tpa", "nk", "R", "max_count", "err", "step",
-                "list_entries", "fixed_point"]
+                "list_entries", "fixed_point", "kspace_tensor_cores"]
         return dict(zip(keys, list(v)))
 
     @property

@@ -2040,9 +2040,10 @@ int cvr_get_info(const cvr_ctx *c, int64_t *out, int len) {
     cudaStreamSynchronize(c->stream);
     for (int v : cnt) entries += v;
   }
-  const int64_t v[14] = {c->n, c->nc[0], c->nc[1], c->nc[2], c->cap, flags[3], c->tpa, c->nk, c->R, flags[2],
-                         flags[1], c->step, entries, c->fixed};
-  for (int k = 0; k < len && k < 14; ++k) out[k] = v[k];
+  const int64_t v[15] = {c->n,     c->nc[0], c->nc[1], c->nc[2], c->cap,   flags[3], c->tpa,
+                         c->nk,    c->R,     flags[2], flags[1], c->step, entries,  c->fixed,
+                         (c->ewk_on && c->nk > 0 && kforce_tc(c)) ? 1 : 0};
+  for (int k = 0; k < len && k < 15; ++k) out[k] = v[k];
   return CVR_OK;
 }
 

@@ -246,7 +246,8 @@ void *cvr_get_stream(const cvr_ctx *ctx);         /* the cudaStream_t the contex
  * per atom, k-vectors, stencil radius, largest neighbour count, error bits,
  * step, total list entries (index 12 costs a device-to-host copy), 1 if the
  * mixed form's pair kernel uses fixed-point displacements (cubic box, see
- * cvr_set_precision). */
+ * cvr_set_precision), 1 if the k-space force runs on the tensor cores (see
+ * cvr_set_kspace_force_kernel). */
 int cvr_get_info(const cvr_ctx *ctx, int64_t *out, int len);
 
 /* Arithmetic-pipe peak of `device` for the compute side of the roofline (no
