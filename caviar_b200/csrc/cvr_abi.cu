@@ -161,6 +161,12 @@ struct cvr_ctx {
   // k space device
   double *d_fk{};
   int2 *d_kxy{}, *d_kpm{};
+  // S(k) columns actually summed (one of each mirror pair) and each column's source
+  std::vector<int2> kxyc;
+  std::vector<int> ksrc;
+  int2 *d_kxyc{};
+  int *d_ksrc{};
+  int ncomp = 0;
   double2 *d_kpartial{}, *d_sk{};
   void *d_ptab{}, *d_kcoef{};
   int nchunks = 0;
@@ -526,8 +532,34 @@ int setup_kspace(cvr_ctx *c) {
     int2 &e = c->kpm[(size_t)std::abs(z) * c->nxy + col_of[k]];
     (z >= 0 ? e.x : e.y) = k;
   }
+  // For real charges S(-nx, -ny, +-m) = conj(S(nx, ny, -+m)) (the phase
+  // products of the mirror are the exact conjugates), so of two columns that
+  // mirror each other only the first in column order is summed; k_sk_reduce
+  // conjugates it for the other.  Columns without their mirror in the
+  // (truncated) k-set are summed themselves.
+  {
+    std::map<std::pair<int, int>, int> col_index;
+    for (int q = 0; q < c->nxy; ++q) col_index[{c->kxy[q].x, c->kxy[q].y}] = q;
+    c->kxyc.clear();
+    c->ksrc.assign(c->nxy, 0);
+    std::vector<int> comp_of(c->nxy, -1);
+    for (int q = 0; q < c->nxy; ++q) {
+      const auto it = col_index.find({-c->kxy[q].x, -c->kxy[q].y});
+      const int mq = (it == col_index.end()) ? -1 : it->second;
+      if (mq >= 0 && mq < q && mq != q) {
+        c->ksrc[q] = comp_of[mq] | (1 << 30);  // taken from the earlier mirror
+      } else {
+        comp_of[q] = (int)c->kxyc.size();
+        c->ksrc[q] = comp_of[q];
+        c->kxyc.push_back(c->kxy[q]);
+      }
+    }
+    c->ncomp = (int)c->kxyc.size();
+  }
   c->kp = std::max(c->kmax[0], std::max(c->kmax[1], c->kmax[2])) + 1;
   if (int r = dalloc(c, &c->d_fk, c->nk)) return r;
+  if (int r = dalloc(c, &c->d_kxyc, c->ncomp)) return r;
+  if (int r = dalloc(c, &c->d_ksrc, c->nxy)) return r;
   if (int r = dalloc(c, &c->d_kxy, c->nxy)) return r;
   if (int r = dalloc(c, &c->d_kpm, c->kpm.size())) return r;
   if (int r = dalloc(c, &c->d_sk, c->nk)) return r;
@@ -535,6 +567,8 @@ int setup_kspace(cvr_ctx *c) {
   if (int r = dalloc(c, (unsigned char **)&c->d_kcoef, (size_t)c->nxy * c->kM * 8 * rb)) return r;
   CVR_CUDA(c, cudaMemcpyAsync(c->d_fk, c->fk.data(), c->nk * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   CVR_CUDA(c, cudaMemcpyAsync(c->d_kxy, c->kxy.data(), c->nxy * sizeof(int2), cudaMemcpyHostToDevice, c->stream));
+  CVR_CUDA(c, cudaMemcpyAsync(c->d_kxyc, c->kxyc.data(), c->ncomp * sizeof(int2), cudaMemcpyHostToDevice, c->stream));
+  CVR_CUDA(c, cudaMemcpyAsync(c->d_ksrc, c->ksrc.data(), c->nxy * sizeof(int), cudaMemcpyHostToDevice, c->stream));
   CVR_CUDA(c, cudaMemcpyAsync(c->d_kpm, c->kpm.data(), c->kpm.size() * sizeof(int2), cudaMemcpyHostToDevice, c->stream));
   c->n_ek_blocks = grid_for(c->kM * c->nxy, 32);
   if (int r = dalloc(c, &c->ek_part, c->n_ek_blocks)) return r;
@@ -744,6 +778,9 @@ KArgs<real> kargs(cvr_ctx *c) {
   KArgs<real> a{};
   a.nk = c->nk;
   a.nxy = c->nxy;
+  a.xyc = c->d_kxyc;
+  a.ksrc = c->d_ksrc;
+  a.ncomp = c->ncomp;
   a.M = c->kM;
   for (int d = 0; d < 3; ++d) {
     a.kmax[d] = c->kmax[d];
@@ -835,7 +872,7 @@ void launch_sk(cvr_ctx *c, cudaStream_t st, bool tables_fresh = false) {
     k_phase<real><<<grid_for(3 * c->n, 256), 256, 0, st>>>(s, a, nullptr);
     c->launches++;
   }
-  dim3 g1(grid_for(((c->kM + KMG - 1) / KMG) * c->nxy, 128), c->nchunks);
+  dim3 g1(grid_for(((c->kM + KMG - 1) / KMG) * c->ncomp, 128), c->nchunks);
   k_sk_partial<real, KMG, KCH><<<g1, 128, sk_smem<real>(c), st>>>(s, a);
   k_sk_reduce<real, KRW><<<c->n_ek_blocks, KRW * 32, 0, st>>>(s, a);
   c->launches += 2;

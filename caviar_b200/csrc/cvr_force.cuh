@@ -449,6 +449,11 @@ __device__ __forceinline__ float to_tf32(float x) {
 template <typename real> struct KArgs {
   int nk, nxy, M, kmax[3], kp;  // M = kmax_z + 1 m-values; kp = max kmax + 1
   const int2 *xy;               // (nx, ny) per column
+  // S(k) symmetry: S(-nx, -ny, +-m) = conj(S(nx, ny, -+m)) for real charges,
+  // so only ncomp columns (one of each mirror pair present) are summed:
+  const int2 *xyc;              // (nx, ny) of the summed columns
+  const int *ksrc;              // per column: its summed column, | 1 << 30 if taken from the mirror
+  int ncomp;
   const int2 *kpm;              // [M][nxy] k indices of (nx, ny, +m), (nx, ny, -m)
   const double *fk;             // exp(-k^2/4a^2)/k^2 per used k
   typename R2<real>::t *ptab;   // phase tables [3 * kp][n]
@@ -554,9 +559,9 @@ __global__ void __launch_bounds__(128) k_sk_partial(DevState<real> s, KArgs<real
   for (int t = threadIdx.x; t < CH; t += blockDim.x) q[t] = (t < na) ? (real)a.charge[s.type[a0 + t]] : (real)0;
   __syncthreads();
   const int task = blockIdx.x * blockDim.x + threadIdx.x;
-  if (task >= ngroups * a.nxy) return;
-  const int g = task / a.nxy, col = task - g * a.nxy;
-  const int2 nn = a.xy[col];
+  if (task >= ngroups * a.ncomp) return;
+  const int g = task / a.ncomp, col = task - g * a.ncomp;  // a summed column
+  const int2 nn = a.xyc[col];
   const int ox = abs(nn.x), oy = a.kp + abs(nn.y), oz = 2 * a.kp + g * MG;
   const bool cx = nn.x < 0, cy = nn.y < 0;
   double tot[MG][4];
@@ -595,7 +600,7 @@ __global__ void __launch_bounds__(128) k_sk_partial(DevState<real> s, KArgs<real
 #pragma unroll
   for (int u = 0; u < MG; ++u) {
     if (g * MG + u < a.M) {
-      const size_t idx = ((size_t)blockIdx.y * a.M + g * MG + u) * a.nxy + col;
+      const size_t idx = ((size_t)blockIdx.y * a.M + g * MG + u) * a.ncomp + col;
       a.partial[2 * idx] = make_double2(tot[u][0], tot[u][1]);
       a.partial[2 * idx + 1] = make_double2(tot[u][2], tot[u][3]);
     }
@@ -605,6 +610,8 @@ __global__ void __launch_bounds__(128) k_sk_partial(DevState<real> s, KArgs<real
 // S(k) = sum of the chunk partials (RW warps: warp w adds chunks w, w + RW,
 // ... in order, four loads in flight; then warp 0 adds the RW sums in warp
 // order: a fixed order, deterministic), one lane per (column, m) pair.
+// A column taken from its mirror reads the mirror's sums and conjugates
+// them with +m and -m swapped (exact).
 // Writes S(k), the FP64 k-space energy partials sum_k f_k |S_k|^2, and the
 // force coefficients of the pair: with A_k = (4 pi / V) f_k conj(S_k) =
 // a + ib at +m and c + id at -m, kcoef = (a+c, d-b, b+d, a-c) and the same
@@ -614,8 +621,11 @@ __global__ void __launch_bounds__(RW * 32) k_sk_reduce(DevState<real> s, KArgs<r
   __shared__ double part[RW][4][32];
   if (*s.err) return;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int np = a.M * a.nxy;
+  const int np = a.M * a.nxy, npc = a.M * a.ncomp;
   const int p = blockIdx.x * 32 + lane;
+  const int pm = p / a.nxy, pcol = p - pm * a.nxy;  // (m, column) of this lane
+  const int src = (p < np) ? a.ksrc[pcol] : 0;
+  const int pc = pm * a.ncomp + (src & ((1 << 30) - 1));  // its summed (m, column)
   double v[4] = {0.0, 0.0, 0.0, 0.0};
   if (p < np) {
     for (int c0 = w; c0 < a.nchunks; c0 += 4 * RW) {
@@ -623,7 +633,7 @@ __global__ void __launch_bounds__(RW * 32) k_sk_reduce(DevState<real> s, KArgs<r
 #pragma unroll
       for (int h = 0; h < 4; ++h) {
         const int c = c0 + h * RW;
-        const size_t idx = (size_t)min(c, a.nchunks - 1) * np + p;
+        const size_t idx = (size_t)min(c, a.nchunks - 1) * npc + pc;
         u[h][0] = a.partial[2 * idx];
         u[h][1] = a.partial[2 * idx + 1];
       }
@@ -647,6 +657,13 @@ __global__ void __launch_bounds__(RW * 32) k_sk_reduce(DevState<real> s, KArgs<r
     for (int ww = 0; ww < RW; ++ww)
 #pragma unroll
       for (int c = 0; c < 4; ++c) S[c] += part[ww][c][lane];
+    if (src >> 30) {  // the mirror's sums: S(+m) = conj(S'(-m)), S(-m) = conj(S'(+m))
+      const double t0 = S[0], t1 = S[1];
+      S[0] = S[2];
+      S[1] = -S[3];
+      S[2] = t0;
+      S[3] = -t1;
+    }
     const int2 kk = a.kpm[p];
     double A[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
