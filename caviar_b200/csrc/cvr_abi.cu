@@ -166,6 +166,8 @@ struct cvr_ctx {
   std::vector<int> ksrc;
   int2 *d_kxyc{};
   int *d_ksrc{};
+  std::vector<int> kmir;  // per summed column: the column taken from it, or -1
+  int *d_kmir{};
   int ncomp = 0;
   double2 *d_kpartial{}, *d_sk{};
   void *d_ptab{}, *d_kcoef{};
@@ -541,6 +543,7 @@ int setup_kspace(cvr_ctx *c) {
     std::map<std::pair<int, int>, int> col_index;
     for (int q = 0; q < c->nxy; ++q) col_index[{c->kxy[q].x, c->kxy[q].y}] = q;
     c->kxyc.clear();
+    c->kmir.clear();
     c->ksrc.assign(c->nxy, 0);
     std::vector<int> comp_of(c->nxy, -1);
     for (int q = 0; q < c->nxy; ++q) {
@@ -548,10 +551,12 @@ int setup_kspace(cvr_ctx *c) {
       const int mq = (it == col_index.end()) ? -1 : it->second;
       if (mq >= 0 && mq < q && mq != q) {
         c->ksrc[q] = comp_of[mq] | (1 << 30);  // taken from the earlier mirror
+        c->kmir[comp_of[mq]] = q;
       } else {
         comp_of[q] = (int)c->kxyc.size();
         c->ksrc[q] = comp_of[q];
         c->kxyc.push_back(c->kxy[q]);
+        c->kmir.push_back(-1);
       }
     }
     c->ncomp = (int)c->kxyc.size();
@@ -560,6 +565,7 @@ int setup_kspace(cvr_ctx *c) {
   if (int r = dalloc(c, &c->d_fk, c->nk)) return r;
   if (int r = dalloc(c, &c->d_kxyc, c->ncomp)) return r;
   if (int r = dalloc(c, &c->d_ksrc, c->nxy)) return r;
+  if (int r = dalloc(c, &c->d_kmir, c->ncomp)) return r;
   if (int r = dalloc(c, &c->d_kxy, c->nxy)) return r;
   if (int r = dalloc(c, &c->d_kpm, c->kpm.size())) return r;
   if (int r = dalloc(c, &c->d_sk, c->nk)) return r;
@@ -569,6 +575,7 @@ int setup_kspace(cvr_ctx *c) {
   CVR_CUDA(c, cudaMemcpyAsync(c->d_kxy, c->kxy.data(), c->nxy * sizeof(int2), cudaMemcpyHostToDevice, c->stream));
   CVR_CUDA(c, cudaMemcpyAsync(c->d_kxyc, c->kxyc.data(), c->ncomp * sizeof(int2), cudaMemcpyHostToDevice, c->stream));
   CVR_CUDA(c, cudaMemcpyAsync(c->d_ksrc, c->ksrc.data(), c->nxy * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  CVR_CUDA(c, cudaMemcpyAsync(c->d_kmir, c->kmir.data(), c->ncomp * sizeof(int), cudaMemcpyHostToDevice, c->stream));
   CVR_CUDA(c, cudaMemcpyAsync(c->d_kpm, c->kpm.data(), c->kpm.size() * sizeof(int2), cudaMemcpyHostToDevice, c->stream));
   c->n_ek_blocks = grid_for(c->kM * c->nxy, 32);
   if (int r = dalloc(c, &c->ek_part, c->n_ek_blocks)) return r;
@@ -576,8 +583,8 @@ int setup_kspace(cvr_ctx *c) {
   // kmax + 1 <= KTC_KPMAX phase rows per axis; its coefficient image is
   // zero wherever k_sk_reduce does not write (padding)
   c->kimg_tiles = 0;
-  if (c->precision != CVR_PREC_FP64 && 2 * c->kM <= KTC_K && c->kp <= KTC_KPMAX && c->nxy <= KTC_MAXCOLS) {
-    c->kimg_tiles = grid_for(c->nxy, KTC_COLS);
+  if (c->precision != CVR_PREC_FP64 && 2 * c->kM <= KTC_K && c->kp <= KTC_KPMAX && c->ncomp <= KTC_MAXCOLS) {
+    c->kimg_tiles = grid_for(c->ncomp, KTC_COLS);
     if (int r = dalloc(c, &c->d_kimg, (size_t)c->kimg_tiles * 2 * KTC_TILE_FLOATS)) return r;
   }
   return CVR_OK;
@@ -781,6 +788,7 @@ KArgs<real> kargs(cvr_ctx *c) {
   a.xyc = c->d_kxyc;
   a.ksrc = c->d_ksrc;
   a.ncomp = c->ncomp;
+  a.kmir = c->d_kmir;
   a.M = c->kM;
   for (int d = 0; d < 3; ++d) {
     a.kmax[d] = c->kmax[d];
@@ -1459,10 +1467,10 @@ int refresh(cvr_ctx *c) {
     // k-force launch shape: warps per block of 32 atoms until ~24 warps per
     // SM exist (at most 16, at most one per column)
     const int atom_blocks = grid_for(c->n, 32);
-    c->kf_warps = std::max(1, std::min(std::min(KF_WMAX, c->nxy), (24 * 148 + atom_blocks - 1) / atom_blocks));
+    c->kf_warps = std::max(1, std::min(std::min(KF_WMAX, c->ncomp), (24 * 148 + atom_blocks - 1) / atom_blocks));
     // columns per warp staged in tiles of equal size within KF_COEF_SMEM
     {
-      const int per_warp = (c->nxy + c->kf_warps - 1) / c->kf_warps;
+      const int per_warp = (c->ncomp + c->kf_warps - 1) / c->kf_warps;
       const int tc_max = std::max<int>(1, (int)(KF_COEF_SMEM / ((size_t)c->kf_warps * c->kM * 8 * (c2b / 2))));
       const int ntiles = (per_warp + tc_max - 1) / tc_max;
       c->kf_tc = (per_warp + ntiles - 1) / ntiles;

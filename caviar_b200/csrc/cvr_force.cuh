@@ -453,6 +453,7 @@ template <typename real> struct KArgs {
   // so only ncomp columns (one of each mirror pair present) are summed:
   const int2 *xyc;              // (nx, ny) of the summed columns
   const int *ksrc;              // per column: its summed column, | 1 << 30 if taken from the mirror
+  const int *kmir;              // per summed column: the column taken from it (its mirror), or -1
   int ncomp;
   const int2 *kpm;              // [M][nxy] k indices of (nx, ny, +m), (nx, ny, -m)
   const double *fk;             // exp(-k^2/4a^2)/k^2 per used k
@@ -665,43 +666,57 @@ __global__ void __launch_bounds__(RW * 32) k_sk_reduce(DevState<real> s, KArgs<r
       S[3] = -t1;
     }
     const int2 kk = a.kpm[p];
-    double A[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
       const int k = h ? kk.y : kk.x;
       if (k >= 0) {
         const double sr = S[2 * h], si = S[2 * h + 1];
         a.sk[k] = make_double2(sr, si);
-        const double f = a.fk[k];
-        const double cf = a.four_pi_over_v * f;
-        A[2 * h] = cf * sr;
-        A[2 * h + 1] = -cf * si;
-        e += f * (sr * sr + si * si);
+        e += a.fk[k] * (sr * sr + si * si);
       }
     }
-    const int m = p / a.nxy, col = p - m * a.nxy;
-    const double c4[4] = {A[0] + A[2], A[3] - A[1], A[1] + A[3], A[0] - A[2]};
-    real *o = a.kcoef + ((size_t)col * a.M + m) * 8;
+    if (!(src >> 30)) {
+      // force coefficients of a summed column: k and its mirror -k (in the
+      // column taken from this one) give the same force term, so the
+      // coefficient of (column, +-m) counts whichever of the two are in the set
+      const int m = pm, col = src;  // col: the summed column's index
+      const int mir = a.kmir[col];
+      const int2 mk = (mir >= 0) ? a.kpm[(size_t)m * a.nxy + mir] : make_int2(-1, -1);
+      double A[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      o[c] = (real)c4[c];
-      o[4 + c] = (real)(m * c4[c]);
-    }
-    if (a.kimg) {
-      // B rows of this column for k = 2m, 2m + 1: Cx (q0, q1), Cy (q2, q3),
-      // Dx (q7, -q6), Dy (-q5, q4) with q4..q7 = m q0..q3 (see kf_term)
-      float *hi = a.kimg + (size_t)(col / KTC_COLS) * 2 * KTC_TILE_FLOATS, *lo = hi + KTC_TILE_FLOATS;
-      const int rb = 4 * (col % KTC_COLS);
-      const float v[4][2] = {{(float)c4[0], (float)c4[1]},
-                             {(float)c4[2], (float)c4[3]},
-                             {(float)(m * c4[3]), -(float)(m * c4[2])},
-                             {-(float)(m * c4[1]), (float)(m * c4[0])}};
+      for (int h = 0; h < 2; ++h) {
+        const int k = h ? kk.y : kk.x, km = h ? mk.x : mk.y;  // (column, +-m) and the mirror's (-+m)
+        const int kf = (k >= 0) ? k : km;
+        if (kf >= 0) {
+          const double wgt = (k >= 0 ? 1.0 : 0.0) + (km >= 0 ? 1.0 : 0.0);
+          const double cf = a.four_pi_over_v * a.fk[kf] * wgt;
+          A[2 * h] = cf * S[2 * h];
+          A[2 * h + 1] = -cf * S[2 * h + 1];
+        }
+      }
+      const double c4[4] = {A[0] + A[2], A[3] - A[1], A[1] + A[3], A[0] - A[2]};
+      real *o = a.kcoef + ((size_t)col * a.M + m) * 8;
 #pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        const int o2 = ktc_off(rb + r, 2 * m) / 4;
-        const float h0 = to_tf32(v[r][0]), h1 = to_tf32(v[r][1]);
-        *reinterpret_cast<float2 *>(hi + o2) = make_float2(h0, h1);
-        *reinterpret_cast<float2 *>(lo + o2) = make_float2(to_tf32(v[r][0] - h0), to_tf32(v[r][1] - h1));
+      for (int c = 0; c < 4; ++c) {
+        o[c] = (real)c4[c];
+        o[4 + c] = (real)(m * c4[c]);
+      }
+      if (a.kimg) {
+        // B rows of this column for k = 2m, 2m + 1: Cx (q0, q1), Cy (q2, q3),
+        // Dx (q7, -q6), Dy (-q5, q4) with q4..q7 = m q0..q3 (see kf_term)
+        float *hi = a.kimg + (size_t)(col / KTC_COLS) * 2 * KTC_TILE_FLOATS, *lo = hi + KTC_TILE_FLOATS;
+        const int rb = 4 * (col % KTC_COLS);
+        const float v[4][2] = {{(float)c4[0], (float)c4[1]},
+                               {(float)c4[2], (float)c4[3]},
+                               {(float)(m * c4[3]), -(float)(m * c4[2])},
+                               {-(float)(m * c4[1]), (float)(m * c4[0])}};
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          const int o2 = ktc_off(rb + r, 2 * m) / 4;
+          const float h0 = to_tf32(v[r][0]), h1 = to_tf32(v[r][1]);
+          *reinterpret_cast<float2 *>(hi + o2) = make_float2(h0, h1);
+          *reinterpret_cast<float2 *>(lo + o2) = make_float2(to_tf32(v[r][0] - h0), to_tf32(v[r][1] - h1));
+        }
       }
     }
   }
@@ -807,7 +822,9 @@ __global__ void __launch_bounds__(512, sizeof(real) == 4 ? CVR_KF_MINB : 1) k_kf
       zy[m] = z.y;
     }
   }
-  const int c0 = (int)(((long)w * a.nxy) / W), c1 = (int)(((long)(w + 1) * a.nxy) / W);
+  // the summed columns only: a column taken from its mirror adds the same
+  // force, which k_sk_reduce has folded into the summed column's coefficients
+  const int c0 = (int)(((long)w * a.ncomp) / W), c1 = (int)(((long)(w + 1) * a.ncomp) / W);
   real fx = 0, fy = 0, fz = 0;
   for (int cb = c0; cb < c1; cb += TC) {
     const int nt = min(TC, c1 - cb);
@@ -826,7 +843,7 @@ __global__ void __launch_bounds__(512, sizeof(real) == 4 ? CVR_KF_MINB : 1) k_kf
         for (int u = 0; u < SB; ++u)
           if (v0 + u * 32 < nv) dst[v0 + u * 32] = r[u];
       }
-      for (int c = lane; c < nt; c += 32) xyw[c] = a.xy[cb + c];
+      for (int c = lane; c < nt; c += 32) xyw[c] = a.xyc[cb + c];
     }
     __syncwarp();
     for (int c = 0; c < nt; ++c) {

@@ -208,8 +208,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(KTC_THREADS, 1)
       }
     } else {
       float4 *xy = reinterpret_cast<float4 *>(sm + KTC_OFF_XY);
-      for (int c = t - 3 * KTC_ATOMS; c < a.nxy; c += KTC_ATOMS) {
-        const int2 nn = a.xy[c];
+      for (int c = t - 3 * KTC_ATOMS; c < a.ncomp; c += KTC_ATOMS) {  // the summed columns
+        const int2 nn = a.xyc[c];
         const int ox = (KTC_KPMAX - 1 + nn.x) * KTC_ATOMS * 8, oy = (KTC_PROWS + KTC_KPMAX - 1 + nn.y) * KTC_ATOMS * 8;
         xy[c] = make_float4(__int_as_float(ox), __int_as_float(oy), (float)nn.x, (float)nn.y);
       }
@@ -280,13 +280,13 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(KTC_THREADS, 1)
           tmem + (uint32_t)((jj & 1) * KTC_N + 4 * KTC_QCOLS * qtr) + ((uint32_t)(32 * (warp & 3)) << 16);
       const int c0 = (int)(rank + 2 * jj) * KTC_COLS + KTC_QCOLS * qtr;
       for (int q = 0; q < KTC_QCOLS / 8; ++q) {
-        if (c0 + 8 * q >= a.nxy) break;
+        if (c0 + 8 * q >= a.ncomp) break;
         uint32_t r[32];
         ktc_ld32(tb + 32 * q, r);
 #pragma unroll
         for (int u = 0; u < 8; ++u) {
           const int c = c0 + 8 * q + u;
-          if (c < a.nxy) {
+          if (c < a.ncomp) {
             const float4 ci = xy[c];
             const float2 X = *reinterpret_cast<const float2 *>(tab_al + __float_as_int(ci.x));
             const float2 Y = *reinterpret_cast<const float2 *>(tab_al + __float_as_int(ci.y));
