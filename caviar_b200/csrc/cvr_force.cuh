@@ -147,16 +147,21 @@ __device__ __forceinline__ void pair_term(PairAcc<real> &A, real dx, real dy, re
   const real r2 = dx * dx + dy * dy + dz * dz;
   real c = 0, vir_lj = 0;
   if (LJ) {
-    // lj.cpp:417-448: skip r^2 > rc^2 (rc2 < 0 when eps = 0)
-    const real r2l = JUMP ? (r2 < pc.jump2 ? pc.jump2 : r2) : r2;
-    const real r2i = fast_rcp(r2l);
-    const real s2 = pc.sig2 * r2i;
-    const real s6 = s2 * s2 * s2;
+    // lj.cpp:417-448: skip r^2 > rc^2 (rc2 < 0 when eps = 0).  With Ewald
+    // real space the list reaches its cutoff, far beyond the LJ one, and few
+    // pairs are inside: the LJ term is then branched around (the same values)
+    // instead of computed for every pair and selected.
     const bool in = (r2 <= pc.rc2) && !(same_mol && ignore_intra);
-    const real cl = r2i * s6 * (pc.eps24 - pc.eps48 * s6) + pc.K;
-    c = in ? cl : (real)0;
-    if (EV && in) A.g_lj += pc.e4 * (s6 * s6 - s6) + pc.C1 * r2l + pc.C0;
-    if (EV && JUMP) vir_lj = c * r2l;
+    if (!EWR || in) {
+      const real r2l = JUMP ? (r2 < pc.jump2 ? pc.jump2 : r2) : r2;
+      const real r2i = fast_rcp(r2l);
+      const real s2 = pc.sig2 * r2i;
+      const real s6 = s2 * s2 * s2;
+      const real cl = r2i * s6 * (pc.eps24 - pc.eps48 * s6) + pc.K;
+      c = in ? cl : (real)0;
+      if (EV && in) A.g_lj += pc.e4 * (s6 * s6 - s6) + pc.C1 * r2l + pc.C0;
+      if (EV && JUMP) vir_lj = c * r2l;
+    }
   }
   const real c_lj = c;
   if (EWR) {
