@@ -30,7 +30,9 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -49,9 +51,15 @@ constexpr int CH = 64;   // atoms per phase-table stage of S(k)
 constexpr int GMAX = 4;  // atom groups per k-run in S(k)
 constexpr int NTH = 8;   // per-replica results: ke, e_lj, e_ewr, e_k, e_self, virial, temperature, steps
 
+// skip: every k of the run has its mirror -k at a smaller index (in a run
+// that is summed); S(k) = conj(S(-k)) is then filled from it and the mirror's
+// force term, equal to this run's, counts twice.
 struct KRunB {
-  int nx, ny, nz0, len, k0;
+  int nx, ny, nz0, len, k0, skip;
 };
+
+constexpr int KFILL_MASK = (1 << 30) - 1;
+constexpr int KTWICE = 1 << 30;
 
 struct BatchDev {
   const int *order;
@@ -63,6 +71,9 @@ struct BatchDev {
   const int *type;
   const int4 *kint;
   const KRunB *runs;
+  // per k: bits 0-29 = 1 + the mirror's index when k's run is skipped (S(k)
+  // filled from it), bit 30 = k's force term counts twice (its mirror is skipped)
+  const int *kinfo;
   double *out;  // [replica][NTH]
   int nk, nruns, kmax, n_types;
   float eps[TMAX * TMAX], sig[TMAX * TMAX], charge[TMAX];
@@ -344,6 +355,7 @@ __device__ void batch_forces(const BatchDev &p, const Smem &S, int r, int n, int
     for (int it = threadIdx.x; it < items; it += TPB) {
       const int ri = it % p.nruns, g = it / p.nruns;
       const KRunB run = p.runs[ri];
+      if (run.skip) continue;
       float2 acc[RUNMAX];
 #pragma unroll
       for (int u = 0; u < RUNMAX; ++u) acc[u] = make_float2(0.f, 0.f);
@@ -370,6 +382,7 @@ __device__ void batch_forces(const BatchDev &p, const Smem &S, int r, int n, int
     }
     __syncthreads();
     for (int k = threadIdx.x; k < nk; k += TPB) {
+      if (p.kinfo[k] & KFILL_MASK) continue;  // filled from its mirror below
       double2 a = S.skd[k];
       for (int g = 0; g < G; ++g) {
         const float2 v = S.skp[(size_t)g * nk + k];
@@ -380,11 +393,19 @@ __device__ void batch_forces(const BatchDev &p, const Smem &S, int r, int n, int
     }
   }
   __syncthreads();
+  for (int k = threadIdx.x; k < nk; k += TPB) {  // S(k) = conj(S(-k)) of the skipped runs
+    const int f = p.kinfo[k] & KFILL_MASK;
+    if (f) {
+      const double2 v = S.skd[f - 1];
+      S.skd[k] = make_double2(v.x, -v.y);
+    }
+  }
+  __syncthreads();
   const double Vd = L * L * L;
   for (int k = threadIdx.x; k < nk; k += TPB) {
     const double2 sk = S.skd[k];
     const double fkk = (double)S.fk[k];
-    const double cf = 12.56637061435917295384 / Vd * fkk;
+    const double cf = 12.56637061435917295384 / Vd * fkk * ((p.kinfo[k] & KTWICE) ? 2.0 : 1.0);
     S.ak[k] = make_float2((float)(cf * sk.x), (float)(-cf * sk.y));
     if (EV) ev[2] += 6.28318530717958647692 / Vd * p.k_e * fkk * (sk.x * sk.x + sk.y * sk.y);
   }
@@ -404,6 +425,7 @@ __device__ void batch_forces(const BatchDev &p, const Smem &S, int r, int n, int
     float fx = 0, fy = 0, fz = 0;
     for (int rr = 0; rr < p.nruns; ++rr) {
       const KRunB run = p.runs[rr];
+      if (run.skip) continue;  // counted twice in its mirror's coefficients
       float2 px = tx[0], py = ty[0], pz = tz[0];
 #pragma unroll
       for (int mm = 0; mm < KP; ++mm) {
@@ -794,18 +816,45 @@ int cvr_batch_set_forces(cvr_batch *b, const double *eps, const double *sigma, c
         if (!runs.empty() && runs.back().nx == a && runs.back().ny == c && runs.back().nz0 + runs.back().len == z)
           runs.back().len++;
         else
-          runs.push_back({a, c, z, 1, k});
+          runs.push_back({a, c, z, 1, k, 0});
       }
   b->dev.nk = (int)kint.size();
   b->dev.nruns = (int)runs.size();
+  // For real charges S(-k) = conj(S(k)) and k, -k give the same force term:
+  // a run whose every k has its mirror at a smaller index is skipped (that
+  // mirror's run is always summed), its S(k) filled by conjugation and its
+  // force counted twice through the mirror's coefficient.
+  std::vector<int> kinfo(kint.size(), 0);
+  {
+    std::map<std::tuple<int, int, int>, int> kidx;
+    for (int k = 0; k < (int)kint.size(); ++k) kidx[std::make_tuple(kint[k].x, kint[k].y, kint[k].z)] = k;
+    std::vector<int> mir(kint.size(), -1);
+    for (int k = 0; k < (int)kint.size(); ++k) {
+      const auto it = kidx.find(std::make_tuple(-kint[k].x, -kint[k].y, -kint[k].z));
+      if (it != kidx.end()) mir[k] = it->second;
+    }
+    for (KRunB &r : runs) {
+      r.skip = 1;
+      for (int u = 0; u < r.len; ++u) r.skip = r.skip && mir[r.k0 + u] >= 0 && mir[r.k0 + u] < r.k0 + u;
+      if (r.skip)
+        for (int u = 0; u < r.len; ++u) {
+          kinfo[r.k0 + u] = mir[r.k0 + u] + 1;
+          kinfo[mir[r.k0 + u]] |= KTWICE;
+        }
+    }
+  }
   int4 *dk;
   KRunB *dr;
+  int *dki;
   if (int rc = balloc(b, &dk, kint.size())) return rc;
   if (int rc = balloc(b, &dr, runs.size())) return rc;
+  if (int rc = balloc(b, &dki, kinfo.size())) return rc;
   cudaMemcpy(dk, kint.data(), kint.size() * sizeof(int4), cudaMemcpyHostToDevice);
   cudaMemcpy(dr, runs.data(), runs.size() * sizeof(KRunB), cudaMemcpyHostToDevice);
+  cudaMemcpy(dki, kinfo.data(), kinfo.size() * sizeof(int), cudaMemcpyHostToDevice);
   b->dev.kint = dk;
   b->dev.runs = dr;
+  b->dev.kinfo = dki;
   for (const Shape &s : kShapes) {
     const int sm = (int)smem_bytes(b->dev.nk, NMAX, groups_for(s.tpb, b->dev.nruns));
     if (cudaFuncSetAttribute(s.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, sm) != cudaSuccess ||
