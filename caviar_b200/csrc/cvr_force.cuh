@@ -613,8 +613,9 @@ __global__ void __launch_bounds__(128) k_sk_partial(DevState<real> s, KArgs<real
   }
 }
 
-// S(k) = sum of the chunk partials (RW warps: warp w adds chunks w, w + RW,
-// ... in order, four loads in flight; then warp 0 adds the RW sums in warp
+// S(k) = sum of the chunk partials (warps 1 .. RW-1: warp w adds chunks
+// w - 1, w - 1 + (RW - 1), ... in order, four loads in flight, while warp 0
+// fetches the k indices and f_k; then warp 0 adds the RW - 1 sums in warp
 // order: a fixed order, deterministic), one lane per (column, m) pair.
 // A column taken from its mirror reads the mirror's sums and conjugates
 // them with +m and -m swapped (exact).
@@ -633,19 +634,42 @@ __global__ void __launch_bounds__(RW * 32) k_sk_reduce(DevState<real> s, KArgs<r
   const int src = (p < np) ? a.ksrc[pcol] : 0;
   const int pc = pm * a.ncomp + (src & ((1 << 30) - 1));  // its summed (m, column)
   double v[4] = {0.0, 0.0, 0.0, 0.0};
-  if (p < np) {
-    for (int c0 = w; c0 < a.nchunks; c0 += 4 * RW) {
+  // warp 0 fetches the lane's k indices, its mirror's and their f_k while
+  // warps 1 .. RW-1 sum the chunks (the two latency chains overlap)
+  int2 kk = make_int2(-1, -1), mk = make_int2(-1, -1);
+  double fe[2] = {0.0, 0.0}, fc[2] = {0.0, 0.0};  // f_k of (+-m); coefficient f_k x weight
+  if (w == 0 && p < np) {
+    kk = a.kpm[p];
+    if (!(src >> 30)) {
+      const int mir = a.kmir[src];
+      if (mir >= 0) mk = a.kpm[(size_t)pm * a.nxy + mir];
+    }
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      // k and its mirror -k (in the column taken from this one) give the same
+      // force term: the coefficient of (column, +-m) counts whichever of the two are in the set
+      const int k = h ? kk.y : kk.x, km = h ? mk.x : mk.y;
+      const int kf = (k >= 0) ? k : km;
+      if (kf >= 0) {
+        const double f = a.fk[kf];
+        if (k >= 0) fe[h] = f;
+        fc[h] = f * ((k >= 0 ? 1.0 : 0.0) + (km >= 0 ? 1.0 : 0.0));
+      }
+    }
+  }
+  if (p < np && w > 0) {
+    for (int c0 = w - 1; c0 < a.nchunks; c0 += 4 * (RW - 1)) {
       double2 u[4][2];
 #pragma unroll
       for (int h = 0; h < 4; ++h) {
-        const int c = c0 + h * RW;
+        const int c = c0 + h * (RW - 1);
         const size_t idx = (size_t)min(c, a.nchunks - 1) * npc + pc;
         u[h][0] = a.partial[2 * idx];
         u[h][1] = a.partial[2 * idx + 1];
       }
 #pragma unroll
       for (int h = 0; h < 4; ++h) {
-        if (c0 + h * RW < a.nchunks) {
+        if (c0 + h * (RW - 1) < a.nchunks) {
           v[0] += u[h][0].x;
           v[1] += u[h][0].y;
           v[2] += u[h][1].x;
@@ -670,34 +694,23 @@ __global__ void __launch_bounds__(RW * 32) k_sk_reduce(DevState<real> s, KArgs<r
       S[2] = t0;
       S[3] = -t1;
     }
-    const int2 kk = a.kpm[p];
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
       const int k = h ? kk.y : kk.x;
       if (k >= 0) {
         const double sr = S[2 * h], si = S[2 * h + 1];
         a.sk[k] = make_double2(sr, si);
-        e += a.fk[k] * (sr * sr + si * si);
+        e += fe[h] * (sr * sr + si * si);
       }
     }
-    if (!(src >> 30)) {
-      // force coefficients of a summed column: k and its mirror -k (in the
-      // column taken from this one) give the same force term, so the
-      // coefficient of (column, +-m) counts whichever of the two are in the set
+    if (!(src >> 30)) {  // force coefficients of a summed column
       const int m = pm, col = src;  // col: the summed column's index
-      const int mir = a.kmir[col];
-      const int2 mk = (mir >= 0) ? a.kpm[(size_t)m * a.nxy + mir] : make_int2(-1, -1);
       double A[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
-        const int k = h ? kk.y : kk.x, km = h ? mk.x : mk.y;  // (column, +-m) and the mirror's (-+m)
-        const int kf = (k >= 0) ? k : km;
-        if (kf >= 0) {
-          const double wgt = (k >= 0 ? 1.0 : 0.0) + (km >= 0 ? 1.0 : 0.0);
-          const double cf = a.four_pi_over_v * a.fk[kf] * wgt;
-          A[2 * h] = cf * S[2 * h];
-          A[2 * h + 1] = -cf * S[2 * h + 1];
-        }
+        const double cf = a.four_pi_over_v * fc[h];
+        A[2 * h] = cf * S[2 * h];
+        A[2 * h + 1] = -cf * S[2 * h + 1];
       }
       const double c4[4] = {A[0] + A[2], A[3] - A[1], A[1] + A[3], A[0] - A[2]};
       real *o = a.kcoef + ((size_t)col * a.M + m) * 8;
