@@ -187,7 +187,9 @@ struct cvr_ctx {
   // CUDA graphs of one step (plain, thermo); rebuilt when buffers move
   bool use_graphs = true;
   int64_t epoch = 0, graph_epoch = -1;
-  cudaGraphExec_t g_step[2] = {nullptr, nullptr};
+  // [deferred kick of the previous step in the head][tail: 0 kick deferred,
+  // 1 kick, 2 kick + thermo record]
+  cudaGraphExec_t g_step[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
   int64_t graph_kernels[2] = {0, 0};
   long long *counters{};
   long long counter_src[2] = {0, 0};
@@ -692,7 +694,7 @@ void launch_build(cvr_ctx *c, int count_only) {
 }
 
 template <typename real, int TPA, bool LJ, bool EWR, bool EV, bool ONE_TYPE, bool FIXED>
-void launch_pair_t(cvr_ctx *c) {
+void launch_pair_t(cvr_ctx *c, int book) {
   DevState<real> s = dev_state<real>(c);
   // fixed-point form: lengths in units of h = L / 2^32 (see upload_tables)
   const double h = FIXED ? c->L[0] / std::ldexp(1.0, 32) : 1.0;
@@ -703,34 +705,35 @@ void launch_pair_t(cvr_ctx *c) {
   ew.cut2 = (real)(c->ewr_cut >= 0 ? c->ewr_cut * c->ewr_cut / (h * h) : -1.0);
   const int blocks = grid_for(c->n * TPA, 128);
   k_pair<real, TPA, LJ, EWR, EV, ONE_TYPE, FIXED><<<blocks, 128, 0, c->stream>>>(
-      s, (const PairCoef<real> *)c->d_coef, (real)(1.0 / h), ew, c->ignore_intra, c->use_mol ? 1 : 0, c->ev_part);
+      s, (const PairCoef<real> *)c->d_coef, (real)(1.0 / h), ew, c->ignore_intra, c->use_mol ? 1 : 0, c->ev_part,
+      book, c->counters);
   c->launches++;
 }
 
 template <typename real, bool LJ, bool EWR, bool EV, bool FIXED>
-void launch_pair_tpa_f(cvr_ctx *c) {
+void launch_pair_tpa_f(cvr_ctx *c, int book) {
   // one type pair, no molecule tests, no jump_tol clamp: LJ constants in registers
   const bool one = LJ && !EWR && c->n_types == 1 && !c->use_mol && !(c->jump_tol > 0);
   switch (c->tpa) {
     case 1:
-      one ? launch_pair_t<real, 1, LJ, EWR, EV, true, FIXED>(c) : launch_pair_t<real, 1, LJ, EWR, EV, false, FIXED>(c);
+      one ? launch_pair_t<real, 1, LJ, EWR, EV, true, FIXED>(c, book) : launch_pair_t<real, 1, LJ, EWR, EV, false, FIXED>(c, book);
       break;
     case 8:
-      one ? launch_pair_t<real, 8, LJ, EWR, EV, true, FIXED>(c) : launch_pair_t<real, 8, LJ, EWR, EV, false, FIXED>(c);
+      one ? launch_pair_t<real, 8, LJ, EWR, EV, true, FIXED>(c, book) : launch_pair_t<real, 8, LJ, EWR, EV, false, FIXED>(c, book);
       break;
     default:
-      one ? launch_pair_t<real, 32, LJ, EWR, EV, true, FIXED>(c)
-          : launch_pair_t<real, 32, LJ, EWR, EV, false, FIXED>(c);
+      one ? launch_pair_t<real, 32, LJ, EWR, EV, true, FIXED>(c, book)
+          : launch_pair_t<real, 32, LJ, EWR, EV, false, FIXED>(c, book);
       break;
   }
 }
 
 template <typename real, bool LJ, bool EWR, bool EV>
-void launch_pair_tpa(cvr_ctx *c) {
+void launch_pair_tpa(cvr_ctx *c, int book) {
   if constexpr (sizeof(real) == 4) {
-    if (c->fixed) return launch_pair_tpa_f<real, LJ, EWR, EV, true>(c);
+    if (c->fixed) return launch_pair_tpa_f<real, LJ, EWR, EV, true>(c, book);
   }
-  launch_pair_tpa_f<real, LJ, EWR, EV, false>(c);
+  launch_pair_tpa_f<real, LJ, EWR, EV, false>(c, book);
 }
 
 // all_atom_test: every owned pair and every ghost image (k_pair_all), in
@@ -759,17 +762,20 @@ void launch_pair_all(cvr_ctx *c) {
     launch_pair_all_t<real, false, true, EV>(c);
 }
 
+// book: the pair kernel takes over the end-of-step bookkeeping of a step
+// whose kick is deferred (only where defer_kick allows it).
 template <typename real>
-void launch_pair(cvr_ctx *c, bool ev) {
+void launch_pair(cvr_ctx *c, bool ev, bool book = false) {
   Bracket br(c, CVR_KT_PAIR);
+  const int b = book ? 1 : 0;
   if (c->all_atom && (c->lj_on || c->ewr_on)) {
     ev ? launch_pair_all<real, true>(c) : launch_pair_all<real, false>(c);
   } else if (c->lj_on && c->ewr_on) {
-    ev ? launch_pair_tpa<real, true, true, true>(c) : launch_pair_tpa<real, true, true, false>(c);
+    ev ? launch_pair_tpa<real, true, true, true>(c, b) : launch_pair_tpa<real, true, true, false>(c, b);
   } else if (c->lj_on) {
-    ev ? launch_pair_tpa<real, true, false, true>(c) : launch_pair_tpa<real, true, false, false>(c);
+    ev ? launch_pair_tpa<real, true, false, true>(c, b) : launch_pair_tpa<real, true, false, false>(c, b);
   } else if (c->ewr_on) {
-    ev ? launch_pair_tpa<real, false, true, true>(c) : launch_pair_tpa<real, false, true, false>(c);
+    ev ? launch_pair_tpa<real, false, true, true>(c, b) : launch_pair_tpa<real, false, true, false>(c, b);
   } else {
     // no pair force field: accelerations start from zero
     const size_t rs = sizeof(real);
@@ -898,6 +904,17 @@ bool phase_in_drift(const cvr_ctx *c) { return c->ewk_on && c->nk > 0 && c->inte
 bool kick_in_kforce(const cvr_ctx *c, bool th) {
   return !th && c->ewk_on && c->nk > 0 && c->integrator == 0 && !c->tstat.kind && !c->sc_on &&
          !c->dipole_mode && !c->timing;
+}
+
+// Whether a plain velocity-Verlet step inside a run may defer its second
+// half kick to the next step's k_kick_drift (which applies it first, with
+// the same acceleration: the same operations, one pass over v and a less):
+// the pair kernel is the step's only force and takes over the kick's flag
+// reset and step count; the run's last step and every step with a thermo
+// record keep their kick.
+bool defer_kick(const cvr_ctx *c) {
+  return !(c->ewk_on && c->nk > 0) && (c->lj_on || c->ewr_on) && !c->all_atom && c->integrator == 0 &&
+         !c->tstat.kind && !c->sc_on && !(c->ewk_on && c->dipole_mode) && !c->timing;
 }
 
 template <typename real>
@@ -1038,7 +1055,7 @@ int launch_slab(cvr_ctx *c) {
 }
 
 template <typename real>
-int forces_now(cvr_ctx *c, bool ev, bool tables_fresh = false, double kick_h = 0.0) {
+int forces_now(cvr_ctx *c, bool ev, bool tables_fresh = false, double kick_h = 0.0, bool book = false) {
   if (c->ewk_on && c->nk > 0 && !c->timing) {
     // The S(k) chain reads only positions and charges and the pair kernel
     // writes only the accelerations and its energy partials, so the chain
@@ -1058,7 +1075,8 @@ int forces_now(cvr_ctx *c, bool ev, bool tables_fresh = false, double kick_h = 0
     launch_kforce<real>(c, s, a, kick_h);
     c->launches += 1;
   } else {
-    launch_pair<real>(c, ev);
+    // book is set only where defer_kick allows it (no k space)
+    launch_pair<real>(c, ev, book);
     if (int r = launch_kspace<real>(c)) return r;
   }
   if (c->sc_on)
@@ -1141,13 +1159,15 @@ LangevinArgs langevin_args(cvr_ctx *c) {
   return lg;
 }
 
+// deferred: the step's kick is left to the next step's k_kick_drift (only
+// where defer_kick allows it, never with a thermo record).
 template <typename real>
-int launch_step_tail(cvr_ctx *c, bool th) {
+int launch_step_tail(cvr_ctx *c, bool th, bool deferred = false) {
   DevState<real> s = dev_state<real>(c);
   const bool fused_kick = kick_in_kforce(c, th);
-  if (int r = forces_now<real>(c, th, phase_in_drift(c), fused_kick ? 0.5 * c->dt : 0.0)) return r;
+  if (int r = forces_now<real>(c, th, phase_in_drift(c), fused_kick ? 0.5 * c->dt : 0.0, deferred)) return r;
   const int nb = grid_for(c->n, 256);
-  if (!fused_kick) {
+  if (!fused_kick && !deferred) {
     Bracket br(c, CVR_KT_INTEGRATE);
     if (c->integrator == 1) {
       const LangevinArgs lg = langevin_args(c);
@@ -1185,15 +1205,19 @@ int launch_step_tail(cvr_ctx *c, bool th) {
   return CVR_OK;
 }
 
+// pending: the previous step deferred its second half kick to this kernel.
 template <typename real>
-void launch_kick_drift(cvr_ctx *c) {
+void launch_kick_drift(cvr_ctx *c, bool pending = false) {
   Bracket br(c, CVR_KT_INTEGRATE);
+  const double pre_h = pending ? 0.5 * c->dt : 0.0;
   if (c->integrator == 1)
     k_lgv_kick_drift<real><<<grid_for(c->n, 256), 256, 0, c->stream>>>(dev_state<real>(c), c->dt, langevin_args(c));
   else if (phase_in_drift(c))
-    k_kick_drift<real, true><<<grid_for(c->n, 256), 256, 0, c->stream>>>(dev_state<real>(c), c->dt, kargs<real>(c));
+    k_kick_drift<real, true>
+        <<<grid_for(c->n, 256), 256, 0, c->stream>>>(dev_state<real>(c), c->dt, kargs<real>(c), pre_h);
   else
-    k_kick_drift<real, false><<<grid_for(c->n, 256), 256, 0, c->stream>>>(dev_state<real>(c), c->dt, KArgs<real>{});
+    k_kick_drift<real, false>
+        <<<grid_for(c->n, 256), 256, 0, c->stream>>>(dev_state<real>(c), c->dt, KArgs<real>{}, pre_h);
   c->launches++;
 }
 
@@ -1218,16 +1242,19 @@ int stage_reference_eta(cvr_ctx *c, int slot) {
 }
 
 void destroy_graphs(cvr_ctx *c) {
-  for (auto &g : c->g_step)
-    if (g) {
-      cudaGraphExecDestroy(g);
-      g = nullptr;
-    }
+  for (auto &gh : c->g_step)
+    for (auto &g : gh)
+      if (g) {
+        cudaGraphExecDestroy(g);
+        g = nullptr;
+      }
   c->graph_epoch = -1;
 }
 
-// One CUDA graph per step kind (plain, thermo):
+// One CUDA graph per step kind (head: with or without the previous step's
+// deferred kick; tail: kick deferred, kick, kick + thermo record):
 //   [kick_drift, set condition] -> IF(rebuild flag) {list build} -> [forces, kick, thermo]
+// The deferred-kick kinds are made only where defer_kick allows them.
 // The build nodes sit in the body of a conditional node whose value a one-thread
 // kernel sets from the device flag, so a step without a rebuild launches none
 // of them.  Kernel parameters are baked in: the graphs are rebuilt whenever a
@@ -1236,13 +1263,16 @@ template <typename real>
 int build_graphs(cvr_ctx *c) {
   destroy_graphs(c);
   const int64_t launches0 = c->launches;
-  for (int th = 0; th < 2; ++th) {
+  const bool dk = defer_kick(c);
+  for (int kind = 0; kind < 6; ++kind) {
+    const int head = kind / 3, tail = kind % 3;
+    if ((head == 1 || tail == 0) && !dk) continue;
     cudaGraph_t g = nullptr, pre = nullptr, post = nullptr, body_out = nullptr;
     CVR_CUDA(c, cudaGraphCreate(&g, 0));
     cudaGraphConditionalHandle h;
     CVR_CUDA(c, cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
     CVR_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-    launch_kick_drift<real>(c);
+    launch_kick_drift<real>(c, head == 1);
     k_set_rebuild_condition<<<1, 1, 0, c->stream>>>(c->flags, h);
     CVR_CUDA(c, cudaStreamEndCapture(c->stream, &pre));
     cudaGraphNode_t n_pre, n_cond, n_post;
@@ -1258,11 +1288,11 @@ int build_graphs(cvr_ctx *c) {
     launch_build<real>(c, 0);
     CVR_CUDA(c, cudaStreamEndCapture(c->stream, &body_out));
     CVR_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-    const int r = launch_step_tail<real>(c, th != 0);
+    const int r = launch_step_tail<real>(c, tail == 2, tail == 0);
     CVR_CUDA(c, cudaStreamEndCapture(c->stream, &post));
     if (r) return r;
     CVR_CUDA(c, cudaGraphAddChildGraphNode(&n_post, g, &n_cond, 1, post));
-    CVR_CUDA(c, cudaGraphInstantiate(&c->g_step[th], g, cudaGraphInstantiateFlagUseNodePriority));
+    CVR_CUDA(c, cudaGraphInstantiate(&c->g_step[head][tail], g, cudaGraphInstantiateFlagUseNodePriority));
     cudaGraphDestroy(pre);
     cudaGraphDestroy(post);
     cudaGraphDestroy(g);
@@ -1328,33 +1358,40 @@ int run_impl(cvr_ctx *c, int64_t nsteps, int64_t every, double *thermo) {
         c->ndist[a] = nd0[a];
       }
     }
-    if (graphs && c->graph_epoch != c->epoch)
+    const bool dk = defer_kick(c);
+    if (graphs && (c->graph_epoch != c->epoch || (dk && !c->g_step[1][0])))
       if (int r = build_graphs<real>(c)) return r;
     const int64_t launches0 = c->launches;
+    bool pending = false;  // the previous step deferred its second half kick
+    int64_t n_kick = 0;    // steps ending with a plain (no thermo) kick
     for (int64_t k = 0; k < nsteps; ++k) {
       const bool th = every > 0 && ((k + 1) % every == 0);
+      const int tail = th ? 2 : ((dk && k + 1 < nsteps) ? 0 : 1);
+      n_kick += tail == 1;
       if (graphs) {
-        CVR_CUDA(c, cudaGraphLaunch(c->g_step[th ? 1 : 0], c->stream));
+        CVR_CUDA(c, cudaGraphLaunch(c->g_step[pending ? 1 : 0][tail], c->stream));
       } else {
         if (host_noise)
           if (int r = stage_reference_eta(c, (int)(k & 1))) return r;
-        launch_kick_drift<real>(c);
+        launch_kick_drift<real>(c, pending);
         launch_build<real>(c, 0);
-        if (int r = launch_step_tail<real>(c, th)) return r;
+        if (int r = launch_step_tail<real>(c, th, tail == 0)) return r;
       }
+      pending = tail == 0;
     }
     int f[4];
     if (int r = read_flags(c, f)) return r;
     collect_timing(c);
     if (graphs) {
       // kernel nodes executed: per step kick_drift + condition + forces +
-      // kick (fused into the k-space force on plain steps when possible) +
-      // thermo record; 8 per rebuild (9 when the build rewrites phase tables)
+      // kick (fused into the k-space force, or deferred to the next step's
+      // kick_drift, on plain steps when possible) + thermo record; 8 per
+      // rebuild (9 when the build rewrites phase tables)
       const int ks = (c->ewk_on && c->nk > 0) ? (phase_in_drift(c) ? 3 : 4) : 0;
       const int tail = (c->lj_on || c->ewr_on ? 1 : 0) + ks + ((c->tstat.kind && c->integrator == 0) ? 2 : 0) +
                        (c->sc_on ? 4 : 0) + ((c->ewk_on && c->dipole_mode) ? 3 : 0);
       const int kick_plain = kick_in_kforce(c, false) ? 0 : 1;
-      c->launches = launches0 + nsteps * (2 + tail) + (nsteps - nrec) * kick_plain + nrec * 2 +
+      c->launches = launches0 + nsteps * (2 + tail) + n_kick * kick_plain + nrec * 2 +
                     (8 + (phase_in_drift(c) ? 1 : 0)) * (int64_t)(f[3] - f0[3]);
     }
     if (f[1] & ERR_NAN) return fail(c, CVR_ERR_NAN, "NaN acceleration");

@@ -217,10 +217,18 @@ __device__ __forceinline__ void pair_disp(const real4 &xj, const real4 &xi, uint
 // FIXED: x4 holds fixed-point coordinates; coef_g and ew are in units of
 // L / 2^32 and fscale = 2^32 / L turns the summed force back into length
 // units (the virial and energies come out unscaled).  Otherwise fscale = 1.
+// book != 0 (a step whose second half kick is deferred to the next step's
+// k_kick_drift): block 0 takes over k_kick's end-of-step bookkeeping, the
+// rebuild flag reset and the step count.
 template <typename real, int TPA, bool LJ, bool EWR, bool EV, bool ONE_TYPE, bool FIXED>
 __global__ void __launch_bounds__(128, CVR_PAIR_MINB) k_pair(DevState<real> s, const PairCoef<real> *__restrict__ coef_g,
                                               real fscale, EwrArgs<real> ew,
-                                              int ignore_intra, int use_mol, double *__restrict__ partials) {
+                                              int ignore_intra, int use_mol, double *__restrict__ partials,
+                                              int book, long long *__restrict__ counters) {
+  if (book && blockIdx.x == 0 && threadIdx.x == 0) {
+    *s.flag = 0;
+    if (counters) counters[0]++;
+  }
   using real4 = typename V4<real>::t;
   __shared__ PairCoef<real> coef[ONE_TYPE ? 1 : MAX_TYPES * MAX_TYPES];
   const int T = s.n_types;
@@ -966,8 +974,12 @@ __device__ __forceinline__ bool update_local(DevState<real> &s, int i, const dou
 
 // PHASE: also the atom's S(k) phase tables at the new position (the values
 // k_phase writes), so the step's S(k) chain starts at the chunk partials.
+// pre_h != 0: the previous step's second half kick (v += pre_h a, deferred
+// from that step, as k_kick computes it) comes first; the two half kicks
+// use the same acceleration, so this is the kick + kick-drift sequence
+// operation for operation.
 template <typename real, bool PHASE>
-__global__ void __launch_bounds__(256) k_kick_drift(DevState<real> s, double dt, KArgs<real> ka) {
+__global__ void __launch_bounds__(256) k_kick_drift(DevState<real> s, double dt, KArgs<real> ka, double pre_h) {
   if (*s.err) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   bool need = false;
@@ -975,7 +987,13 @@ __global__ void __launch_bounds__(256) k_kick_drift(DevState<real> s, double dt,
     const double a0 = (double)s.ax[i], a1 = (double)s.ay[i], a2 = (double)s.az[i];
     if (isnan(a0) || isnan(a1) || isnan(a2)) atomicOr(s.err, ERR_NAN);  // md_simulator.cpp:584-590
     const double h = 0.5 * dt;
-    const double v0 = s.vx[i] + h * a0, v1 = s.vy[i] + h * a1, v2 = s.vz[i] + h * a2;
+    double u0 = s.vx[i], u1 = s.vy[i], u2 = s.vz[i];
+    if (pre_h != 0.0) {
+      u0 = u0 + pre_h * a0;
+      u1 = u1 + pre_h * a1;
+      u2 = u2 + pre_h * a2;
+    }
+    const double v0 = u0 + h * a0, v1 = u1 + h * a1, v2 = u2 + h * a2;
     const double p[3] = {s.x[i] + dt * v0, s.y[i] + dt * v1, s.z[i] + dt * v2};
     s.vx[i] = v0;
     s.vy[i] = v1;

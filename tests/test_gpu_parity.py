@@ -363,6 +363,31 @@ def test_graph_and_stream_paths_agree(cuda_lib):
     assert abs(th_a[-1, 1] - 0.5 * np.sum(v * v)) < 1e-10 * th_a[-1, 1]
 
 
+@pytest.mark.parametrize("prec", ["mixed", "fp64"])
+def test_deferred_kick_matches_separate_kicks(cuda_lib, prec):
+    """Inside one cvr_run a plain step (no thermo record, not the last) leaves
+    its second half kick to the next step's kick-drift kernel, which applies
+    it first with the same acceleration.  The trajectory must equal, bit for
+    bit, runs of one step each (whose step always ends with its own kick)."""
+    from caviar_b200 import workloads as W
+    s = W.fcc_lattice(8, 0.8442, 0.72, seed=11, jitter=0.05)
+    a = sim_for(cuda_lib, s, prec)
+    a.run(40)
+    b = sim_for(cuda_lib, s, prec)
+    for _ in range(40):
+        b.run(1)
+    for x, y in zip(a.state(), b.state()):
+        assert np.array_equal(x, y)
+    assert a.info()["builds"] == b.info()["builds"] > 1
+    # a run that ends on a thermo record, then one that does not: same state
+    c = sim_for(cuda_lib, s, prec)
+    th = c.run(30, 15)
+    c.run(10)
+    for x, y in zip(a.state(), c.state()):
+        assert np.array_equal(x, y)
+    assert th[:, 0].tolist() == [15, 30]
+
+
 def test_changed_dt_reaches_the_step_graphs(cuda_lib):
     """cvr_set_integrator between two runs: the graph path (which bakes dt
     and k_b into its kernels) must follow the new values exactly like the
