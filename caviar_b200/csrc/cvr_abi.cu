@@ -688,7 +688,7 @@ void launch_build(cvr_ctx *c, int count_only) {
   }
   c->launches += 8;
   if (phase_in_drift(c)) {  // the atoms moved in memory: the step's phase tables follow them
-    k_phase<real><<<grid_for(3 * c->n, 256), 256, 0, c->stream>>>(s, kargs<real>(c), s.flag);
+    k_phase<real><<<grid_for(3 * (int64_t)c->kp * c->n, 256), 256, 0, c->stream>>>(s, kargs<real>(c), s.flag);
     c->launches++;
   }
 }
@@ -883,7 +883,7 @@ void launch_sk(cvr_ctx *c, cudaStream_t st, bool tables_fresh = false) {
   DevState<real> s = dev_state<real>(c);
   KArgs<real> a = kargs<real>(c);
   if (!tables_fresh) {
-    k_phase<real><<<grid_for(3 * c->n, 256), 256, 0, st>>>(s, a, nullptr);
+    k_phase<real><<<grid_for(3 * (int64_t)c->kp * c->n, 256), 256, 0, st>>>(s, a, nullptr);
     c->launches++;
   }
   dim3 g1(grid_for(((c->kM + KMG - 1) / KMG) * c->ncomp, 128), c->nchunks);
@@ -1213,8 +1213,8 @@ void launch_kick_drift(cvr_ctx *c, bool pending = false) {
   if (c->integrator == 1)
     k_lgv_kick_drift<real><<<grid_for(c->n, 256), 256, 0, c->stream>>>(dev_state<real>(c), c->dt, langevin_args(c));
   else if (phase_in_drift(c))
-    k_kick_drift<real, true>
-        <<<grid_for(c->n, 256), 256, 0, c->stream>>>(dev_state<real>(c), c->dt, kargs<real>(c), pre_h);
+    k_kick_drift<real, true><<<grid_for((int64_t)c->n * KD_PHASE_SUB, 256), 256, 0, c->stream>>>(
+        dev_state<real>(c), c->dt, kargs<real>(c), pre_h);
   else
     k_kick_drift<real, false>
         <<<grid_for(c->n, 256), 256, 0, c->stream>>>(dev_state<real>(c), c->dt, KArgs<real>{}, pre_h);

@@ -521,11 +521,13 @@ template <typename real>
 __global__ void __launch_bounds__(256) k_phase(DevState<real> s, KArgs<real> a, const int *__restrict__ gate) {
   if (gate && *gate == 0) return;
   if (*s.err) return;
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= 3 * s.n) return;
-  const int d = t / s.n, i = t - d * s.n;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;  // one thread per table entry
+  if (t >= 3 * a.kp * s.n) return;
+  const int r = t / s.n, i = t - r * s.n;
+  const int d = r / a.kp, m = r - d * a.kp;
+  if (m > a.kmax[d]) return;
   const double x = ((d == 0) ? s.x[i] : ((d == 1) ? s.y[i] : s.z[i])) * a.inv_L[d];
-  for (int m = 0; m <= a.kmax[d]; ++m) a.ptab[(size_t)(d * a.kp + m) * s.n + i] = phase<real>(x, m);
+  a.ptab[(size_t)r * s.n + i] = phase<real>(x, m);
 }
 
 // S(k) partial sums (electrostatic_ewald_k/initialize.cpp:117-146): one thread per
@@ -972,6 +974,9 @@ __device__ __forceinline__ bool update_local(DevState<real> &s, int i, const dou
   return need;
 }
 
+#ifndef KD_PHASE_SUB
+#define KD_PHASE_SUB 8
+#endif
 // PHASE: also the atom's S(k) phase tables at the new position (the values
 // k_phase writes), so the step's S(k) chain starts at the chunk partials.
 // pre_h != 0: the previous step's second half kick (v += pre_h a, deferred
@@ -980,12 +985,16 @@ __device__ __forceinline__ bool update_local(DevState<real> &s, int i, const dou
 // operation for operation.
 template <typename real, bool PHASE>
 __global__ void __launch_bounds__(256) k_kick_drift(DevState<real> s, double dt, KArgs<real> ka, double pre_h) {
+  // PHASE: KD_PHASE_SUB neighbouring lanes per atom; each computes the
+  // atom's update (same loads, merged by the coalescer; same result), the
+  // first stores it, and the lanes split the 3 (kmax + 1) phase rows
+  constexpr int SUB = PHASE ? KD_PHASE_SUB : 1;
   if (*s.err) return;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = t / SUB, sub = t - i * SUB;
   bool need = false;
   if (i < s.n) {
     const double a0 = (double)s.ax[i], a1 = (double)s.ay[i], a2 = (double)s.az[i];
-    if (isnan(a0) || isnan(a1) || isnan(a2)) atomicOr(s.err, ERR_NAN);  // md_simulator.cpp:584-590
     const double h = 0.5 * dt;
     double u0 = s.vx[i], u1 = s.vy[i], u2 = s.vz[i];
     if (pre_h != 0.0) {
@@ -995,18 +1004,21 @@ __global__ void __launch_bounds__(256) k_kick_drift(DevState<real> s, double dt,
     }
     const double v0 = u0 + h * a0, v1 = u1 + h * a1, v2 = u2 + h * a2;
     const double p[3] = {s.x[i] + dt * v0, s.y[i] + dt * v1, s.z[i] + dt * v2};
-    s.vx[i] = v0;
-    s.vy[i] = v1;
-    s.vz[i] = v2;
-    s.x[i] = p[0];
-    s.y[i] = p[1];
-    s.z[i] = p[2];
-    need = update_local(s, i, p);
+    if (sub == 0) {
+      if (isnan(a0) || isnan(a1) || isnan(a2)) atomicOr(s.err, ERR_NAN);  // md_simulator.cpp:584-590
+      s.vx[i] = v0;
+      s.vy[i] = v1;
+      s.vz[i] = v2;
+      s.x[i] = p[0];
+      s.y[i] = p[1];
+      s.z[i] = p[2];
+      need = update_local(s, i, p);
+    }
     if constexpr (PHASE) {
-#pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        const double x = p[d] * ka.inv_L[d];
-        for (int m = 0; m <= ka.kmax[d]; ++m) ka.ptab[(size_t)(d * ka.kp + m) * s.n + i] = phase<real>(x, m);
+      for (int r = sub; r < 3 * ka.kp; r += SUB) {
+        const int d = r / ka.kp, m = r - d * ka.kp;
+        const double pd = (d == 0) ? p[0] : ((d == 1) ? p[1] : p[2]);  // static indices: p stays in registers
+        if (m <= ka.kmax[d]) ka.ptab[(size_t)r * s.n + i] = phase<real>(pd * ka.inv_L[d], m);
       }
     }
   }
