@@ -1101,18 +1101,29 @@ int forces_now(cvr_ctx *c, bool ev, bool tables_fresh = false, double kick_h = 0
   return CVR_OK;
 }
 
+int regrow(cvr_ctx *c);
+
+// List build and first forces before a run.  A state denser than the one the
+// list was sized for (a new state on a kept context) overflows it: the list
+// grows from the largest count seen and the build is redone.
 template <typename real>
 int setup_run(cvr_ctx *c) {
-  if (int r = do_build<real>(c, true)) return r;
-  CVR_CUDA(c, cudaMemsetAsync(c->flags, 0, sizeof(int), c->stream));
-  if (int r = forces_now<real>(c, false)) return r;
-  int f[4];
-  if (int r = read_flags(c, f)) return r;
-  if (f[1] & ERR_OVERFLOW) return fail(c, CVR_ERR_CAPACITY, "neighbour list overflow at setup");
-  if (f[1] & ERR_KSPACE_TC) return fail(c, CVR_ERR_CUDA, "tensor-core k-space force: a wait ran out");
-  c->list_valid = true;
-  c->setup_done = true;
-  return CVR_OK;
+  for (int attempt = 0; attempt < 4; ++attempt) {
+    if (int r = do_build<real>(c, true)) return r;
+    CVR_CUDA(c, cudaMemsetAsync(c->flags, 0, sizeof(int), c->stream));
+    if (int r = forces_now<real>(c, false)) return r;
+    int f[4];
+    if (int r = read_flags(c, f)) return r;
+    if (f[1] & ERR_OVERFLOW) {
+      if (int r = regrow(c)) return r;
+      continue;
+    }
+    if (f[1] & ERR_KSPACE_TC) return fail(c, CVR_ERR_CUDA, "tensor-core k-space force: a wait ran out");
+    c->list_valid = true;
+    c->setup_done = true;
+    return CVR_OK;
+  }
+  return fail(c, CVR_ERR_CAPACITY, "neighbour list overflow at setup");
 }
 
 // Grow the list after an overflow: capacity from the largest count seen.
@@ -1946,9 +1957,13 @@ int cvr_set_state(cvr_ctx *c, int64_t n, const double *pos, const double *vel, c
     // list interleave: TPA lanes per atom, or quads of four entries when one lane per atom
     c->log2_tpa = (c->tpa == 32) ? 5 : (c->tpa == 8 ? 3 : 2);
   }
-  // Types first: atoms per type on the GPU (the range check of every type,
-  // and the charge and mass sums at one term per type), read back before
-  // the positions and velocities are sent.
+  // The types first, then the atoms per type on the GPU (the range check of
+  // every type, and the charge and mass sums at one term per type), read
+  // back with the positions behind them: the staged arrays reach the state
+  // only after the check.  The velocities follow on the side stream: on a
+  // context whose cells, tables and graphs stay, their copy runs beside the
+  // run's setup (list build and first forces, which need no velocities),
+  // done here, and they reach the atoms' places by id at the end.
   CVR_CUDA(c, cudaMemcpyAsync(c->stage_i, type, (size_t)n * sizeof(int32_t), cudaMemcpyHostToDevice, c->stream));
   CVR_CUDA(c, cudaMemsetAsync(c->d_type_hist, 0, (MAX_TYPES + 1) * sizeof(unsigned long long), c->stream));
   k_type_hist<<<std::min<int64_t>(grid_for(n, 256), 4 * 148), 256, 0, c->stream>>>(c->stage_i, (int)n, c->n_types,
@@ -1956,12 +1971,19 @@ int cvr_set_state(cvr_ctx *c, int64_t n, const double *pos, const double *vel, c
   c->launches++;
   unsigned long long per_type[MAX_TYPES + 1];
   CVR_CUDA(c, cudaMemcpyAsync(per_type, c->d_type_hist, sizeof(per_type), cudaMemcpyDeviceToHost, c->stream));
-  CVR_CUDA(c, cudaStreamSynchronize(c->stream));
-  if (per_type[MAX_TYPES] != 0) return fail(c, CVR_ERR_INVALID, "atom type out of range");
   CVR_CUDA(c, cudaMemcpyAsync(c->stage, pos, (size_t)n * 3 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-  if (vel)
-    CVR_CUDA(c, cudaMemcpyAsync(c->stage + 3 * n, vel, (size_t)n * 3 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   if (mol) CVR_CUDA(c, cudaMemcpyAsync(c->stage_i + n, mol, (size_t)n * sizeof(int32_t), cudaMemcpyHostToDevice, c->stream));
+  CVR_CUDA(c, cudaEventRecord(c->k_fork, c->stream));  // after the positions: they take the link first
+  CVR_CUDA(c, cudaStreamWaitEvent(c->kstream, c->k_fork, 0));
+  if (vel)
+    CVR_CUDA(c, cudaMemcpyAsync(c->stage + 3 * n, vel, (size_t)n * 3 * sizeof(double), cudaMemcpyHostToDevice,
+                                c->kstream));
+  CVR_CUDA(c, cudaEventRecord(c->k_join, c->kstream));
+  CVR_CUDA(c, cudaStreamSynchronize(c->stream));
+  if (per_type[MAX_TYPES] != 0) {
+    cudaStreamSynchronize(c->kstream);  // the caller's velocity array is borrowed until the copy ends
+    return fail(c, CVR_ERR_INVALID, "atom type out of range");
+  }
   c->have_state = true;
   const bool mol_changed = (mol != nullptr) != c->use_mol;
   c->use_mol = mol != nullptr;
@@ -1977,30 +1999,42 @@ int cvr_set_state(cvr_ctx *c, int64_t n, const double *pos, const double *vel, c
   c->e_self = self_energy(c);
   if (c->precision == CVR_PREC_FP64) {
     DevState<double> s = dev_state<double>(c);
-    k_scatter_state<double><<<grid_for(n, 256), 256, 0, c->stream>>>(s, c->stage, vel ? c->stage + 3 * n : nullptr,
-                                                                      c->stage_i, mol ? c->stage_i + n : nullptr);
+    k_scatter_state<double><<<grid_for(n, 256), 256, 0, c->stream>>>(s, c->stage, nullptr, c->stage_i,
+                                                                      mol ? c->stage_i + n : nullptr);
   } else {
     DevState<float> s = dev_state<float>(c);
-    k_scatter_state<float><<<grid_for(n, 256), 256, 0, c->stream>>>(s, c->stage, vel ? c->stage + 3 * n : nullptr,
-                                                                    c->stage_i, mol ? c->stage_i + n : nullptr);
+    k_scatter_state<float><<<grid_for(n, 256), 256, 0, c->stream>>>(s, c->stage, nullptr, c->stage_i,
+                                                                    mol ? c->stage_i + n : nullptr);
   }
   c->launches++;
   CVR_CUDA(c, cudaMemsetAsync(c->flags, 0, 4 * sizeof(int), c->stream));
   c->step = 0;
+  int rs = CVR_OK;
   if (!c->refreshed || mol_changed) {
-    if (int r = refresh(c)) return r;
+    rs = refresh(c);
   } else {
     // same atom count and settings: cells, tables and buffers stay (and so
-    // do the step graphs); only the list and the forces are redone
+    // do the step graphs); the list and the forces are redone now, beside
+    // the velocity copy (what the next run's setup would do)
     c->list_valid = false;
     c->setup_done = false;
+    rs = DISPATCH(c, setup_run, c);
   }
   // the host arrays are borrowed for this call only: the copies from them
   // (asynchronous when they are pinned) end before it returns
-  cudaError_t e = cudaStreamSynchronize(c->stream);
+  cudaError_t e = cudaStreamWaitEvent(c->stream, c->k_join, 0);
+  if (vel && e == cudaSuccess) {
+    if (c->precision == CVR_PREC_FP64)
+      k_place_velocities<double><<<grid_for(n, 256), 256, 0, c->stream>>>(dev_state<double>(c), c->stage + 3 * n);
+    else
+      k_place_velocities<float><<<grid_for(n, 256), 256, 0, c->stream>>>(dev_state<float>(c), c->stage + 3 * n);
+    c->launches++;
+  }
+  const cudaError_t e2 = cudaStreamSynchronize(c->stream);
+  if (e == cudaSuccess) e = e2;
   if (e == cudaSuccess) e = cudaGetLastError();
   if (e != cudaSuccess) return fail(c, CVR_ERR_CUDA, cudaGetErrorString(e));
-  return CVR_OK;
+  return rs;
 }
 
 int cvr_build_neighbors(cvr_ctx *c, int force, int *rebuilt) {

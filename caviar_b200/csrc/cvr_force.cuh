@@ -1707,4 +1707,16 @@ __global__ void k_scatter_state(DevState<real> s, const double *__restrict__ pos
   s.az[i] = 0;
 }
 
+// Velocities in the caller's order (AoS) to the atoms' current places, by
+// id: the state may have been reordered since the positions were placed.
+template <typename real>
+__global__ void k_place_velocities(DevState<real> s, const double *__restrict__ vel) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= s.n) return;
+  const size_t k = 3 * (size_t)s.id[i];
+  s.vx[i] = vel[k];
+  s.vy[i] = vel[k + 1];
+  s.vz[i] = vel[k + 2];
+}
+
 }  // namespace cvr

@@ -196,6 +196,10 @@ int cvr_clear_thermostat(cvr_ctx *c);
 
 /* Atoms from HOST memory: pos, vel: n*3 (x,y,z per atom, = Vector<double> AoS);
  * type: n; mol: n molecule indices or NULL (-1 = none).  Atom i gets id i.
+ * The arrays are read before the call returns.  On a context that keeps its
+ * atom count and settings, the next run's setup (list build, first forces)
+ * runs inside this call, beside the velocity copy; a list overflow there is
+ * reported here.
  * Replaces: Atom_data::add_atom (atom_data.cpp:487-521) / add_xyz_data_file
  *           (atom_data/add_xyz_data_file.cpp:22-168). */
 int cvr_set_state(cvr_ctx *ctx, int64_t n, const double *pos, const double *vel, const int32_t *type,

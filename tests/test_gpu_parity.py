@@ -471,9 +471,10 @@ def test_all_atom_test_vs_reference(cuda_lib, prec):
 
 
 def test_type_out_of_range_rejected_and_state_kept(cuda_lib):
-    """cvr_set_state checks every type on the GPU (atoms per type) before it
-    sends the positions: a type outside [0, n_types) is CVR_ERR_INVALID and
-    the context keeps its previous state (a run continues from it)."""
+    """cvr_set_state checks every type on the GPU (atoms per type) before the
+    staged arrays reach the state: a type outside [0, n_types) is
+    CVR_ERR_INVALID and the context keeps its previous state (a run
+    continues from it)."""
     s, _ = load_ref_fixture("lj500")
     sim = sim_for(cuda_lib, s, "fp64")
     p0, v0, _ = sim.state()
