@@ -310,7 +310,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(KTC_THREADS, 1)
       atomicOr(s.err, ERR_KSPACE_TC);
     }
     ktc_fence_before();
-    bad = __syncthreads_or(bad);  // one verdict for the block
+    bad = __syncthreads_or(bad);  // one answer for the whole block
     if (warp == 0) {
       ktc_fence_after();
       asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(KTC_TMEM_COLS) : "memory");
