@@ -411,51 +411,85 @@ __global__ void __launch_bounds__(128) k_build_list_warp(DevState<real> s, int c
         }
       }
     }
+    // The live pieces, in stencil order, laid end to end: a per-warp table
+    // in shared memory of each piece's start in that sequence, first
+    // candidate, image offset and entry bits.  The warp then sweeps the
+    // sequence 32 candidates at a time, so a round spans piece boundaries
+    // instead of idling the lanes past the end of a short row.
     constexpr uint32_t kUnshifted = 1u | (1u << 2) | (1u << 4);
-    for (int k = 0; k < KP; ++k) {
-      // this round's pieces, selected with static indices (the arrays stay in registers)
-      int kst = pst[0], klen = plen[0];
-      uint32_t kcode = pcode[0];
+    constexpr int PMAX = 3 * (2 * MAX_STENCIL_R + 1) * (2 * MAX_STENCIL_R + 1);
+    __shared__ int s_off[4][PMAX + 1];
+    __shared__ float4 s_geo[4][PMAX];  // image offset bx, by, bz; first candidate (int bits)
+    __shared__ uint32_t s_pc[4][PMAX];
+    const int w = threadIdx.x >> 5;
+    int nlive = 0, total = 0;
 #pragma unroll
-      for (int t = 1; t < KP; ++t)
-        if (k == t) {
-          kst = pst[t];
-          klen = plen[t];
-          kcode = pcode[t];
-        }
-      unsigned todo = __ballot_sync(0xffffffffu, klen > 0);  // live pieces, in stencil order
-      while (todo) {
-        const int src = __ffs(todo) - 1;
-        todo &= todo - 1;
-        const int len = __shfl_sync(0xffffffffu, klen, src);
-        const int jb = __shfl_sync(0xffffffffu, kst, src);
-        const uint32_t pc = __shfl_sync(0xffffffffu, kcode, src);
-        const uint32_t code = pc & 63u;
-        const uint32_t ebase = pc & ~((1u << CODE_SHIFT) - 1u);
+    for (int k = 0; k < KP; ++k) {
+      const int len = plen[k];
+      int incl = len;  // inclusive scan of the lengths across the lanes
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+      }
+      const unsigned live = __ballot_sync(0xffffffffu, len > 0);
+      if (len > 0) {
+        const int q = nlive + __popc(live & lt);
+        const uint32_t code = pcode[k] & 63u;
         const int sx = (int)(code & 3u) - 1, sy = (int)((code >> 2) & 3u) - 1, sz = (int)(code >> 4) - 1;
-        const float bx = sx * s.box.Lf[0] - xi.x, by = sy * s.box.Lf[1] - xi.y, bz = sz * s.box.Lf[2] - xi.z;
+        s_off[w][q] = total + incl - len;
+        s_geo[w][q] = make_float4(sx * s.box.Lf[0] - xi.x, sy * s.box.Lf[1] - xi.y, sz * s.box.Lf[2] - xi.z,
+                                  __int_as_float(pst[k]));
+        s_pc[w][q] = pcode[k];
+      }
+      nlive += __popc(live);
+      total += __shfl_sync(0xffffffffu, incl, 31);
+    }
+    if (lane == 0) s_off[w][nlive] = total;
+    __syncwarp();
+    int q0 = 0;  // the live piece that holds candidate `base`
+    for (int base = 0; base < total; base += 32) {
+      // pieces that start inside this round (after its first candidate)
+      const int qt = q0 + 1 + lane;
+      unsigned bit = 0u;
+      if (qt < nlive) {
+        const int o = s_off[w][qt];
+        if (o < base + 32) bit = 1u << (o - base);
+      }
+      const unsigned starts = __reduce_or_sync(0xffffffffu, bit);
+      const int c = base + lane;
+      bool ok = false;
+      int j = 0;
+      float4 q = xi;
+      uint32_t pc = 0;
+      if (c < total) {
+        const int qp = q0 + __popc(starts & ((2u << lane) - 1u));  // this lane's piece
+        const float4 g = s_geo[w][qp];
+        pc = s_pc[w][qp];
+        j = __float_as_int(g.w) + (c - s_off[w][qp]);
+        const uint32_t code = pc & 63u;
         const bool shifted = code != kUnshifted;
-        const bool fast_ok = !shifted || s.regular_images;
-        const int self = shifted ? -1 : i;
-        for (int base = 0; base < len; base += 32) {
-          const int j = jb + base + lane;
-          bool ok = false;
-          float4 q = xi;
-          if (base + lane < len && j != self) {
-            q = s.xb[j];
-            const float ex = q.x + bx, ey = q.y + by, ez = q.z + bz;
-            const float d2 = ex * ex + ey * ey + ez * ez;
-            if (d2 < s.rl_sq_hi) ok = (d2 <= s.rl_sq_lo && fast_ok) || in_list_slow(s, pi, gi, j, d2, sx, sy, sz);
+        if (!shifted ? j != i : true) {
+          q = s.xb[j];
+          const float ex = q.x + g.x, ey = q.y + g.y, ez = q.z + g.z;
+          const float d2 = ex * ex + ey * ey + ez * ez;
+          if (d2 < s.rl_sq_hi) {
+            const bool fast_ok = !shifted || s.regular_images;
+            ok = (d2 <= s.rl_sq_lo && fast_ok) ||
+                 in_list_slow(s, pi, gi, j, d2, (int)(code & 3u) - 1, (int)((code >> 2) & 3u) - 1, (int)(code >> 4) - 1);
           }
-          const unsigned m = __ballot_sync(0xffffffffu, ok);
-          if (ok && !count_only) {
-            const int k2 = cnt + __popc(m & lt);
-            if (k2 < s.cap)
-              row[list_slot(k2, log2_tpa, stride)] = (uint32_t)j | (ebase + ((uint32_t)__float_as_int(q.w) << CODE_SHIFT));
-          }
-          cnt += __popc(m);
         }
       }
+      const unsigned m = __ballot_sync(0xffffffffu, ok);
+      if (ok && !count_only) {
+        const int k2 = cnt + __popc(m & lt);
+        const uint32_t ebase = pc & ~((1u << CODE_SHIFT) - 1u);
+        if (k2 < s.cap)
+          row[list_slot(k2, log2_tpa, stride)] = (uint32_t)j | (ebase + ((uint32_t)__float_as_int(q.w) << CODE_SHIFT));
+      }
+      cnt += __popc(m);
+      q0 += __popc(starts);  // the piece that holds candidate base + 32
+      if (q0 + 1 < nlive && s_off[w][q0 + 1] <= base + 32) ++q0;
     }
   } else
   for (int dz = -R; dz <= R; ++dz) {

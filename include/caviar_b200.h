@@ -154,7 +154,7 @@ int cvr_set_langevin(cvr_ctx *c, double temperature, double friction, double kb,
 /* Verlet-list search kernel (a tuning and testing knob; both kernels build
  * the same pair set, Neighborlist::update_verlet_list_from_cell_list,
  * neighborlist.cpp:515-573): CVR_LIST_AUTO picks by system size (a warp per
- * atom up to 131072 atoms, else a thread per atom), CVR_LIST_THREAD one
+ * atom up to 65536 atoms, else a thread per atom), CVR_LIST_THREAD one
  * thread per atom, CVR_LIST_WARP one warp per atom.  Takes effect at the
  * next list build. */
 /* k-space force kernel of the mixed form (a tuning and testing knob; both
