@@ -318,9 +318,11 @@ __device__ __forceinline__ size_t list_slot(int cnt, int log2_tpa, size_t stride
 // The same search with one WARP per atom, for systems too small to fill the
 // GPU with one thread per atom: the 32 lanes take consecutive candidates of a
 // stencil cell, and a ballot keeps the accepted ones in candidate order, so
-// the list is identical to the one-thread-per-atom build.
+// the list is identical to the one-thread-per-atom build.  Launched with 128
+// threads (four warps: the per-warp piece tables); a register cap rather than
+// launch bounds keeps the sweep free of spills.
 template <typename real>
-__global__ void __launch_bounds__(128) k_build_list_warp(DevState<real> s, int count_only, int log2_tpa) {
+__global__ void __maxnreg__(80) k_build_list_warp(DevState<real> s, int count_only, int log2_tpa) {
   if (*s.flag == 0) return;
   if (blockIdx.x == 0 && threadIdx.x == 0 && !count_only) atomicAdd(s.n_builds, 1);
   const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
