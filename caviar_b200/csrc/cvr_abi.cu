@@ -689,7 +689,7 @@ void launch_build(cvr_ctx *c, int count_only) {
   }
   c->launches += 8;
   if (phase_in_drift(c)) {  // the atoms moved in memory: the step's phase tables follow them
-    k_phase<real><<<grid_for(3 * (int64_t)c->kp * c->n, 256), 256, 0, c->stream>>>(s, kargs<real>(c), s.flag);
+    k_phase<real><<<grid_for(3 * (int64_t)c->n, 256), 256, 0, c->stream>>>(s, kargs<real>(c), s.flag);
     c->launches++;
   }
 }
@@ -884,7 +884,7 @@ void launch_sk(cvr_ctx *c, cudaStream_t st, bool tables_fresh = false) {
   DevState<real> s = dev_state<real>(c);
   KArgs<real> a = kargs<real>(c);
   if (!tables_fresh) {
-    k_phase<real><<<grid_for(3 * (int64_t)c->kp * c->n, 256), 256, 0, st>>>(s, a, nullptr);
+    k_phase<real><<<grid_for(3 * (int64_t)c->n, 256), 256, 0, st>>>(s, a, nullptr);
     c->launches++;
   }
   dim3 g1(grid_for(((c->kM + KMG - 1) / KMG) * c->ncomp, 128), c->nchunks);

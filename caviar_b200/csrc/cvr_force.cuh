@@ -511,6 +511,24 @@ __device__ __forceinline__ T conj_if(T a, bool c) {
   return a;
 }
 
+// One atom's phase-table row of one axis: e^{i 2 pi m x / L}, m = 0..kmax,
+// into ptab[(row0 + m) * n + i].  Every fourth m is evaluated directly
+// (phase), the others as the previous value times the m = 1 phase, so each
+// entry is at most three complex products away from a direct value.
+template <typename real>
+__device__ __forceinline__ void phase_row(typename R2<real>::t *__restrict__ ptab, size_t n, int i, int row0,
+                                          double x_over_L, int kmax) {
+  using c2 = typename R2<real>::t;
+  const c2 e1 = phase<real>(x_over_L, 1);
+  c2 z;
+  z.x = (real)1;
+  z.y = (real)0;
+  for (int m = 0; m <= kmax; ++m) {
+    if (m > 0) z = (m & 3) ? cmul(z, e1) : phase<real>(x_over_L, m);
+    ptab[(size_t)(row0 + m) * n + i] = z;
+  }
+}
+
 // Phase tables of every atom, once per force evaluation:
 // ptab[(d * kp + m) * n + i] = e^{i 2 pi m x_d / L_d}, m = 0..kmax_d
 // (row-major by (d, m), so 32 consecutive atoms are 32 consecutive words).
@@ -521,13 +539,11 @@ template <typename real>
 __global__ void __launch_bounds__(256) k_phase(DevState<real> s, KArgs<real> a, const int *__restrict__ gate) {
   if (gate && *gate == 0) return;
   if (*s.err) return;
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;  // one thread per table entry
-  if (t >= 3 * a.kp * s.n) return;
-  const int r = t / s.n, i = t - r * s.n;
-  const int d = r / a.kp, m = r - d * a.kp;
-  if (m > a.kmax[d]) return;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;  // one thread per (axis, atom)
+  if (t >= 3 * s.n) return;
+  const int d = t / s.n, i = t - d * s.n;
   const double x = ((d == 0) ? s.x[i] : ((d == 1) ? s.y[i] : s.z[i])) * a.inv_L[d];
-  a.ptab[(size_t)r * s.n + i] = phase<real>(x, m);
+  phase_row<real>(a.ptab, s.n, i, d * a.kp, x, a.kmax[d]);
 }
 
 // S(k) partial sums (electrostatic_ewald_k/initialize.cpp:117-146): one thread per
@@ -975,7 +991,7 @@ __device__ __forceinline__ bool update_local(DevState<real> &s, int i, const dou
 }
 
 #ifndef KD_PHASE_SUB
-#define KD_PHASE_SUB 8
+#define KD_PHASE_SUB 4
 #endif
 // PHASE: also the atom's S(k) phase tables at the new position (the values
 // k_phase writes), so the step's S(k) chain starts at the chunk partials.
@@ -987,8 +1003,9 @@ template <typename real, bool PHASE>
 __global__ void __launch_bounds__(256) k_kick_drift(DevState<real> s, double dt, KArgs<real> ka, double pre_h) {
   // PHASE: KD_PHASE_SUB neighbouring lanes per atom; each computes the
   // atom's update (same loads, merged by the coalescer; same result), the
-  // first stores it, and the lanes split the 3 (kmax + 1) phase rows
+  // first stores it, and the first three write one axis's phase row each
   constexpr int SUB = PHASE ? KD_PHASE_SUB : 1;
+  static_assert(SUB >= 3 || !PHASE, "one lane per axis for the phase rows");
   if (*s.err) return;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int i = t / SUB, sub = t - i * SUB;
@@ -1015,10 +1032,9 @@ __global__ void __launch_bounds__(256) k_kick_drift(DevState<real> s, double dt,
       need = update_local(s, i, p);
     }
     if constexpr (PHASE) {
-      for (int r = sub; r < 3 * ka.kp; r += SUB) {
-        const int d = r / ka.kp, m = r - d * ka.kp;
-        const double pd = (d == 0) ? p[0] : ((d == 1) ? p[1] : p[2]);  // static indices: p stays in registers
-        if (m <= ka.kmax[d]) ka.ptab[(size_t)r * s.n + i] = phase<real>(pd * ka.inv_L[d], m);
+      if (sub < 3) {
+        const double pd = (sub == 0) ? p[0] : ((sub == 1) ? p[1] : p[2]);  // static indices: p stays in registers
+        phase_row<real>(ka.ptab, s.n, i, sub * ka.kp, pd * ka.inv_L[sub], ka.kmax[sub]);
       }
     }
   }
